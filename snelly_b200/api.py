@@ -1,0 +1,736 @@
+"""Headless mirror of the reference's scene API (js/sceneAPI.js, js/snelly.js, js/renderer.js,
+js/materials.js, js/spectra.js) over libsnelly.
+
+A user scene is written exactly as for the reference: an object with `init(snelly)`, `shader()`
+returning GLSL that defines SDF_SURFACE / SDF_METAL / SDF_DIELECTRIC and optional hooks, and
+optional `syncShader(snelly, shader)`, `getLengthScale()`, `getMinLengthScale()`,
+`getMaxLengthScale()`, `envMap()`, `preframeCallback`, `postframeCallback`, `isReady`.
+`Snelly(scene)` then exposes the same objects (`getRenderer()`, `getCamera()`, `getControls()`,
+`getMaterials()`, ...) with the same property names, defaults and unit conventions (log10 powers,
+log-sqrt(2) aperture). Each `render()` call renders one progressive frame on the GPU.
+"""
+import ctypes
+import json
+import math
+import os
+
+import numpy as np
+
+from . import _native as N
+
+DATA = json.load(open(os.path.join(os.path.dirname(os.path.abspath(__file__)), "data", "materials.json")))
+
+
+# ---------------------------------------------------------------------------------------------
+# small 3-vector helpers (THREE.Vector3 semantics where the reference uses THREE)
+# ---------------------------------------------------------------------------------------------
+class Vector3:
+    def __init__(self, x=0.0, y=0.0, z=0.0):
+        self.x, self.y, self.z = float(x), float(y), float(z)
+
+    def set(self, x, y, z):
+        self.x, self.y, self.z = float(x), float(y), float(z)
+        return self
+
+    def copy(self, v):
+        return self.set(v.x, v.y, v.z)
+
+    def clone(self):
+        return Vector3(self.x, self.y, self.z)
+
+    def tolist(self):
+        return [self.x, self.y, self.z]
+
+
+def _sub(a, b):
+    return [a[0] - b[0], a[1] - b[1], a[2] - b[2]]
+
+
+def _cross(a, b):
+    return [a[1] * b[2] - a[2] * b[1], a[2] * b[0] - a[0] * b[2], a[0] * b[1] - a[1] * b[0]]
+
+
+def _normalize(a):
+    n = math.sqrt(a[0] * a[0] + a[1] * a[1] + a[2] * a[2])
+    return [a[0] / n, a[1] / n, a[2] / n] if n > 0 else [0.0, 0.0, 0.0]
+
+
+class Camera:
+    """THREE.PerspectiveCamera fields the renderer reads (js/snelly.js:40-47, :244-245)."""
+
+    def __init__(self, fov=45.0, aspect=1.0):
+        self.fov = fov
+        self.aspect = aspect
+        self.position = Vector3(1.0, 1.0, 1.0)
+        self.up = Vector3(0.0, 1.0, 0.0)
+        self.aperture = -10.0      # log base sqrt(2), relative to lengthScale
+        self.focalDistance = 1.0   # log base 10, relative to lengthScale
+        self.auto_focus = False
+
+
+class Controls:
+    """The OrbitControls target the camera looks at."""
+
+    def __init__(self):
+        self.target = Vector3(0.0, 0.0, 0.0)
+
+    def update(self):
+        pass
+
+
+def camera_basis(position, target, up):
+    """camPos, camDir, camX, camY as uploaded by js/renderer.js:521-531.
+
+    THREE's lookAt makes the camera's -z axis point at the target and its x axis
+    normalize(cross(up, z)); the world-space up vector is then cross(z, x). camDir is the world
+    direction (-z) and camX = cross(camUp, camDir).
+    """
+    p, t, u = position, target, up
+    z = _normalize(_sub(p, t))
+    if z == [0.0, 0.0, 0.0]:
+        z = [0.0, 0.0, 1.0]
+    x = _cross(u, z)
+    if math.sqrt(sum(v * v for v in x)) == 0.0:  # up parallel to the view axis: nudge as THREE does
+        z = _normalize([z[0] + 1e-4, z[1], z[2]])
+        x = _cross(u, z)
+    x = _normalize(x)
+    y = _cross(z, x)
+    cam_dir = [-z[0], -z[1], -z[2]]
+    # camera.up.transformDirection(matrixWorld): the up vector expressed through the camera axes
+    cam_up = _normalize([x[i] * u[0] + y[i] * u[1] + z[i] * u[2] for i in range(3)])
+    cam_x = _cross(cam_up, cam_dir)
+    return list(p), cam_dir, cam_x, cam_up
+
+
+# ---------------------------------------------------------------------------------------------
+# materials (js/materials.js)
+# ---------------------------------------------------------------------------------------------
+class Surface:
+    """Uber surface (js/materials.js:39-83)."""
+
+    def __init__(self):
+        self.diffuseAlbedo = [1.0, 1.0, 1.0]
+        self.specAlbedo = [1.0, 1.0, 1.0]
+        self.roughness = 0.1
+        self.ior = 1.5
+        self.subsurface = 0.0
+        self.subsurfaceAlbedoRGB = [0.5, 0.5, 0.5]
+        self.subsurfaceMFP = 0.0
+        self.subsurfaceAnisotropy = 0.0
+        self.subsurfaceDiffuseWeight = 1.0
+
+    def syncShader(self, p, snelly):
+        p.surfaceDiffuseAlbedoRGB[:] = self.diffuseAlbedo
+        p.surfaceSpecAlbedoRGB[:] = self.specAlbedo
+        p.surfaceRoughness = self.roughness
+        p.surfaceIor = self.ior
+        p.subsurface = self.subsurface
+        p.subsurfaceAlbedoRGB[:] = self.subsurfaceAlbedoRGB
+        p.subsurfaceMFP = self.subsurfaceMFP
+        p.subsurfaceAnisotropy = self.subsurfaceAnisotropy
+        p.subsurfaceDiffuseWeight = self.subsurfaceDiffuseWeight
+
+
+class Volume:
+    """Homogeneous atmosphere + fog (js/materials.js:193-275)."""
+
+    def __init__(self):
+        self.atmosphereMinX, self.atmosphereMaxX = -10.0, 10.0
+        self.atmosphereMinY, self.atmosphereMaxY = 0.0, 10.0
+        self.atmosphereMinZ, self.atmosphereMaxZ = -10.0, 10.0
+        self.lof10_mfp = 1.0
+        self.scatteringColor = [0.0, 0.0, 0.0]
+        self.absorptionColor = [0.0, 0.0, 0.0]
+        self.anisotropy = 0.0
+        self.emission = 0.0
+        self.emissionColor = [1.0, 1.0, 1.0]
+        self.fogEnable = False
+        self.fogMFP = 0.0
+        self.fogMaxOpticalDepth = 5.0
+        self.fogEmission = [1.0, 1.0, 1.0]
+        self.fogTint = [0.5, 0.5, 0.5]
+
+    def syncShader(self, p, snelly):
+        sca = list(self.scatteringColor)
+        ext = [self.absorptionColor[c] + self.scatteringColor[c] for c in range(3)]
+        p.atmosphereMFP = 10.0 ** self.lof10_mfp
+        p.atmosphereExtinctionCoeffRGB[:] = ext
+        p.atmosphereScatteringCoeffRGB[:] = sca
+        p.atmosphereAnisotropy = self.anisotropy
+        p.atmosphereBoundsMin[:] = [self.atmosphereMinX, self.atmosphereMinY, self.atmosphereMinZ]
+        p.atmosphereBoundsMax[:] = [self.atmosphereMaxX, self.atmosphereMaxY, self.atmosphereMaxZ]
+        p.volumeEmission = self.emission
+        p.volumeEmissionColorRGB[:] = self.emissionColor
+        p.fogEnable = 1 if self.fogEnable else 0
+        p.fogMFP = 10.0 ** self.fogMFP
+        p.fogMaxOpticalDepth = self.fogMaxOpticalDepth
+        p.fogEmission[:] = self.fogEmission
+        p.fogTint[:] = self.fogTint
+
+
+class Metal:
+    """Tabulated conductor (js/materials.js:479-501, 631-669)."""
+
+    def __init__(self, name, table):
+        self._name = name
+        self.roughness = 0.02
+        self.specAlbedo = [1.0, 1.0, 1.0]
+        self.n = list(table["n"])
+        self.k = list(table["k"])
+
+    def getName(self):
+        return self._name
+
+    def syncShader(self, p, snelly):
+        p.metalRoughness = self.roughness
+        p.metalSpecAlbedoRGB[:] = self.specAlbedo
+        p.metalN[:] = self.n
+        p.metalK[:] = self.k
+
+
+class Dielectric:
+    """Dielectric with one of the reference's IOR models (js/materials.js:727-1099)."""
+
+    def __init__(self, name, model, coeffs):
+        self._name = name
+        self.model = model
+        self.coeffs = list(coeffs)
+        self.roughness = 0.005
+        self.absorptionScale = -1.0  # set from the scene's maxLengthScale on first use
+        self.absorptionColor = [1.0, 1.0, 1.0]
+        self.specAlbedo = [1.0, 1.0, 1.0]
+        if model == "abbe":
+            self.iorVal, self.abbe = coeffs[0], coeffs[1]
+
+    def getName(self):
+        return self._name
+
+    def syncShader(self, p, snelly):
+        if self.absorptionScale < 0.0:
+            self.absorptionScale = snelly.maxLengthScale
+        p.dieleRoughness = self.roughness
+        p.dieleSpecAlbedoRGB[:] = self.specAlbedo
+        s = snelly.lengthScale / max(self.absorptionScale, 1.0e-3)
+        p.dieleAbsorptionRGB[:] = [s * max(0.0, 1.0 - self.absorptionColor[c]) for c in range(3)]
+        p.dieleModel = N.IOR_MODELS[self.model]
+        coeffs = [self.iorVal, self.abbe] if self.model == "abbe" else self.coeffs
+        p.dieleNumCoeffs = len(coeffs)
+        for i, c in enumerate(coeffs):
+            p.dieleCoeffs[i] = c
+
+
+class Materials:
+    """Material registry (js/materials.js:1117-1342); defaults BK7 glass and aluminium."""
+
+    def __init__(self):
+        self.dielectrics = {n: Dielectric(n, d["model"], d["coeffs"]) for n, d in DATA["dielectrics"].items()}
+        self.metals = {n: Metal(n, DATA["metal_tables"][t]) for n, t in DATA["metals"].items()}
+        self.surfaceObj = Surface()
+        self.volumeObj = Volume()
+        self.dielectricObj = self.dielectrics["Glass (BK7)"]
+        self.metalObj = self.metals["Aluminium"]
+
+    def loadDielectric(self, name):
+        self.dielectricObj = self.dielectrics[name]
+        return self.dielectricObj
+
+    def loadMetal(self, name):
+        self.metalObj = self.metals[name]
+        return self.metalObj
+
+    def loadSurface(self):
+        return self.surfaceObj
+
+    def loadVolume(self):
+        return self.volumeObj
+
+    getLoadedDielectric = getDielectric = lambda self: self.dielectricObj
+    getLoadedMetal = getMetal = lambda self: self.metalObj
+    getSurface = loadSurface
+    getVolume = loadVolume
+    getDielectrics = lambda self: self.dielectrics
+    getMetals = lambda self: self.metals
+
+    def syncShader(self, p, snelly):
+        self.metalObj.syncShader(p, snelly)
+        self.dielectricObj.syncShader(p, snelly)
+        self.surfaceObj.syncShader(p, snelly)
+        self.volumeObj.syncShader(p, snelly)
+
+
+# ---------------------------------------------------------------------------------------------
+# spectra (js/spectra.js)
+# ---------------------------------------------------------------------------------------------
+class BlackbodySpectrum:
+    def __init__(self, name, desc, temperature):
+        self._name, self._desc, self.skyTemperature = name, desc, temperature
+
+    def getName(self):
+        return self._name
+
+    def native(self):
+        return N.Spectrum(N.SPECTRUM_BLACKBODY, self.skyTemperature, 390.0, 750.0, 550.0)
+
+
+class FlatSpectrum:
+    def __init__(self, name, desc, bandmin, bandmax):
+        self._name, self._desc = name, desc
+        self.min, self.max = bandmin, bandmax
+
+    def getName(self):
+        return self._name
+
+    def native(self):
+        return N.Spectrum(N.SPECTRUM_FLAT, 6000.0, self.min, self.max, 550.0)
+
+
+class MonochromaticSpectrum:
+    def __init__(self, name, desc, wavelength):
+        self._name, self._desc, self.wavelength = name, desc, wavelength
+
+    def getName(self):
+        return self._name
+
+    def native(self):
+        return N.Spectrum(N.SPECTRUM_MONO, 6000.0, 390.0, 750.0, self.wavelength)
+
+
+# ---------------------------------------------------------------------------------------------
+# shader uniform recorder: what a scene's syncShader(snelly, shader) calls
+# ---------------------------------------------------------------------------------------------
+class Shader:
+    """Records the uniform* calls a scene makes (js/gl.js:262-408) for snelly_set_uniforms."""
+
+    def __init__(self):
+        self.calls = {}
+
+    def _put(self, name, typ, vals):
+        self.calls[name] = (typ, vals)
+
+    def uniformF(self, name, v):
+        self._put(name, N.U_FLOAT, [float(v)])
+
+    def uniformI(self, name, v):
+        self._put(name, N.U_INT, [int(v)])
+
+    def uniform2F(self, name, a, b):
+        self._put(name, N.U_VEC2, [float(a), float(b)])
+
+    def uniform3F(self, name, a, b, c):
+        self._put(name, N.U_VEC3, [float(a), float(b), float(c)])
+
+    def uniform4F(self, name, a, b, c, d):
+        self._put(name, N.U_VEC4, [float(a), float(b), float(c), float(d)])
+
+    def uniform2Fv(self, name, v):
+        self._put(name, N.U_VEC2, [float(x) for x in v])
+
+    def uniform3Fv(self, name, v):
+        self._put(name, N.U_VEC3, [float(x) for x in v])
+
+    def uniform4Fv(self, name, v):
+        self._put(name, N.U_VEC4, [float(x) for x in v])
+
+    def uniform1Fv(self, name, v):
+        self._put(name, N.U_FLOAT, [float(x) for x in v])
+
+    def uniformMatrix3Fv(self, name, v):
+        self._put(name, N.U_MAT3, [float(x) for x in v])
+
+
+# ---------------------------------------------------------------------------------------------
+# renderer (js/renderer.js) and the application facade (js/snelly.js)
+# ---------------------------------------------------------------------------------------------
+class Renderer:
+    """Renderer settings with the reference's defaults (js/renderer.js:78-126)."""
+
+    def __init__(self, snelly):
+        self._snelly = snelly
+        self.width = None
+        self.height = None
+        self.renderMode = "pt"
+        self.dispersive = False
+        self.maxSamplesPerFrame = 1
+        self.maxSpp = 1024
+        self.maxBounces = 3
+        self.maxAtmosphereScatters = 1
+        self.maxMarchSteps = 256
+        self.maxSSSSteps = 128
+        self.radianceClamp = 3.0
+        self.wavelengthSamples = 256
+        self.filterRadius = 2.0
+        self.goalFPS = 20.0
+        self.minsSPPToRedraw = 0.0
+        self.shadowStrength = 1.0
+        self.maxStepsIsMiss = True
+        self.interactive = True
+        self.skyPower = 0.0
+        self.skyTemperature = 6000.0
+        self.skyTintUp = [1.0, 1.0, 1.0]
+        self.skyTintDown = [1.0, 1.0, 1.0]
+        self.envMapVisible = True
+        self.envMapPhiRotation = 0.0
+        self.envMapThetaRotation = 0.0
+        self.envMapTransitionAngle = 135.0
+        self.sunPower = -7.0
+        self.sunAngularSize = 5.0
+        self.sunColor = [1.0, 1.0, 1.0]
+        self.sunLatitude = 50.0
+        self.sunLongitude = 0.0  # the reference misspells the default (sunLongitudef, :113)
+        self.sunVisibleDirectly = True
+        self.sphereLightRadius = 1.0
+        self.sphereLightPower = -7.0
+        self.sphereLightColor = [1.0, 1.0, 1.0]
+        self.sphereLightPosition = [0.0, 0.0, 0.0]
+        self.exposure = 0.0
+        self.gamma = 2.2
+        self.contrast = 1.0
+        self.saturation = 1.0
+        self.hueShift = 0.0
+        self.skipProbability = 0.0
+        self.spp = 0.0
+        # B200 build options (no reference counterpart)
+        self.mathMode = N.MATH_FAST
+        self.kernelMode = N.KERNEL_MEGA
+
+    def sun_dir(self):
+        """updateSunDir, js/renderer.js:371-383."""
+        lat = (90.0 - self.sunLatitude) * math.pi / 180.0
+        lon = self.sunLongitude * math.pi / 180.0
+        return [math.sin(lat) * math.cos(lon), math.cos(lat), math.sin(lat) * math.sin(lon)]
+
+    def getSPP(self):
+        return self.spp
+
+
+class Snelly:
+    """The application facade of js/snelly.js, headless: one GPU context and one scene."""
+
+    LAMBDA_MIN, LAMBDA_MAX, SPECTRUM_SAMPLES = 390.0, 750.0, 1024
+
+    def __init__(self, scene, width=256, height=256, device=0, hbm_budget=0, context=None):
+        self.sceneObj = scene
+        self.width, self.height = width, height
+        self.camera = Camera(45.0, width / height)
+        self.camControls = Controls()
+        self.materials = Materials()
+        self.pathtracer = Renderer(self)
+        self.spectra = {}
+        self.spectrumObj = None
+        self._ctx = context if context is not None else Context(device, hbm_budget)
+        self._scene_id = None
+        self._scene_key = None
+        self._job = None
+        self.seed = 1
+        self.initScene()
+
+    # js/snelly.js:209-291
+    def initScene(self):
+        sc = self.sceneObj
+        self.lengthScale = sc.getLengthScale() if hasattr(sc, "getLengthScale") else 1.0
+        self.minLengthScale = sc.getMinLengthScale() if hasattr(sc, "getMinLengthScale") else 1.0e-4
+        self.minLengthScale = max(1.0e-12, self.minLengthScale)
+        self.maxLengthScale = sc.getMaxLengthScale() if hasattr(sc, "getMaxLengthScale") else 1.0e2
+        self.maxLengthScale = min(1.0e9, self.maxLengthScale)
+        po = 2.0 * self.lengthScale
+        self.camera.position.set(po, po, po)
+        self.camControls.target.set(0.0, 0.0, 0.0)
+        self.camera.aperture = -10.0
+        self.camera.focalDistance = 1.0
+        if hasattr(sc, "init"):
+            sc.init(self)
+        r = self.pathtracer
+        if r.width is not None and r.height is not None:
+            self.width, self.height = int(r.width), int(r.height)
+        self.camera.aspect = self.width / self.height  # Snelly._resize
+        self.addSpectrum(BlackbodySpectrum("blackbody", "Blackbody spectrum", r.skyTemperature))
+        self.loadSpectrum("blackbody")
+        self.reset()
+
+    # accessors of the reference's facade
+    def getRenderer(self):
+        return self.pathtracer
+
+    def getCamera(self):
+        return self.camera
+
+    def getControls(self):
+        return self.camControls
+
+    def getMaterials(self):
+        return self.materials
+
+    def getSurface(self):
+        return self.materials.loadSurface()
+
+    def getVolume(self):
+        return self.materials.loadVolume()
+
+    def getLoadedDielectric(self):
+        return self.materials.getLoadedDielectric()
+
+    def getLoadedMetal(self):
+        return self.materials.getLoadedMetal()
+
+    def loadDielectric(self, name):
+        self.materials.loadDielectric(name)
+        self.reset()
+
+    def loadMetal(self, name):
+        self.materials.loadMetal(name)
+        self.reset()
+
+    def getSpectra(self):
+        return self.spectra
+
+    def addSpectrum(self, s):
+        self.spectra[s.getName()] = s
+
+    def loadSpectrum(self, name):
+        self.spectrumObj = self.spectra[name]
+        self.reset()
+
+    def getScene(self):
+        return self.sceneObj
+
+    def showGUI(self, *a):
+        pass
+
+    # -- compile + uniforms ---------------------------------------------------------------------
+    def scene_opts(self):
+        r = self.pathtracer
+        v = self.materials.volumeObj
+        has_atm = any(c > 0.0 for c in v.scatteringColor) or any(c > 0.0 for c in v.absorptionColor)
+        return N.SceneOpts(int(round(r.maxBounces)), int(round(r.maxMarchSteps)), int(round(r.maxAtmosphereScatters)),
+                           int(round(r.maxSamplesPerFrame)), 1 if r.dispersive else 0, 1 if r.interactive else 0,
+                           1 if has_atm else 0, 1 if v.fogEnable else 0, 1 if r.sphereLightPower > -7.0 else 0,
+                           int(r.mathMode), int(r.kernelMode))
+
+    def compileShaders(self):
+        """Renderer.compileShaders (js/renderer.js:217-359): one NVRTC module per source+options."""
+        glsl = self.sceneObj.shader()
+        opts = self.scene_opts()
+        key = (glsl, bytes(opts))
+        if key != self._scene_key:
+            self._scene_id = self._ctx.create_scene(glsl, opts)
+            self._scene_key = key
+        return self._scene_id
+
+    def uniform_params(self):
+        """The uniform block js/renderer.js:520-584 + material syncShader uploads, as SnellyParams."""
+        r, cam = self.pathtracer, self.camera
+        p = N.SnellyParams()
+        p.resolution[:] = [float(self.width), float(self.height)]
+        pos, cdir, cx, cy = camera_basis(cam.position.tolist(), self.camControls.target.tolist(), cam.up.tolist())
+        p.camPos[:], p.camDir[:], p.camX[:], p.camY[:] = pos, cdir, cx, cy
+        p.camFovy = cam.fov
+        p.camAspect = cam.aspect
+        p.camAperture = 0.0 if cam.aperture == -math.inf else self.lengthScale * 1.4142135 ** cam.aperture
+        p.camFocalDistance = self.lengthScale * 10.0 ** cam.focalDistance
+        p.filterRadius = r.filterRadius
+        p.radianceClamp = 10.0 ** r.radianceClamp
+        p.skipProbability = r.skipProbability
+        p.lengthScale = max(self.lengthScale, 1.0e-6)
+        p.maxLengthScale = max(self.maxLengthScale, 1.0e-6)
+        p.minLengthScale = max(self.minLengthScale, 1.0e-6)
+        p.shadowStrength = r.shadowStrength
+        p.maxSSSSteps = int(r.maxSSSSteps)
+        p.maxStepsIsMiss = 1 if r.maxStepsIsMiss else 0
+        p.wavelengthSamples = int(r.wavelengthSamples)
+        p.skyPower = 10.0 ** r.skyPower
+        p.skyTintUp[:] = r.skyTintUp
+        p.skyTintDown[:] = r.skyTintDown
+        p.envMapVisible = 1 if r.envMapVisible else 0
+        p.envMapPhiRotation = min(max(r.envMapPhiRotation, 0.0), 360.0)
+        p.envMapThetaRotation = min(max(r.envMapThetaRotation, 0.0), 180.0)
+        p.envMapTransitionAngle = min(max(r.envMapTransitionAngle, 0.0), 180.0)
+        p.sunPower = 10.0 ** r.sunPower
+        p.sunAngularSize = r.sunAngularSize
+        p.sunLatitude = r.sunLatitude
+        p.sunLongitude = r.sunLongitude
+        p.sunColor[:] = r.sunColor
+        p.sunDir[:] = r.sun_dir()
+        p.sunVisibleDirectly = 1 if r.sunVisibleDirectly else 0
+        p.sphereLightPosition[:] = [x * self.lengthScale for x in r.sphereLightPosition]
+        p.sphereLightRadius = r.sphereLightRadius * self.lengthScale
+        p.sphereLightPower = 10.0 ** r.sphereLightPower / (4.0 * math.pi * r.sphereLightRadius ** 2)
+        p.sphereLightColor[:] = r.sphereLightColor
+        self.materials.syncShader(p, self)
+        return p
+
+    def scene_uniforms(self):
+        sh = Shader()
+        if hasattr(self.sceneObj, "syncShader"):
+            self.sceneObj.syncShader(self, sh)
+        return sh.calls
+
+    def render_desc(self, frames):
+        d = N.RenderDesc()
+        d.width, d.height = int(self.width), int(self.height)
+        d.frames = int(frames)
+        d.mode = {"pt": N.MODE_PT, "normals": N.MODE_NORMALS, "ao": N.MODE_AO}.get(self.pathtracer.renderMode, N.MODE_PT)
+        d.seed = int(self.seed)
+        d.params = self.uniform_params()
+        d.spectrum = self.spectrumObj.native()
+        d.accum_fp64 = 0
+        return d
+
+    # -- progressive rendering ---------------------------------------------------------------------
+    def reset(self, no_recompile=False):
+        """Snelly.reset / Renderer.reset: drop accumulated samples (js/renderer.js:191-201)."""
+        if self._job is not None:
+            self._ctx.destroy_job(self._job)
+            self._job = None
+        self.pathtracer.spp = 0.0
+
+    def render(self, frames=1):
+        """Renderer.render: enqueue `frames` progressive frames (js/renderer.js:462-673)."""
+        r = self.pathtracer
+        if r.spp >= r.maxSpp:
+            return
+        if hasattr(self.sceneObj, "preframeCallback"):
+            self.sceneObj.preframeCallback(self, None)
+        if self._job is None:
+            sid = self.compileShaders()
+            self._ctx.set_uniforms(sid, self.scene_uniforms())
+            self._job = self._ctx.render(sid, self.render_desc(frames))
+        else:
+            self._ctx.advance(self._job, frames)
+        r.spp += frames * int(round(r.maxSamplesPerFrame))
+        if hasattr(self.sceneObj, "postframeCallback"):
+            self.sceneObj.postframeCallback(self, None)
+
+    def readback(self):
+        """(H, W, 4) float32 array: mean X, Y, Z and sample count; row 0 is the bottom row."""
+        return self._ctx.readback(self._job, self.width, self.height)
+
+    def job_id(self):
+        return self._job
+
+
+# ---------------------------------------------------------------------------------------------
+# thin object wrapper of the C ABI
+# ---------------------------------------------------------------------------------------------
+class Context:
+    """One libsnelly context (device, stream, module cache, jobs)."""
+
+    def __init__(self, device=0, hbm_budget=0):
+        self._lib = N.lib()
+        h = ctypes.c_void_p()
+        N.check(self._lib.snelly_init(ctypes.byref(h), int(device), int(hbm_budget)))
+        self._h = h
+
+    def close(self):
+        if self._h:
+            self._lib.snelly_shutdown(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def handle(self):
+        return self._h
+
+    def create_scene(self, glsl, opts):
+        sid = ctypes.c_uint64()
+        log = ctypes.create_string_buffer(1 << 16)
+        N.check(self._lib.snelly_create_scene(self._h, glsl.encode(), ctypes.byref(opts), ctypes.byref(sid), log,
+                                              len(log)))
+        return sid.value
+
+    def destroy_scene(self, sid):
+        N.check(self._lib.snelly_destroy_scene(self._h, sid))
+
+    def set_uniforms(self, sid, calls):
+        if not calls:
+            return
+        arr = (N.Uniform * len(calls))()
+        keep = []
+        for k, (name, (typ, vals)) in enumerate(calls.items()):
+            comps = {N.U_FLOAT: 1, N.U_INT: 1, N.U_BOOL: 1, N.U_VEC2: 2, N.U_VEC3: 3, N.U_VEC4: 4, N.U_MAT3: 9}[typ]
+            count = max(1, len(vals) // comps)
+            arr[k].name = name.encode()
+            arr[k].type = typ
+            arr[k].count = count
+            if typ in (N.U_INT, N.U_BOOL):
+                buf = (ctypes.c_int * len(vals))(*vals)
+                arr[k].i = buf
+            else:
+                buf = (ctypes.c_float * len(vals))(*vals)
+                arr[k].f = buf
+            keep.append(buf)
+        N.check(self._lib.snelly_set_uniforms(self._h, sid, arr, len(calls)))
+
+    def set_texture(self, sid, name, array, linear=True):
+        a = np.ascontiguousarray(array)
+        fmt = {np.dtype(np.float32): 0, np.dtype(np.float16): 1, np.dtype(np.uint8): 2}[a.dtype]
+        if a.ndim == 3:  # (h, w, c) 2-D texture
+            h, w, c = a.shape
+            d = 1
+        else:            # (d, h, w, c) 3-D texture
+            d, h, w, c = a.shape
+        N.check(self._lib.snelly_set_texture(self._h, sid, name.encode(), a.ctypes.data, w, h, d, c, fmt,
+                                             1 if linear else 0))
+
+    def render(self, sid, desc):
+        jid = ctypes.c_uint64()
+        N.check(self._lib.snelly_render(self._h, sid, ctypes.byref(desc), ctypes.byref(jid)))
+        return jid.value
+
+    def restore(self, sid, desc, rng, acc, comp):
+        jid = ctypes.c_uint64()
+        rng, acc, comp = (np.ascontiguousarray(x) for x in (rng, acc, comp))
+        N.check(self._lib.snelly_restore(self._h, sid, ctypes.byref(desc), rng.ctypes.data, acc.ctypes.data,
+                                         comp.ctypes.data, ctypes.byref(jid)))
+        return jid.value
+
+    def advance(self, jid, frames):
+        N.check(self._lib.snelly_advance(self._h, jid, int(frames)))
+
+    def readback(self, jid, width, height, out=None, poll=False):
+        if out is None:
+            out = np.empty((height, width, 4), np.float32)
+        N.check(self._lib.snelly_readback(self._h, jid, out.ctypes.data, out.nbytes, N.READ_POLL if poll else N.READ_WAIT))
+        return out
+
+    def readback_state(self, jid, width, height, fp64=False):
+        n = width * height
+        rng = np.empty((n, 4), np.uint32)
+        acc = np.empty((n, 4), np.float32)
+        comp = np.empty((n, 4), np.float32)
+        acc64 = np.empty((n, 4), np.float64) if fp64 else None
+        N.check(self._lib.snelly_readback_state(self._h, jid, rng.ctypes.data, acc.ctypes.data, comp.ctypes.data,
+                                                acc64.ctypes.data if fp64 else None))
+        return rng, acc, comp, acc64
+
+    def status(self, jid):
+        a, b = ctypes.c_int(), ctypes.c_int()
+        N.check(self._lib.snelly_job_status(self._h, jid, ctypes.byref(a), ctypes.byref(b)))
+        return a.value, b.value
+
+    def cancel(self, jid):
+        N.check(self._lib.snelly_cancel(self._h, jid))
+
+    def destroy_job(self, jid):
+        N.check(self._lib.snelly_destroy_job(self._h, jid))
+
+    def sync(self):
+        N.check(self._lib.snelly_sync(self._h))
+
+    def stream(self):
+        return self._lib.snelly_stream(self._h)
+
+    def launch_count(self):
+        return self._lib.snelly_launch_count(self._h)
+
+    def fp32_peak(self):
+        t, ms = ctypes.c_double(), ctypes.c_double()
+        N.check(self._lib.snelly_measure_fp32_peak(self._h, ctypes.byref(t), ctypes.byref(ms)))
+        return t.value, ms.value
+
+    def flush_l2(self, nbytes=256 << 20):
+        N.check(self._lib.snelly_flush_l2(self._h, int(nbytes)))

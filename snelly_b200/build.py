@@ -1,0 +1,52 @@
+"""Build libsnelly.so (host runtime + ahead-of-time sm_100a kernels) in place.
+
+The scene-dependent kernels (csrc/kernels/*.cu[h]) are compiled at run time by NVRTC for
+sm_100a, one module per scene; this step compiles the C ABI runtime, the GLSL translator and the
+scene-independent kernels with nvcc for sm_100a into snelly_b200/libsnelly.so.
+"""
+import os
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(HERE)
+CUDA = os.environ.get("CUDA_HOME", "/usr/local/cuda")
+SOURCES = ["runtime.cpp", "glsl_transform.cpp", "wavefront.cpp", "aot_kernels.cu"]
+OUT = os.path.join(HERE, "libsnelly.so")
+
+
+def needs_build():
+    if not os.path.exists(OUT):
+        return True
+    t = os.path.getmtime(OUT)
+    csrc = os.path.join(HERE, "csrc")
+    for dp, _, fs in os.walk(csrc):
+        for f in fs:
+            if os.path.getmtime(os.path.join(dp, f)) > t:
+                return True
+    for f in os.listdir(os.path.join(ROOT, "include")):
+        if os.path.getmtime(os.path.join(ROOT, "include", f)) > t:
+            return True
+    return False
+
+
+def build(force=False, verbose=False):
+    if not force and not needs_build():
+        return OUT
+    csrc = os.path.join(HERE, "csrc")
+    cmd = [os.path.join(CUDA, "bin", "nvcc"), "-shared", "-Xcompiler", "-fPIC", "-O2", "-std=c++17",
+           "-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo",
+           "-I" + csrc, "-I" + os.path.join(ROOT, "include"), "-I" + os.path.join(CUDA, "include"),
+           "-o", OUT + ".tmp"]
+    cmd += [os.path.join(csrc, s) for s in SOURCES]
+    cmd += ["-L" + os.path.join(CUDA, "lib64"),
+            "-lnvrtc", "-lcudart", "-Xlinker", "-rpath=" + os.path.join(CUDA, "lib64")]
+    if verbose:
+        print(" ".join(cmd))
+    subprocess.run(cmd, check=True)
+    os.replace(OUT + ".tmp", OUT)
+    return OUT
+
+
+if __name__ == "__main__":
+    build(force="--force" in sys.argv, verbose=True)

@@ -1,0 +1,535 @@
+// pt_integrator.cuh - the per-sample estimator: next-event estimation, homogeneous atmosphere,
+// subsurface random walk and the camera path (PT:1221-1989), on top of pt_device.cuh.
+//
+// Used as is by the path-per-thread kernel, and piecewise by the wavefront stages.
+#pragma once
+#include "pt_device.cuh"
+
+namespace sdev {
+
+// Next-event estimation at a surface vertex (PT:1221-1295).
+SD_FN Rad direct_surface(const Ctx& c, const vec3& pW, const Frame& f, const vec3& wiW, int mat, Rng& g,
+                         float& skyPdf, float& sunPdf, float& sphPdf) {
+  const SnellyParams& P = c.P;
+  vec3 wiL = to_local(wiW, f);
+  Rad Ld = Rad(0.0f);
+  if (P.skyPower > kRadianceEps) {
+    vec3 woL = sample_cosine(g, skyPdf);
+    vec3 woW = to_world(woL, f);
+    Rad Li = sky_radiance(c, woW);
+    if (avg(Li) > kRadianceEps) {
+      Li = shadow_scale(c, Li, transmittance(c, pW, woW, P.maxLengthScale));
+      if (avg(Li) > kRadianceEps) {
+        float bp = fmaxf(kPdfEps, bsdf_pdf(c, pW, f, wiL, woL, mat));
+        Rad fv = bsdf_eval(c, pW, f, wiL, woL, mat);
+        float w = balance(skyPdf, bp);
+        Ld += fv * Li / fmaxf(kPdfEps, skyPdf) * fabsf(glsl::dot(woW, f.n)) * w;
+      }
+    }
+  }
+  if (P.sunPower > kRadianceEps) {
+    vec3 woW = sample_sun_dir(c, g, sunPdf);
+    vec3 woL = to_local(woW, f);
+    Rad Li = woL.z < 0.0f ? Rad(0.0f) : sun_radiance(c, woW);
+    if (avg(Li) > kRadianceEps) {
+      Li = shadow_scale(c, Li, transmittance(c, pW, woW, P.maxLengthScale));
+      if (avg(Li) > kRadianceEps) {
+        float bp = fmaxf(kPdfEps, bsdf_pdf(c, pW, f, wiL, woL, mat));
+        Rad fv = bsdf_eval(c, pW, f, wiL, woL, mat);
+        float w = balance(sunPdf, bp);
+        Ld += fv * Li / fmaxf(kPdfEps, sunPdf) * fabsf(glsl::dot(woW, f.n)) * w;
+      }
+    }
+  }
+#ifdef HAS_SPHERE_LIGHT
+  if (P.sphereLightPower > kRadianceEps &&
+      glsl::dot(pW - v3(P.sphereLightPosition), f.n) <= P.sphereLightRadius) {
+    vec3 pHit;
+    Rad Li = sample_sphere_light(c, g, pW, pHit, sphPdf);
+    if (avg(Li) > kRadianceEps) {
+      float dist = fmaxf(0.0f, glsl::length(pHit - pW) - 3.0f * P.minLengthScale);
+      vec3 woW = glsl::normalize(pHit - pW);
+      vec3 woL = to_local(woW, f);
+      Li = shadow_scale(c, Li, transmittance(c, pW, woW, dist));
+      if (avg(Li) > kRadianceEps) {
+        float bp = fmaxf(kPdfEps, bsdf_pdf(c, pW, f, wiL, woL, mat));
+        Rad fv = bsdf_eval(c, pW, f, wiL, woL, mat);
+        float w = balance(sphPdf, bp);
+        Ld += fv * Li / fmaxf(kPdfEps, sphPdf) * fabsf(glsl::dot(woW, f.n)) * w;
+      }
+    }
+  }
+#endif
+  return glsl::min(Rad(P.radianceClamp), Ld);
+}
+
+#ifdef HAS_ATMOSPHERE
+// Light scattered towards -rayDir at a point of the atmosphere (PT:1299-1363).
+SD_FN Rad direct_volume(const Ctx& c, const vec3& pW, const vec3& rayDir, Rng& g) {
+  const SnellyParams& P = c.P;
+  Rad Ld = Rad(0.0f);
+  if (P.skyPower > kRadianceEps) {
+    vec3 woW = sample_sphere_ref(g);
+    float pdf = 1.0f / (4.0f * kPi);
+    Rad Li = sky_radiance(c, woW);
+    if (avg(Li) > kRadianceEps) {
+      Li = shadow_scale(c, Li, transmittance(c, pW, woW, P.maxLengthScale));
+      if (avg(Li) > kRadianceEps) {
+        float ph = hg_phase(glsl::dot(-rayDir, -woW), P.atmosphereAnisotropy);
+        Ld += ph * Li / fmaxf(kPdfEps, pdf);
+      }
+    }
+  }
+  if (P.sunPower > kRadianceEps) {
+    float pdf;
+    vec3 woW = sample_sun_dir(c, g, pdf);
+    Rad Li = sun_radiance(c, woW);
+    if (avg(Li) > kRadianceEps) {
+      Li = shadow_scale(c, Li, transmittance(c, pW, woW, P.maxLengthScale));
+      if (avg(Li) > kRadianceEps) {
+        float ph = hg_phase(glsl::dot(-rayDir, -woW), P.atmosphereAnisotropy);
+        Ld += ph * Li / fmaxf(kPdfEps, pdf);
+      }
+    }
+  }
+#ifdef HAS_SPHERE_LIGHT
+  if (P.sphereLightPower > kRadianceEps) {
+    float pdf;
+    vec3 pHit;
+    Rad Li = sample_sphere_light(c, g, pW, pHit, pdf);
+    if (avg(Li) > kRadianceEps) {
+      float dist = fmaxf(0.0f, glsl::length(pHit - pW) - 3.0f * P.minLengthScale);
+      vec3 woW = glsl::normalize(pHit - pW);
+      Li = shadow_scale(c, Li, transmittance(c, pW, woW, dist));
+      if (avg(Li) > kRadianceEps) {
+        float ph = hg_phase(glsl::dot(-rayDir, -woW), P.atmosphereAnisotropy);
+        Ld += ph * Li / fmaxf(kPdfEps, pdf);
+      }
+    }
+  }
+#endif
+  return glsl::min(Rad(P.radianceClamp), Ld);
+}
+
+// Single-scattering estimate over a segment (PT:1365-1417).
+SD_FN Rad atm_inscatter(const Ctx& c, const vec3& pW, const vec3& d, float len, Rng& g) {
+  const SnellyParams& P = c.P;
+  Rad Ls = Rad(0.0f);
+#ifdef HAS_FOG
+  if (P.fogEnable) {
+    Rad TrFog = transmittance_free(c, pW, d, len);
+    Ls = (Rad(1.0f) - TrFog) * albedo(v3(P.fogEmission), c.cmf);
+  }
+#endif
+  Rad ext = vol_extinction(c), sca = vol_scattering(c);
+  float en = avg(ext), sn = avg(sca);
+  if (en < kRadianceEps || sn < kRadianceEps) return Ls;
+  float t0, t1;
+  if (!atmosphere_segment(c, pW, d, len, t0, t1)) return Ls;
+  float T01 = expf(-(t1 - t0) * en);
+  float ts = t0 - logf(1.0f - rand01(g) * (1.0f - T01)) / en;
+  vec3 ps = pW + ts * d;
+  Rad od = (ts - t0) * ext;
+  Rad Trp = glsl::exp(-od);
+  float inv = (1.0f - T01) * expf(avg(od)) / en;
+  Rad Li = direct_volume(c, ps, d, g);
+  Ls += Trp * sca * Li * inv;
+#ifdef HAS_VOLUME_EMISSION
+  vec3 wo = sample_hg(d, P.atmosphereAnisotropy, g);
+  Hit h = march_ray(c.job, ps, wo, P.maxLengthScale);
+  if (h.hit) Ls += Trp * sca * vol_emission(c, h.p) * inv;
+#endif
+  return Ls;
+}
+
+// Scatter-point and direction sample for a continuing path (PT:1419-1442).
+SD_FN Rad atm_scatter_sample(const Ctx& c, const vec3& pW, const vec3& d, float len, Rng& g, vec3& ps, vec3& wo) {
+  Rad ext = vol_extinction(c), sca = vol_scattering(c);
+  float en = avg(ext);
+  float t0, t1;
+  if (!atmosphere_segment(c, pW, d, len, t0, t1)) return Rad(0.0f);
+  float T01 = expf(-(t1 - t0) * en);
+  float ts = t0 - logf(1.0f - rand01(g) * (1.0f - T01)) / en;
+  ps = pW + ts * d;
+  Rad od = (ts - t0) * ext;
+  Rad Trp = glsl::exp(-od);
+  float inv = (1.0f - T01) * expf(avg(od)) / en;
+  wo = sample_hg(d, c.P.atmosphereAnisotropy, g);
+  return sca * Trp * inv;
+}
+#endif  // HAS_ATMOSPHERE
+
+// PT:1446-1457
+SD_FN float scatter_prob(const Ctx& c, const Rad& Tr) {
+#ifdef HAS_ATMOSPHERE
+  Rad ext = vol_extinction(c), sca = vol_scattering(c);
+  return avg(sca / ext) * (1.0f - avg(Tr));
+#else
+  (void)c;
+  (void)Tr;
+  return 0.0f;
+#endif
+}
+
+#ifdef HAS_SURFACE
+// Subsurface random walk inside SDF_SURFACE (PT:1464-1518). Returns true at an exit point.
+SD_FN bool sss_walk(const Ctx& c, const vec3& pW, const Frame& f, Rng& g, const Rad& ssAlb, Rad& walkThr, vec3& pExit) {
+  const SnellyParams& P = c.P;
+  vec3 pw = pW - 3.0f * P.minLengthScale * f.n;
+  float pdf;
+  vec3 dl = sample_cosine(g, pdf);
+  vec3 dw = -to_world(dl, f);
+  walkThr = Rad(1.0f);
+  for (int n = 0; n < 2048; ++n) {
+    if (n > P.maxSSSSteps) break;
+    float step = -logf(rand01(g)) * P.subsurfaceMFP * P.lengthScale;
+    Hit h = march_ray(c.job, pw, dw, step);
+    if (h.hit) {
+      pExit = h.p;
+      return true;
+    }
+    if (n > 4) {
+      float cont = glsl::clamp(10.0f * maxc(walkThr), 0.0f, 1.0f);
+      if (rand01(g) < 1.0f - cont) break;
+      walkThr /= cont;
+    }
+    dw = sample_hg(dw, P.subsurfaceAnisotropy, g);
+    pw += step * dw;
+    walkThr *= ssAlb;
+  }
+  return false;
+}
+
+// Direct light at a subsurface exit point through a Lambertian lobe (PT:1521-1593).
+SD_FN Rad sss_exit_radiance(const Ctx& c, const vec3& pW, const Frame& f, Rng& g, const Rad& dAlbExit,
+                            float& skyPdf, float& sunPdf, float& sphPdf) {
+  const SnellyParams& P = c.P;
+  vec3 off = 3.0f * P.minLengthScale * f.n;
+  Rad Ld = Rad(0.0f);
+  Rad lobe = glsl::mix(Rad(1.0f), dAlbExit, P.subsurfaceDiffuseWeight) / kPi;
+  if (P.skyPower > kRadianceEps) {
+    vec3 woL = sample_cosine(g, skyPdf);
+    vec3 woW = to_world(woL, f);
+    Rad Li = sky_radiance(c, woW);
+    if (avg(Li) > kRadianceEps) {
+      Li = shadow_scale(c, Li, transmittance(c, pW + off, woW, P.maxLengthScale));
+      if (avg(Li) > kRadianceEps) {
+        float w = balance(skyPdf, pdf_cosine(woL));
+        Ld += lobe * Li / fmaxf(kPdfEps, skyPdf) * fabsf(glsl::dot(woW, f.n)) * w;
+      }
+    }
+  }
+  if (P.sunPower > kRadianceEps) {
+    vec3 woW = sample_sun_dir(c, g, sunPdf);
+    vec3 woL = to_local(woW, f);
+    Rad Li = woL.z < 0.0f ? Rad(0.0f) : sun_radiance(c, woW);
+    if (avg(Li) > kRadianceEps) {
+      Li = shadow_scale(c, Li, transmittance(c, pW + off, woW, P.maxLengthScale));
+      if (avg(Li) > kRadianceEps) {
+        float w = balance(sunPdf, pdf_cosine(woL));
+        Ld += lobe * Li / fmaxf(kPdfEps, sunPdf) * fabsf(glsl::dot(woW, f.n)) * w;
+      }
+    }
+  }
+#ifdef HAS_SPHERE_LIGHT
+  if (P.sphereLightPower > kRadianceEps &&
+      glsl::dot(pW - v3(P.sphereLightPosition), f.n) <= P.sphereLightRadius) {
+    vec3 pHit;
+    Rad Li = sample_sphere_light(c, g, pW, pHit, sphPdf);
+    if (avg(Li) > kRadianceEps) {
+      float dist = fmaxf(0.0f, glsl::length(pHit - pW) - 3.0f * P.minLengthScale);
+      vec3 woW = glsl::normalize(pHit - pW);
+      vec3 woL = to_local(woW, f);
+      Li = shadow_scale(c, Li, transmittance(c, pW + off, woW, dist));
+      if (avg(Li) > kRadianceEps) {
+        float w = balance(sphPdf, pdf_cosine(woL));
+        Ld += lobe * Li / fmaxf(kPdfEps, sphPdf) * fabsf(glsl::dot(woW, f.n)) * w;
+      }
+    }
+  }
+#endif
+  return glsl::min(Rad(P.radianceClamp), Ld);
+}
+#endif  // HAS_SURFACE
+
+// Primary ray through the (jittered) pixel, pinhole or thin lens (PT:1602-1622).
+SD_FN void primary_ray(const SnellyParams& P, const vec2& pixel, Rng& g, vec3& start, vec3& dir) {
+  vec2 ndc = -1.0f + 2.0f * (pixel / vec2(P.resolution[0], P.resolution[1]));
+  float fh = tanf(0.5f * glsl::radians(P.camFovy));
+  float fw = P.camAspect * fh;
+  vec3 s = -fw * ndc.x * v3(P.camX) + fh * ndc.y * v3(P.camY);
+  dir = safe_normalize(v3(P.camDir) + s);
+  if (P.camAperture <= 0.0f) {
+    start = v3(P.camPos);
+    return;
+  }
+  vec3 focal = v3(P.camPos) + P.camFocalDistance * dir / glsl::dot(dir, v3(P.camDir));
+  float rad = P.camAperture * sqrtf(rand01(g));
+  float th = 2.0f * kPi * rand01(g);
+  vec3 lens = v3(P.camPos) + rad * (-v3(P.camX) * cosf(th) + v3(P.camY) * sinf(th));
+  start = lens;
+  dir = safe_normalize(focal - lens);
+}
+
+// Triangle-filter importance sample in [-1, 1] (PT:1928-1932).
+SD_FN float tent(float xi) { return xi < 0.5f ? sqrtf(2.0f * xi) - 1.0f : 1.0f - sqrtf(2.0f - 2.0f * xi); }
+
+// One camera path (PT:1625-1926).
+SD_FN Rad camera_path(const Ctx& c, vec3 pW, vec3 rayDir, Rng& g) {
+  const SnellyParams& P = c.P;
+  Rad L = Rad(0.0f);
+  float misSky = 1.0f, misSun = 1.0f;
+#ifdef HAS_SPHERE_LIGHT
+  float misSph = 1.0f;
+#endif
+#ifdef HAS_DIELECTRIC
+  bool inDiele = c.sc.SDF_DIELECTRIC(pW) < 0.0f;
+#endif
+  Rad thr = Rad(1.0f);
+  int atmScatters = 0;
+  (void)atmScatters;
+  for (int vertex = 0; vertex <= MAX_BOUNCES; ++vertex) {
+    if (maxc(thr) < kThroughputEps) break;
+    Hit h = march_ray(c.job, pW, rayDir, P.maxLengthScale);
+    float rayLength = P.maxLengthScale;
+    if (h.hit) {
+      rayLength = glsl::length(h.p - pW);
+    } else {
+      // escaped: environment, sun and sphere light (PT:1657-1712)
+      float segLen;
+      Rad Tr;
+#ifdef HAS_SPHERE_LIGHT
+      vec3 pLight;
+      Rad LiSph = (P.sphereLightPower < kRadianceEps) ? Rad(0.0f) : sphere_light_hit(c, pW, rayDir, pLight);
+      if (avg(LiSph) > kRadianceEps) {
+        segLen = glsl::length(pLight - pW);
+        Tr = transmittance_free(c, pW, rayDir, segLen);
+        float sp = scatter_prob(c, Tr);
+        L += thr * Tr * misSph * LiSph / (1.0f - sp);
+      } else
+#endif
+      {
+        segLen = P.maxLengthScale;
+        Tr = transmittance_free(c, pW, rayDir, segLen);
+        float sp = scatter_prob(c, Tr);
+        if (avg(Tr) > kRadianceEps) {
+          if (!(vertex == 0 && !P.envMapVisible) && misSky > 0.0f)
+            L += thr * Tr * misSky * sky_radiance(c, rayDir) / (1.0f - sp);
+          if (!(vertex == 0 && !P.sunVisibleDirectly) && misSun > 0.0f)
+            L += thr * Tr * misSun * sun_radiance(c, rayDir) / (1.0f - sp);
+        }
+      }
+#ifdef HAS_ATMOSPHERE
+      if (vertex < 2) L += thr * atm_inscatter(c, pW, rayDir, segLen, g);
+      if (atmScatters + 1 < MAX_ATMOSPHERE_SCATTERS) {
+        float sp = scatter_prob(c, Tr);
+        if (sp > rand01(g)) {
+          vec3 ps(0.0f), wo(0.0f);
+          thr *= atm_scatter_sample(c, pW, rayDir, segLen, g, ps, wo) / fmaxf(kDenomTol, sp);
+          pW = ps;
+          rayDir = wo;
+          atmScatters++;
+          continue;
+        }
+      }
+#endif
+      (void)segLen;
+      break;
+    }
+
+    Rad Tr = Rad(1.0f);
+    bool hitSphereLight = false;
+    (void)hitSphereLight;
+#ifdef HAS_SPHERE_LIGHT
+    {
+      vec3 pLight;
+      Rad LiSph = (P.sphereLightPower < kRadianceEps) ? Rad(0.0f) : sphere_light_hit(c, pW, rayDir, pLight);
+      if (avg(LiSph) > kRadianceEps) {
+        float segLen = glsl::length(pLight - pW);
+        if (segLen < rayLength) {
+          hitSphereLight = true;
+          Tr = transmittance_free(c, pW, rayDir, segLen);
+          L += thr * Tr * misSph * LiSph;
+#ifdef HAS_ATMOSPHERE
+          if (vertex < 2) L += thr * atm_inscatter(c, pW, rayDir, segLen, g);
+#endif
+        }
+      }
+    }
+#endif
+#ifdef HAS_DIELECTRIC
+    if (inDiele) thr *= glsl::exp(-rayLength * diele_absorption(c, pW));  // Beer's law (PT:1740-1744)
+#endif
+#ifdef HAS_ATMOSPHERE
+    if (vertex < 2) L += thr * atm_inscatter(c, pW, rayDir, rayLength, g);
+    if (!hitSphereLight) Tr = transmittance_free(c, pW, rayDir, rayLength);
+    if (atmScatters + 1 < MAX_ATMOSPHERE_SCATTERS) {
+      float sp = scatter_prob(c, Tr);
+      if (sp > rand01(g)) {
+        vec3 ps(0.0f), wo(0.0f);
+        thr *= atm_scatter_sample(c, pW, rayDir, rayLength, g, ps, wo) / fmaxf(kDenomTol, sp);
+        pW = ps;
+        rayDir = wo;
+        atmScatters++;
+        continue;
+      }
+      thr /= fmaxf(kDenomTol, 1.0f - sp);
+    }
+    if (hitSphereLight) break;
+    thr *= transmittance_free(c, pW, rayDir, rayLength);
+#endif
+    (void)Tr;
+
+    // surface interaction (PT:1782-1794)
+    pW = h.p;
+    vec3 nW = sdf_normal(c.job, pW, h.mat);
+    vec3 ngW = nW;
+    Frame fr = make_frame(nW);
+#ifdef HAS_NORMALMAP
+    nW = perturb_normal(c, pW, fr, h.mat);
+    if (glsl::dot(nW, rayDir) > 0.0f && h.mat != MAT_DIELE) nW = 2.0f * ngW * glsl::dot(ngW, nW) - nW;
+    fr = make_frame(nW);
+#endif
+
+    // surface scatter or subsurface walk (PT:1796-1811)
+    bool doSSS = false;
+    float probSSS = 0.0f;
+    Rad ssAlb = Rad(0.0f);
+    (void)ssAlb;
+#ifdef HAS_SURFACE
+    if (P.subsurfaceMFP > 0.0f) {
+      ssAlb = subsurf_albedo(c, pW, fr.n);
+      float wd = (1.0f - P.subsurface) * avg(surf_diffuse(c, pW, fr.n, -rayDir));
+      float ws = avg(surf_specular(c, pW, fr.n, -rayDir));
+      float wss = P.subsurface * avg(ssAlb) * 3.0f;
+      float tot = wd + ws + wss;
+      probSSS = wss / (tot + kDenomTol);
+      probSSS = glsl::clamp(probSSS, 0.0f, 1.0f - kPdfEps);
+      doSSS = rand01(g) < probSSS;
+    }
+#endif
+    if (!doSSS) {
+      vec3 wiW = -rayDir;
+      vec3 wiL = to_local(wiW, fr);
+      vec3 woL(0.0f);  // an uninitialised local in the reference (PT:1820), zero under WebGL
+      float bsdfPdf = 0.0f;
+      Rad f = bsdf_sample(c, pW, fr, wiL, h.mat, woL, bsdfPdf, g);
+      vec3 woW = to_world(woL, fr);
+#ifdef HAS_DIELECTRIC
+      if (h.mat == MAT_DIELE && glsl::dot(wiW, ngW) * glsl::dot(woW, ngW) < 0.0f) inDiele = !inDiele;
+#endif
+#ifdef HAS_VOLUME_EMISSION
+      L += thr * vol_emission(c, pW);
+#endif
+      rayDir = woW;
+      pW += ngW * glsl::sign(glsl::dot(rayDir, ngW)) * 3.0f * P.minLengthScale;
+      float skyPdf = 0.0f, sunPdf = 0.0f, sphPdf = 0.0f;
+#ifdef HAS_DIELECTRIC
+      if (!inDiele)
+#endif
+        L += thr * direct_surface(c, pW, fr, wiW, h.mat, g, skyPdf, sunPdf, sphPdf);
+      Rad fop = glsl::min(Rad(P.radianceClamp), f / fmaxf(kPdfEps, bsdfPdf));
+      thr *= fop * fabsf(glsl::dot(woW, nW)) / fmaxf(kPdfEps, 1.0f - probSSS);
+      misSky = balance(bsdfPdf, skyPdf);
+      misSun = balance(bsdfPdf, sunPdf);
+#ifdef HAS_SPHERE_LIGHT
+      misSph = balance(bsdfPdf, sphPdf);
+#endif
+    }
+#ifdef HAS_SURFACE
+    else {
+      // subsurface random walk to a new vertex (PT:1866-1918)
+      Rad dAlbEntry = surf_diffuse(c, pW, fr.n, -rayDir);
+      (void)dAlbEntry;
+      Rad walkThr = Rad(0.0f);
+      vec3 pExit(0.0f);
+      Frame fw = fr;
+      fw.n = ngW;  // geometric normal for the entry (the tangents stay those of the shading frame)
+      if (!sss_walk(c, pW, fw, g, ssAlb, walkThr, pExit)) break;
+      pW = pExit;
+      nW = sdf_normal(c.job, pExit, MAT_SURFA);
+      Frame fe = make_frame(nW);
+      float bsdfPdf = 0.0f;
+      vec3 dExit = sample_cosine(g, bsdfPdf);
+      vec3 woW = to_world(dExit, fe);
+      rayDir = woW;
+      thr *= walkThr;
+      float skyPdf = 0.0f, sunPdf = 0.0f, sphPdf = 0.0f;
+      Rad dAlbExit = surf_diffuse(c, pW, nW, -rayDir);
+#ifdef HAS_DIELECTRIC
+      if (!inDiele)
+#endif
+        L += thr * sss_exit_radiance(c, pExit, fe, g, dAlbExit, skyPdf, sunPdf, sphPdf);
+      misSky = balance(bsdfPdf, skyPdf);
+      misSun = balance(bsdfPdf, sunPdf);
+#ifdef HAS_SPHERE_LIGHT
+      misSph = balance(bsdfPdf, sphPdf);
+#endif
+      Rad lobe = glsl::mix(Rad(1.0f), dAlbExit, P.subsurfaceDiffuseWeight) / kPi;
+      Rad fop = glsl::min(Rad(P.radianceClamp), lobe / fmaxf(kPdfEps, bsdfPdf));
+      thr *= fop * fabsf(glsl::dot(woW, nW)) / fmaxf(kPdfEps, probSSS);
+      pW += nW * glsl::sign(glsl::dot(rayDir, nW)) * 3.0f * P.minLengthScale;
+    }
+#endif
+    if (maxc(thr) < kThroughputEps) break;
+  }
+  return L;
+}
+
+// Wavelength for this pixel and frame (PT:1936-1947): the inverse CDF of the emission spectrum
+// at a stratum centre in [0.1, 0.9]; returns the CIE XYZ weights at that wavelength.
+SD_FN vec3 pick_wavelength(Ctx& c, Rng& g) {
+#ifdef DISPERSION_ENABLED
+  const SnellyParams& P = c.P;
+  float ns = float(P.wavelengthSamples);
+  float xi = 0.1f + 0.8f * (0.5f + floorf(ns * rand01(g))) / ns;
+  float w = table1(c.Pg->icdfTable, SNELLY_ICDF_SAMPLES, xi);
+  c.lambda = 390.0f + (750.0f - 390.0f) * w;
+  vec3 xyz = table_xyz(c.Pg->xyzTable, w);
+  c.cmf = xyz_to_rgb_normalized(xyz);
+  return xyz;
+#else
+  (void)g;
+  c.lambda = 390.0f + (750.0f - 390.0f) * 0.5f;
+  c.cmf = vec3(0.0f);
+  return vec3(0.0f);
+#endif
+}
+
+// A scene's CONSTRUCT_PRIMARY_RAY hook works on the reference's float RNG state; the integer
+// state converts to and from it exactly (all lanes are integers below 2^23).
+SD_FN void primary_ray_hook(const Ctx& c, const vec2& pixel, Rng& g, vec3& start, vec3& dir) {
+#ifdef HAS_CUSTOM_CAMERA
+  vec4 r(float(g.s[0]), float(g.s[1]), float(g.s[2]), float(g.s[3]));
+  c.sc.CONSTRUCT_PRIMARY_RAY(pixel, r, start, dir);
+  g.s[0] = unsigned(r.x);
+  g.s[1] = unsigned(r.y);
+  g.s[2] = unsigned(r.z);
+  g.s[3] = unsigned(r.w);
+#else
+  primary_ray(c.P, pixel, g, start, dir);
+#endif
+}
+
+// All samples of one pixel for one frame (PT:1934-1989); returns the XYZ contribution.
+SD_FN vec3 pixel_samples(Ctx& c, const vec2& pixel, Rng& g) {
+  vec3 xyz = pick_wavelength(c, g);
+  c.sun = make_frame(v3(c.P.sunDir));
+  Rad L = Rad(0.0f);
+  for (int n = 0; n < MAX_SAMPLES_PER_FRAME; ++n) {
+    float jx = 0.5f * c.P.filterRadius * tent(rand01(g));
+    float jy = 0.5f * c.P.filterRadius * tent(rand01(g));
+    vec3 start, dir;
+    primary_ray_hook(c, pixel + vec2(jx, jy), g, start, dir);
+    L += camera_path(c, start, dir, g);
+  }
+  L /= float(MAX_SAMPLES_PER_FRAME);
+#ifdef DISPERSION_ENABLED
+  return xyz * L;
+#else
+  (void)xyz;
+  return rgb_to_xyz(L);
+#endif
+}
+
+}  // namespace sdev

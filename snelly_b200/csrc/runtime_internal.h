@@ -1,0 +1,109 @@
+// runtime_internal.h - internal types of libsnelly (not part of the C ABI).
+#pragma once
+#include <cuda_runtime.h>
+
+#include <map>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "glsl_transform.h"
+#include "snelly.h"
+
+#ifndef SNELLY_MAX_BATCH
+#define SNELLY_MAX_BATCH 32
+#endif
+
+namespace snelly {
+
+int fail(int code, const std::string& msg);
+
+struct DevBuf {
+  void* ptr = nullptr;
+  size_t bytes = 0;
+};
+
+// The scene string after the host-side assembly of js/renderer.js:217-316.
+struct SceneSource {
+  std::string glsl;     // with default hooks appended
+  std::string defines;  // HAS_* / MAX_* preprocessor lines
+  GlslTransformResult xf;
+  bool has_custom_camera = false, has_surface = false, has_metal = false, has_dielectric = false;
+  bool has_surface_nm = false, has_metal_nm = false, has_dielectric_nm = false, has_volume_emission = false;
+};
+
+struct Module {
+  std::string key;
+  cudaLibrary_t lib = nullptr;
+  cudaKernel_t f_seed = nullptr, f_frame_mega = nullptr, f_resolve = nullptr;
+  cudaKernel_t f_wf_generate = nullptr, f_wf_extend = nullptr, f_wf_shade = nullptr, f_wf_shadow = nullptr,
+               f_wf_accumulate = nullptr;
+  cudaKernel_t f_firsthit = nullptr;
+  char* c_params = nullptr;  // device addresses of the constant banks
+  char* c_uniforms = nullptr;
+  size_t c_uniforms_bytes = 0, slot_uniform_bytes = 0;
+};
+
+struct Scene {
+  uint64_t id = 0;
+  SceneSource src;
+  snelly_scene_opts opts{};
+  int kernel_mode = SNELLY_KERNEL_MEGA;
+  std::vector<unsigned char> ublock;  // uniform block (host copy), snapshotted by jobs
+  std::map<std::string, DevBuf> textures;
+  std::shared_ptr<Module> module;
+};
+
+struct Job {
+  uint64_t id = 0;
+  Scene* scene = nullptr;
+  snelly_render_desc desc{};
+  SnellyParams params{};
+  std::vector<unsigned char> ublock;
+  DevBuf rng, acc, comp, acc64, out, icdf, env, gparams, tables;
+  DevBuf wf;  // wavefront path state and queues
+  int blocks = 0;
+  int frames_enqueued = 0;
+  bool cancelled = false;
+  cudaEvent_t done = nullptr;
+};
+
+struct Context {
+  int device = 0;
+  int sm_count = 0;
+  cudaStream_t stream = nullptr;
+  std::mutex mu;
+  std::map<uint64_t, Scene> scenes;
+  std::map<uint64_t, Job> jobs;
+  std::map<std::string, std::shared_ptr<Module>> module_cache;
+  DevBuf xyz;
+  size_t budget = 0, used = 0;
+  uint64_t next_id = 0;
+  uint64_t launches = 0;
+  std::string csrc_dir, kernel_dir, include_dir, cache_dir;
+
+  ~Context();
+  int alloc(DevBuf& b, size_t bytes);
+  void release(DevBuf& b);
+  int compile_module(const std::string& src, int math_mode, std::shared_ptr<Module>* out, std::string* log);
+  int launch(cudaKernel_t f, int blocks, int threads, void** args);
+  int upload_slot(Job& j, int slot);
+  int single_job_tables(Job& j);
+  int enqueue_frames(Job& j, int frames);
+  void free_job(Job& j);
+  // wavefront integrator (wavefront.cpp)
+  int alloc_wavefront(Job& j);
+  void release_wavefront(Job& j);
+  int enqueue_wavefront_frame(Job& j);
+};
+
+int assemble_scene(const std::string& glsl, const snelly_scene_opts& o, SceneSource* out);
+std::string program_source(const SceneSource& ss);
+
+}  // namespace snelly
+
+// The opaque handle of the C ABI.
+struct snelly_ctx {
+  std::unique_ptr<snelly::Context> c;
+};

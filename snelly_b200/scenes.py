@@ -1,0 +1,234 @@
+"""Benchmark and test scenes, written against the reference's scene API.
+
+Each scene is the synthetic workload of one benchmark configuration: C0 "plain method, small
+size", C1 "dispersive and metallic fractal" (the headline 1080p workload), C2 "volumetric and
+subsurface". Their GLSL is written for this package; the fractal distance estimators are the
+standard Menger-sponge and Mandelbox formulations.
+"""
+import math
+
+import numpy as np
+
+from .api import Dielectric, FlatSpectrum
+
+
+class PlainSphere:
+    """C0: sphere of radius 1 unioned with the plane y = -1, diffuse grey 0.8, roughness 0.3,
+    uniform white environment of radiance 1, 256x256, pinhole camera at (0,1,5) looking at the
+    origin, fov 45, maxBounces 4, 16 spp, maxMarchSteps 256, minLengthScale 1e-4, wavelengths
+    drawn from a flat 390-750 nm spectrum."""
+
+    width, height, spp = 256, 256, 16
+
+    def init(self, snelly):
+        r = snelly.getRenderer()
+        r.width, r.height = self.width, self.height
+        r.dispersive = True
+        r.interactive = False
+        r.maxBounces = 4
+        r.maxMarchSteps = 256
+        r.skyPower = 0.0          # 10^0 = radiance 1
+        r.sunPower = -7.0         # off
+        r.envMapVisible = True
+        cam = snelly.getCamera()
+        cam.fov = 45.0
+        cam.position.set(0.0, 1.0, 5.0)
+        cam.aperture = -math.inf  # pinhole
+        snelly.getControls().target.set(0.0, 0.0, 0.0)
+        s = snelly.getMaterials().loadSurface()
+        s.diffuseAlbedo = [0.8, 0.8, 0.8]
+        s.specAlbedo = [0.0, 0.0, 0.0]
+        s.roughness = 0.3
+        snelly.addSpectrum(FlatSpectrum("flat", "Flat spectrum", 390.0, 750.0))
+        snelly.loadSpectrum("flat")
+
+    def shader(self):
+        return """
+float SDF_SURFACE(vec3 X)
+{
+    float sphere = length(X) - 1.0;
+    float ground = X.y + 1.0;
+    return min(sphere, ground);
+}
+"""
+
+    def getMinLengthScale(self):
+        return 1.0e-4
+
+
+def c1_camera(seed=2):
+    """Camera pose of C1 drawn from `seed`: a point at distance U(4.5, 6) from the look-at point
+    (0.6, 0, 0), azimuth U(0, 2 pi), elevation U(12, 35) degrees."""
+    rs = np.random.RandomState(seed)
+    az = rs.uniform(0.0, 2.0 * math.pi)
+    el = math.radians(rs.uniform(12.0, 35.0))
+    dist = rs.uniform(4.5, 6.0)
+    target = (0.6, 0.0, 0.0)
+    pos = (target[0] + dist * math.cos(el) * math.cos(az), target[1] + dist * math.sin(el),
+           target[2] + dist * math.cos(el) * math.sin(az))
+    return pos, target
+
+
+class DispersiveFractal:
+    """C1: a 5-iteration Menger sponge of side 2 as a dispersive dielectric (Cauchy
+    n = 1.50 + 0.0042 / lambda_um^2, roughness 0.02), a gold sphere of radius 0.7 at (1.8, 0, 0)
+    (the reference's tabulated gold n,k, roughness 0.15) and a ground plane y = -1.2 of diffuse
+    albedo 0.5; a 3-degree sun cone of radiance 20 over a sky of radiance 0.5. 1920x1080,
+    64 spp, maxBounces 8, maxMarchSteps 512."""
+
+    width, height, spp = 1920, 1080, 64
+
+    def __init__(self, width=None, height=None, iterations=5, seed=2):
+        if width:
+            self.width = width
+        if height:
+            self.height = height
+        self.iterations = iterations
+        self.seed = seed
+
+    def init(self, snelly):
+        r = snelly.getRenderer()
+        r.width, r.height = self.width, self.height
+        r.dispersive = True
+        r.interactive = False
+        r.maxBounces = 8
+        r.maxMarchSteps = 512
+        r.skyPower = math.log10(0.5)
+        r.sunPower = math.log10(20.0)
+        r.sunAngularSize = 3.0
+        r.sunLatitude = 45.0
+        r.sunLongitude = 30.0
+        r.envMapTransitionAngle = 135.0
+        cam = snelly.getCamera()
+        cam.fov = 45.0
+        pos, target = c1_camera(self.seed)
+        cam.position.set(*pos)
+        cam.aperture = -math.inf
+        snelly.getControls().target.set(*target)
+        m = snelly.getMaterials()
+        d = Dielectric("C1 Cauchy", "cauchy", [1.50, 0.0042, -2.0])  # CauchyDielectric coefficients
+        m.dielectrics[d.getName()] = d
+        m.loadDielectric(d.getName())
+        d.roughness = 0.02
+        g = m.loadMetal("Gold")
+        g.roughness = 0.15
+        s = m.loadSurface()
+        s.diffuseAlbedo = [0.5, 0.5, 0.5]
+        s.specAlbedo = [0.0, 0.0, 0.0]
+        s.roughness = 0.5
+
+    def shader(self):
+        return f"""
+float box(vec3 p, vec3 halfSize)
+{{
+    vec3 q = abs(p) - halfSize;
+    return min(max(q.x, max(q.y, q.z)), 0.0) + length(max(q, 0.0));
+}}
+
+float SDF_DIELECTRIC(vec3 X)
+{{
+    // Menger sponge of side 2 centred at the origin
+    float d = box(X, vec3(1.0));
+    float s = 1.0;
+    for (int i = 0; i < {self.iterations}; ++i)
+    {{
+        vec3 a = mod(X * s, 2.0) - 1.0;
+        s *= 3.0;
+        vec3 r = abs(1.0 - 3.0 * abs(a));
+        float da = max(r.x, r.y);
+        float db = max(r.y, r.z);
+        float dc = max(r.z, r.x);
+        float c = (min(da, min(db, dc)) - 1.0) / s;
+        d = max(d, c);
+    }}
+    return d;
+}}
+
+float SDF_METAL(vec3 X)
+{{
+    return length(X - vec3(1.8, 0.0, 0.0)) - 0.7;
+}}
+
+float SDF_SURFACE(vec3 X)
+{{
+    return X.y + 1.2;
+}}
+"""
+
+    def getMinLengthScale(self):
+        return 1.0e-4
+
+
+class VolumetricSubsurface:
+    """C2 (surface part): a 12-iteration Mandelbox of scale 2 and minimum radius 0.5 with
+    subsurface scattering (albedo (0.9, 0.6, 0.4), mean free path 0.05, Henyey-Greenstein
+    g = 0.3), sky light and sun; 1024x1024, 128 spp, maxBounces 12."""
+
+    width, height, spp = 1024, 1024, 128
+
+    def __init__(self, width=None, height=None):
+        if width:
+            self.width = width
+        if height:
+            self.height = height
+
+    def init(self, snelly):
+        r = snelly.getRenderer()
+        r.width, r.height = self.width, self.height
+        r.dispersive = True
+        r.interactive = False
+        r.maxBounces = 12
+        r.maxMarchSteps = 256
+        r.maxSSSSteps = 128
+        r.skyPower = math.log10(0.8)
+        r.sunPower = math.log10(8.0)
+        r.sunAngularSize = 4.0
+        r.sunLatitude = 55.0
+        r.sunLongitude = 120.0
+        cam = snelly.getCamera()
+        cam.fov = 45.0
+        cam.position.set(-7.5, 5.0, -6.0)
+        cam.aperture = -math.inf
+        snelly.getControls().target.set(0.0, 0.0, 0.0)
+        s = snelly.getMaterials().loadSurface()
+        s.diffuseAlbedo = [0.8, 0.7, 0.6]
+        s.specAlbedo = [0.1, 0.1, 0.1]
+        s.roughness = 0.2
+        s.subsurface = 1.0
+        s.subsurfaceAlbedoRGB = [0.9, 0.6, 0.4]
+        s.subsurfaceMFP = 0.05
+        s.subsurfaceAnisotropy = 0.3
+
+    def shader(self):
+        return """
+uniform float boxScale;
+uniform float minRadius2;
+
+float SDF_SURFACE(vec3 X)
+{
+    // Mandelbox distance estimate: box fold, sphere fold, scale and translate
+    vec3 z = X;
+    float dr = 1.0;
+    float fixedRadius2 = 1.0;
+    for (int i = 0; i < 12; ++i)
+    {
+        z = clamp(z, -1.0, 1.0) * 2.0 - z;
+        float r2 = dot(z, z);
+        if (r2 < minRadius2) { float t = fixedRadius2 / minRadius2; z *= t; dr *= t; }
+        else if (r2 < fixedRadius2) { float t = fixedRadius2 / r2; z *= t; dr *= t; }
+        z = boxScale * z + X;
+        dr = dr * abs(boxScale) + 1.0;
+    }
+    return length(z) / abs(dr);
+}
+"""
+
+    def syncShader(self, snelly, shader):
+        shader.uniformF("boxScale", 2.0)
+        shader.uniformF("minRadius2", 0.25)
+
+    def getMinLengthScale(self):
+        return 1.0e-4
+
+
+SCENES = {"c0": PlainSphere, "c1": DispersiveFractal, "c2": VolumetricSubsurface}
