@@ -185,8 +185,11 @@ int snelly_compile_check(const char* scene_glsl, const snelly_scene_opts* opts, 
                          size_t* cubin_bytes);
 
 /* GLSL -> C++ translation of a scene string (what snelly_create_scene compiles), for tools that
- * build CPU code from the same source. Writes the C++ text into out (NUL-terminated). */
-int snelly_glsl_to_cpp(const char* glsl, const char* struct_name, char* out, size_t out_cap);
+ * build CPU code from the same source. extra_members: C++ member declarations to add to the
+ * struct (NULL: the scene defaults, i.e. the reference's rand()). Writes the C++ text into out
+ * (NUL-terminated). */
+int snelly_glsl_to_cpp(const char* glsl, const char* struct_name, const char* extra_members, char* out,
+                       size_t out_cap);
 
 #ifdef __cplusplus
 }

@@ -1,0 +1,229 @@
+"""CPU oracle for the spectral path tracer: build per scene, render pixels, seed, compare.
+
+TEST INFRASTRUCTURE. Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg use
+this module. It compiles oracle/pt_oracle.h (a sequential C++ restatement of
+shaders/pathtracer-fragment-shader.glsl) together with one scene into a shared library with
+g++ (-O3, no fast-math, no FMA contraction, OpenMP over pixels).
+
+The host-side steps the reference performs before drawing are restated here as well:
+  * the hook defaults and #defines of Renderer.compileShaders (js/renderer.js:217-316);
+  * the emission-spectrum inverse CDF of Spectrum.inverseCDF (js/spectra.js:28-61) with float32
+    storage and float64 arithmetic, as the reference's Float32Arrays do.
+The GLSL-to-C++ translation itself is the package's translator (snelly_glsl_to_cpp).
+"""
+import ctypes
+import hashlib
+import json
+import os
+import re
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(HERE)
+BUILD = os.path.join(HERE, "_build")
+
+# js/renderer.js:228-263: (substring searched for, default appended when absent)
+HOOK_DEFAULTS = [
+    ("INIT(", "void INIT() {}"),
+    ("SURFACE_DIFFUSE_REFLECTANCE(", "vec3 SURFACE_DIFFUSE_REFLECTANCE(in vec3 C, in vec3 X, in vec3 N, in vec3 V) { return C; }"),
+    ("SURFACE_SPECULAR_REFLECTANCE(", "vec3 SURFACE_SPECULAR_REFLECTANCE(in vec3 C, in vec3 X, in vec3 N, in vec3 V) { return C; }"),
+    ("SURFACE_ROUGHNESS(", "float SURFACE_ROUGHNESS(in float roughness, in vec3 X, in vec3 N) { return roughness; }"),
+    ("SUBSURFACE_ALBEDO(", "vec3 SUBSURFACE_ALBEDO(in vec3 C, in vec3 X, in vec3 N) { return C; }"),
+    ("METAL_SPECULAR_REFLECTANCE(", "vec3 METAL_SPECULAR_REFLECTANCE(in vec3 C, in vec3 X, in vec3 N, in vec3 V) { return C; }"),
+    ("METAL_ROUGHNESS(", "float METAL_ROUGHNESS(in float roughness, in vec3 X, in vec3 N) { return roughness; }"),
+    ("DIELECTRIC_SPECULAR_REFLECTANCE(", "vec3 DIELECTRIC_SPECULAR_REFLECTANCE(in vec3 C, in vec3 X, in vec3 N, in vec3 V) { return C; }"),
+    ("DIELECTRIC_ROUGHNESS(", "float DIELECTRIC_ROUGHNESS(in float roughness, in vec3 X, in vec3 N) { return roughness; }"),
+    ("DIELECTRIC_ABSORPTION(", "vec3 DIELECTRIC_ABSORPTION(vec3 absorption_ui, vec3 X) { return absorption_ui; }"),
+    ("VOLUME_EXTINCTION(", "float VOLUME_EXTINCTION(float extinction_ui, vec3 X) { return extinction_ui; }"),
+    ("VOLUME_EXTINCTION_MAX(", "float VOLUME_EXTINCTION_MAX(float extinction_ui) { return extinction_ui; }"),
+    ("VOLUME_SCATTERING_COLOR(", "vec3 VOLUME_SCATTERING_COLOR(vec3 scattering_color_ui, vec3 X) { return scattering_color_ui; }"),
+    ("VOLUME_ABSORPTION_COLOR(", "vec3 VOLUME_ABSORPTION_COLOR(vec3 absorption_color_ui, vec3 X) { return absorption_color_ui; }"),
+    ("VOLUME_ANISOTROPY(", "float VOLUME_ANISOTROPY(float anisotropy, vec3 X) { return anisotropy; }"),
+    ("VOLUME_EMISSION(", "vec3 VOLUME_EMISSION(vec3 emission, vec3 X) { return emission; }"),
+]
+
+
+def assemble(glsl, opts):
+    """(GLSL with defaults, #define block) as js/renderer.js:217-316 builds them."""
+    s = glsl
+    for needle, body in HOOK_DEFAULTS:
+        if needle not in s:
+            s += "\n " + body + "\n"
+    d = []
+    if "CONSTRUCT_PRIMARY_RAY(" in glsl:
+        d.append("HAS_CUSTOM_CAMERA")
+    for key, name in (("SDF_SURFACE(", "HAS_SURFACE"), ("SDF_METAL(", "HAS_METAL"), ("SDF_DIELECTRIC(", "HAS_DIELECTRIC")):
+        if key in glsl:
+            d.append(name)
+    if opts.has_atmosphere:
+        d.append("HAS_ATMOSPHERE")
+    if opts.has_fog:
+        d.append("HAS_FOG")
+    if "VOLUME_EMISSION(" in glsl:
+        d.append("HAS_VOLUME_EMISSION")
+    d.append("HAS_GEOMETRY")
+    nm = [k for k in ("SURFACE_NORMAL_MAP(", "METAL_NORMAL_MAP(", "DIELECTRIC_NORMAL_MAP(") if k in glsl]
+    if nm:
+        d.append("HAS_NORMALMAP")
+    for k in nm:
+        d.append("HAS_" + k[:-len("_NORMAL_MAP(")] + "_NORMALMAP")
+    if opts.interactive:
+        d.append("INTERACTIVE_MODE")
+    if opts.dispersive:
+        d.append("DISPERSION_ENABLED")
+    if opts.has_sphere_light:
+        d.append("HAS_SPHERE_LIGHT")
+    defs = "".join(f"#define {x}\n" for x in d)
+    defs += (f"#define MAX_MARCH_STEPS {opts.max_march_steps}\n#define MAX_BOUNCES {opts.max_bounces}\n"
+             f"#define MAX_ATMOSPHERE_SCATTERS {opts.max_atmosphere_scatters}\n"
+             f"#define MAX_SAMPLES_PER_FRAME {opts.max_samples_per_frame}\n")
+    return s, defs
+
+
+def inverse_cdf(kind, temperature=6000.0, band=(390.0, 750.0), wavelength=550.0, lmin=390.0, lmax=750.0, ns=1024):
+    """Spectrum.inverseCDF (js/spectra.js:28-61): float64 arithmetic, float32 stores."""
+    if kind == "mono":  # js/spectra.js:76-86
+        w = max(lmin, min(wavelength, lmax))
+        return np.full(4 * ns, np.float32((w - lmin) / (lmax - lmin)), np.float32)
+
+    def spec(l):
+        if kind == "flat":  # js/spectra.js:123-128
+            return 0.0 if (l < band[0] or l > band[1]) else 1.0
+        b = 1.43877737467e7 / (l * temperature)  # js/spectra.js:179-184
+        x = l / 360.0
+        return 1.0 / (x * x * x * x * x * (np.exp(b) - 1.0))
+
+    cdf = np.zeros(ns + 1, np.float32)
+    dl = (lmax - lmin) / ns
+    for n in range(ns):
+        cdf[n + 1] = np.float32(float(cdf[n]) + spec(lmin + dl * n))
+    total = float(cdf[ns])
+    for n in range(ns):
+        cdf[n + 1] = np.float32(float(cdf[n + 1]) / total)
+    cdf[ns] = 1.0
+    icdf = np.zeros(4 * ns, np.float32)
+    idx = 0
+    for n in range(4 * ns):
+        xi = min((n + 1) / (4.0 * ns), 1.0)
+        while float(cdf[idx]) < xi:
+            idx += 1
+        idx = max(1, idx)
+        lo, hi = float(cdf[idx - 1]), float(cdf[idx])
+        icdf[n] = np.float32((idx - 1.0) / ns + (1.0 / ns) * (xi - lo) / (hi - lo))
+    return icdf
+
+
+def _translate(glsl):
+    from snelly_b200 import _native
+    return _native.glsl_to_cpp(glsl, "Scene")
+
+
+def uniform_layout(cpp):
+    """[(name, type, offset, array_len)] from the translated uniform block."""
+    body = re.search(r"struct SceneUniforms \{(.*?)\};", cpp, re.S).group(1)
+    out = []
+    for m in re.finditer(r"(\w+) (\w+)(?:\[(\d+)\])?;\s*// offset (\d+)", body):
+        out.append((m.group(2), m.group(1), int(m.group(4)), int(m.group(3) or 0)))
+    size = int(re.search(r"sizeof\(SceneUniforms\) == (\d+)", cpp).group(1))
+    return out, size
+
+
+def pack_uniforms(cpp, calls):
+    """Uniform block bytes for the recorded shader.uniform* calls ({name: (type, values)})."""
+    layout, size = uniform_layout(cpp)
+    buf = bytearray(size)
+    for name, typ, off, alen in layout:
+        if name not in calls:
+            continue
+        _, vals = calls[name]
+        if typ in ("int",):
+            buf[off:off + 4 * len(vals)] = np.asarray(vals, np.int32).tobytes()
+        else:
+            buf[off:off + 4 * len(vals)] = np.asarray(vals, np.float32).tobytes()
+    return bytes(buf)
+
+
+class OracleLib:
+    """A compiled oracle for one scene string and one set of compile-time options."""
+
+    def __init__(self, glsl, opts, count_ops=False):
+        full, defs = assemble(glsl, opts)
+        cpp = _translate(full)
+        self.cpp = cpp
+        key = hashlib.sha1((defs + cpp + str(count_ops)).encode() + self._sources_digest()).hexdigest()[:16]
+        d = os.path.join(BUILD, key)
+        so = os.path.join(d, "liboracle.so")
+        if not os.path.exists(so):
+            os.makedirs(d, exist_ok=True)
+            with open(os.path.join(d, "scene.inc"), "w") as f:
+                f.write(defs + cpp)
+            cmd = ["g++", "-O3", "-march=native", "-ffp-contract=off", "-fno-fast-math", "-fopenmp", "-std=c++17",
+                   "-shared", "-fPIC", "-w", "-I" + os.path.join(ROOT, "snelly_b200", "csrc"),
+                   "-I" + os.path.join(ROOT, "include"), "-I" + HERE, "-I" + d, '-DSCENE_INC="scene.inc"']
+            if count_ops:
+                cmd.append("-DORACLE_COUNT_OPS")
+            cmd += [os.path.join(HERE, "oracle_main.cpp"), "-o", so + ".tmp"]
+            subprocess.run(cmd, check=True)
+            os.replace(so + ".tmp", so)
+        self.path = so
+        L = ctypes.CDLL(so)
+        vp, i32 = ctypes.c_void_p, ctypes.c_int
+        L.oracle_render.argtypes = [vp, vp, i32, i32, vp, i32, i32, vp, vp, vp, i32]
+        L.oracle_render.restype = i32
+        L.oracle_seed.argtypes = [ctypes.c_uint64, ctypes.c_uint64, vp]
+        L.oracle_rand.argtypes = [vp]
+        L.oracle_rand.restype = ctypes.c_float
+        L.oracle_uniform_block_size.restype = ctypes.c_size_t
+        self.lib = L
+
+    @staticmethod
+    def _sources_digest():
+        h = hashlib.sha1()
+        for f in ("pt_oracle.h", "pt_oracle_bsdf.inc", "pt_oracle_integrator.inc", "oracle_main.cpp", "counted.h"):
+            p = os.path.join(HERE, f)
+            if os.path.exists(p):
+                h.update(open(p, "rb").read())
+        for p in (os.path.join(ROOT, "snelly_b200", "csrc", "glslcompat.h"), os.path.join(ROOT, "include", "snelly_params.h")):
+            h.update(open(p, "rb").read())
+        return h.digest()
+
+    def seed(self, seed, pixels):
+        out = np.empty((len(pixels), 4), np.uint32)
+        for k, p in enumerate(pixels):
+            self.lib.oracle_seed(seed, int(p), out[k].ctypes.data)
+        return out
+
+    def render(self, params, uniforms, width, height, pixels, frames, rng, threads=0):
+        """Render `frames` frames of the listed pixels. Returns (xyz_sum float64 (n,3),
+        running mean float32 (n,4), final rng (n,4))."""
+        pixels = np.ascontiguousarray(pixels, np.int32)
+        n = len(pixels)
+        rng = np.ascontiguousarray(rng, np.uint32).copy()
+        xyz = np.zeros((n, 3), np.float64)
+        mean = np.zeros((n, 4), np.float32)
+        ub = ctypes.create_string_buffer(bytes(uniforms), max(1, len(uniforms)))
+        rc = self.lib.oracle_render(ctypes.byref(params), ub, int(width), int(height), pixels.ctypes.data, n,
+                                    int(frames), rng.ctypes.data, xyz.ctypes.data, mean.ctypes.data, int(threads))
+        assert rc == 0
+        return xyz, mean, rng
+
+
+def host_params(snelly):
+    """SnellyParams of a host-mirror Snelly object with host table pointers filled in for the
+    oracle: the XYZ table and the inverse CDF of the loaded spectrum (restated here)."""
+    from snelly_b200 import api
+    p = snelly.uniform_params()
+    xyz = np.asarray(api.DATA["xyz_table"], np.float32)
+    sp = snelly.spectrumObj
+    if isinstance(sp, api.FlatSpectrum):
+        icdf = inverse_cdf("flat", band=(sp.min, sp.max))
+    elif isinstance(sp, api.MonochromaticSpectrum):
+        icdf = inverse_cdf("mono", wavelength=sp.wavelength)
+    else:
+        icdf = inverse_cdf("blackbody", temperature=sp.skyTemperature)
+    keep = (xyz, icdf)
+    p.xyzTable = xyz.ctypes.data
+    p.icdfTable = icdf.ctypes.data
+    return p, keep

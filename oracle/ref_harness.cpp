@@ -1,0 +1,63 @@
+// ref_harness.cpp - runs the reference's own path tracer fragment shader (translated to C++ by
+// oracle/build_ref.py into ref_shader.inc) once per pixel and frame on the CPU.
+//
+// TEST INFRASTRUCTURE: part of the oracle/_ref build recipe.
+#include <cstdint>
+#include <cstring>
+#include <vector>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+#include "glslcompat.h"
+namespace glsl {
+#include "ref_shader.inc"
+}
+
+extern "C" size_t ref_block_size(void) { return sizeof(glsl::RefShaderUniforms); }
+
+// block: the uniform block (samplers included); off_radiance / off_rng: offsets of the Radiance
+// and RngData sampler records, re-pointed for each pixel at a 1x1 NEAREST texture holding that
+// pixel's state. rng: 4 lanes per listed pixel (in/out); mean: (X, Y, Z, N) per pixel, the
+// shader's own running mean (in/out, N = 0 for a fresh pixel).
+extern "C" int ref_render(const void* block, size_t block_bytes, size_t off_radiance, size_t off_rng, int width,
+                          int height, const int* pixels, int n, int frames, uint32_t* rng, float* mean, int threads) {
+  (void)height;
+  if (block_bytes != sizeof(glsl::RefShaderUniforms)) return -1;
+#ifdef _OPENMP
+  if (threads > 0) omp_set_num_threads(threads);
+#endif
+#pragma omp parallel
+  {
+    std::vector<unsigned char> local(block_bytes + 16);
+    unsigned char* lb = local.data();
+    float rad[4], st[4];
+    glsl::sampler2D radS{rad, 1, 1, 4, 0, 0, 0}, rngS{st, 1, 1, 4, 0, 0, 0};
+#pragma omp for schedule(dynamic, 16)
+    for (int k = 0; k < n; ++k) {
+      std::memcpy(lb, block, block_bytes);
+      std::memcpy(lb + off_radiance, &radS, sizeof radS);
+      std::memcpy(lb + off_rng, &rngS, sizeof rngS);
+      int idx = pixels[k], x = idx % width, y = idx / width;
+      for (int c = 0; c < 4; ++c) {
+        rad[c] = mean[4 * k + c];
+        st[c] = (float)rng[4 * k + c];
+      }
+      for (int f = 0; f < frames; ++f) {
+        glsl::RefShader sh(*reinterpret_cast<const glsl::RefShaderUniforms*>(lb));
+        sh.gl_FragCoord = glsl::vec4(float(x) + 0.5f, float(y) + 0.5f, 0.5f, 1.0f);
+        sh.vTexCoord = glsl::vec2(0.5f, 0.5f);
+        sh.main();
+        for (int c = 0; c < 4; ++c) {
+          rad[c] = sh.gbuf_rad[c];
+          st[c] = sh.gbuf_rng[c];
+        }
+      }
+      for (int c = 0; c < 4; ++c) {
+        mean[4 * k + c] = rad[c];
+        rng[4 * k + c] = (uint32_t)st[c];
+      }
+    }
+  }
+  return 0;
+}

@@ -132,7 +132,7 @@ def lib():
         "snelly_flush_l2": (i32, [vp, sz]),
         "snelly_abi_sizeof": (sz, [i32]),
         "snelly_compile_check": (i32, [ctypes.c_char_p, P(SceneOpts), ctypes.c_char_p, sz, P(sz)]),
-        "snelly_glsl_to_cpp": (i32, [ctypes.c_char_p, ctypes.c_char_p, ctypes.c_char_p, sz]),
+        "snelly_glsl_to_cpp": (i32, [ctypes.c_char_p, ctypes.c_char_p, ctypes.c_char_p, ctypes.c_char_p, sz]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)
@@ -152,11 +152,12 @@ def check(rc):
     return rc
 
 
-def glsl_to_cpp(glsl, struct_name="Scene"):
+def glsl_to_cpp(glsl, struct_name="Scene", extra_members=None):
     """C++ text of a GLSL scene string (the translation snelly_create_scene compiles)."""
     cap = 16 * len(glsl) + (1 << 16)
     buf = ctypes.create_string_buffer(cap)
-    check(lib().snelly_glsl_to_cpp(glsl.encode(), struct_name.encode(), buf, cap))
+    extra = extra_members.encode() if extra_members is not None else None
+    check(lib().snelly_glsl_to_cpp(glsl.encode(), struct_name.encode(), extra, buf, cap))
     return buf.value.decode()
 
 

@@ -150,7 +150,9 @@ const std::set<std::string>& cxx_only_keywords() {
       "bitand", "bitor", "compl", "and_eq", "or_eq", "not_eq", "xor_eq", "goto", "union", "enum",
       "typedef", "extern", "static", "inline", "volatile", "sizeof", "short", "long", "double",
       "unsigned", "wchar_t", "char16_t", "char32_t", "concept", "requires", "final", "override",
-      "gfloat"};
+      "gfloat",
+      // identifiers that are macros of the C/C++ math headers
+      "HUGE_VAL", "HUGE_VALF", "INFINITY", "NAN", "NULL", "EOF"};
   return s;
 }
 

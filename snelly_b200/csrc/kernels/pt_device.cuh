@@ -244,11 +244,14 @@ SD_FN float fresnel_dielectric(float cosi, float eta) {
 // One launch serves up to SNELLY_MAX_BATCH jobs of the same scene module. Scalars are read from
 // the constant bank (broadcast when a warp works on one job); the lane-divergent table lookups
 // (metal n,k) go to the global-memory copy of the same block.
+}  // namespace sdev
 #ifndef SNELLY_MAX_BATCH
 #define SNELLY_MAX_BATCH 32
 #endif
+// Unmangled module globals: the runtime looks them up by name.
 __constant__ SnellyParams c_params[SNELLY_MAX_BATCH];
 __constant__ __align__(16) unsigned char c_uniforms[SNELLY_MAX_BATCH][sizeof(glsl::SceneUniforms)];
+namespace sdev {
 SD_FN const glsl::SceneUniforms& uniforms_of(int job) {
   return *reinterpret_cast<const glsl::SceneUniforms*>(c_uniforms[job]);
 }

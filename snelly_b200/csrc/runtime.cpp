@@ -815,10 +815,11 @@ int snelly_compile_check(const char* glsl, const snelly_scene_opts* opts, char* 
   return rc;
 }
 
-int snelly_glsl_to_cpp(const char* glsl, const char* struct_name, char* out, size_t out_cap) {
+int snelly_glsl_to_cpp(const char* glsl, const char* struct_name, const char* extra_members, char* out,
+                       size_t out_cap) {
   if (!glsl || !out || !out_cap) return fail(SNELLY_EINVAL, "null argument to snelly_glsl_to_cpp");
   GlslTransformResult r;
-  if (!glsl_transform(glsl, struct_name ? struct_name : "Scene", kSceneExtraMembers, &r))
+  if (!glsl_transform(glsl, struct_name ? struct_name : "Scene", extra_members ? extra_members : kSceneExtraMembers, &r))
     return fail(SNELLY_ECOMPILE, "GLSL translation failed: " + r.error);
   if (r.code.size() + 1 > out_cap) return fail(SNELLY_EINVAL, "output buffer too small: need " + std::to_string(r.code.size() + 1));
   memcpy(out, r.code.c_str(), r.code.size() + 1);

@@ -58,9 +58,10 @@ float SDF_SURFACE(vec3 X)
 
 def c1_camera(seed=2):
     """Camera pose of C1 drawn from `seed`: a point at distance U(4.5, 6) from the look-at point
-    (0.6, 0, 0), azimuth U(0, 2 pi), elevation U(12, 35) degrees."""
+    (0.6, 0, 0), azimuth U(60, 120) degrees about +y from the +x axis (so the sponge and the gold
+    sphere are side by side in view), elevation U(12, 35) degrees."""
     rs = np.random.RandomState(seed)
-    az = rs.uniform(0.0, 2.0 * math.pi)
+    az = math.radians(rs.uniform(60.0, 120.0))
     el = math.radians(rs.uniform(12.0, 35.0))
     dist = rs.uniform(4.5, 6.0)
     target = (0.6, 0.0, 0.0)
