@@ -1,0 +1,331 @@
+#!/usr/bin/env python
+"""Benchmark: spectral path samples per second on the 1080p dispersive + metallic fractal workload.
+
+Workload (one step = one progressive frame = one spectral path sample per pixel): a 5-iteration
+Menger sponge (Cauchy dielectric, roughness 0.02), a tabulated-gold sphere and a diffuse ground
+plane under a 3-degree sun and a sky, 1920x1080, maxBounces 8, maxMarchSteps 512, dispersive,
+random-pose camera drawn from seed 2. A full image is 64 frames.
+
+Prints one JSON line (rank 0). `value`: path samples/s with all state resident on the device,
+timed with CUDA events on the renderer's stream around each step, L2 flushed between steps,
+max over ranks. `e2e`: the same through the public scene API with host buffers (per step:
+parameter upload, the frame, and a device-to-host read of the whole mean image into pinned host
+memory), wall clock. `--impl reference` times the reference's own shader built for the host CPU
+(oracle/_ref, else the oracle port) on a bounded pixel sample per step, all host threads.
+
+Multi-GPU: replicas (one job per GPU, no collective): `value` sums all ranks' samples over the
+slowest rank's time.
+"""
+import argparse
+import json
+import os
+import re
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+WORKLOAD = "c1_dispersive_metallic_fractal_1080p"
+METRIC = "spectral path samples/sec at 1080p"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=12)
+    ap.add_argument("--warmup", type=int, default=4)
+    ap.add_argument("--impl", choices=["snelly", "reference"], default="snelly")
+    ap.add_argument("--kernel", choices=["mega", "wavefront"], default=None)
+    ap.add_argument("--width", type=int, default=1920)
+    ap.add_argument("--height", type=int, default=1080)
+    ap.add_argument("--cpu-seconds", type=float, default=12.0, help="budget of the CPU baseline sample")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def workload_scene(args, seed_offset=0):
+    from snelly_b200 import scenes
+    return scenes.DispersiveFractal(args.width, args.height)
+
+
+# ---------------------------------------------------------------------------------------------
+# clocks during the timed region
+# ---------------------------------------------------------------------------------------------
+class ClockSampler:
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.QUERY}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.t.join(timeout=2)
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for l in self.lines:
+            f = [x.strip() for x in l.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax = float(f[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ---------------------------------------------------------------------------------------------
+# CPU side: algorithmic FLOPs per path, CPU baseline
+# ---------------------------------------------------------------------------------------------
+def flops_per_path(host):
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+    return oracle.flops_per_path(host, pixels=1000, frames=2)
+
+
+def cpu_sampler(host, prefer_reference=True):
+    """A callable running `n` random pixels x 1 frame of the workload on all host cores, and its
+    kind ("reference": the reference's shader built for the CPU; "port": the oracle)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+    W, H = host.width, host.height
+    rs = np.random.RandomState(11)
+    ref = None
+    if prefer_reference:
+        try:
+            import build_ref
+            ref = build_ref.ref_for(host, name="bench_c1", prebuilt_only=not os.path.isdir(
+                os.path.join(build_ref.REF_ROOT, "shaders")))
+        except Exception:
+            ref = None
+    lib = oracle.OracleLib(host.sceneObj.shader(), host.scene_opts())
+    if ref is not None:
+        rlib, p, tables, keep = ref
+        calls = host.scene_uniforms()
+
+        def run(n):
+            pix = np.sort(rs.choice(W * H, n, replace=False))
+            rng0 = lib.seed(host.seed, pix)
+            t = time.perf_counter()
+            rlib.render(p, calls, tables, W, H, pix, 1, rng0)
+            return time.perf_counter() - t
+        return run, "reference", (keep,)
+    p, keep = oracle.host_params(host)
+    ub = oracle.pack_uniforms(lib.cpp, host.scene_uniforms())
+
+    def run(n):
+        pix = np.sort(rs.choice(W * H, n, replace=False))
+        rng0 = lib.seed(host.seed, pix)
+        t = time.perf_counter()
+        lib.render(p, ub, W, H, pix, 1, rng0)
+        return time.perf_counter() - t
+    return run, "port", (keep,)
+
+
+def cpu_baseline(host, budget_s):
+    run, kind, keep = cpu_sampler(host)
+    t = run(2000)  # calibration
+    rate = 2000 / max(t, 1e-6)
+    n = int(min(host.width * host.height, max(2000, rate * budget_s)))
+    dt = run(n)
+    return {"value": n / dt, "unit": "path samples/s", "cores": os.cpu_count(), "kind": kind,
+            "sample": f"{n} random pixels of the {host.width}x{host.height} workload, 1 frame each "
+                      f"({dt:.1f} s on {os.cpu_count()} host threads)"}
+
+
+def traffic_from_profiles(kernel_name):
+    """DRAM bytes per launch of the frame kernel from the committed ncu summary, if any."""
+    d = os.path.join(ROOT, "profiles")
+    if not os.path.isdir(d):
+        return None
+    for f in sorted(os.listdir(d)):
+        if kernel_name in f and f.endswith(".md"):
+            m = re.search(r"dram_bytes_per_launch_1080p:\s*([0-9.eE+]+)", open(os.path.join(d, f)).read())
+            if m:
+                return float(m.group(1))
+    return None
+
+
+# ---------------------------------------------------------------------------------------------
+# the arms
+# ---------------------------------------------------------------------------------------------
+def reference_arm(args, rank):
+    if rank != 0:
+        return
+    from snelly_b200.testing import HostSnelly
+    host = HostSnelly(workload_scene(args))
+    run, kind, keep = cpu_sampler(host)
+    t = run(1000)
+    per_step = int(min(host.width * host.height, max(1000, (1000 / max(t, 1e-6)) * args.cpu_seconds / max(1, args.steps))))
+    for _ in range(args.warmup):
+        run(min(per_step, 2000))
+    times = [run(per_step) for _ in range(args.steps)]
+    value = per_step * args.steps / sum(times)
+    sample = f"{per_step} random pixels x 1 frame per step of the {host.width}x{host.height} workload"
+    out = {"impl": "reference", "metric": METRIC, "value": value, "unit": "path samples/s", "n_gpus": args.gpus,
+           "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * sum(times) / args.steps,
+           "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+           "data": "synthetic (procedural SDF scene, seeded camera)",
+           "config": {"workload": WORKLOAD, "width": host.width, "height": host.height, "spp_per_step": 1,
+                      "device": "host CPU"},
+           "cpu_baseline": {"value": value, "unit": "path samples/s", "cores": os.cpu_count(), "kind": kind,
+                            "sample": sample},
+           "e2e": {"value": value, "unit": "path samples/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(out), flush=True)
+
+
+def gpu_arm(args, rank, world, local_rank):
+    import ctypes
+
+    import torch
+    from snelly_b200 import _native as N
+    from snelly_b200 import api
+    torch.cuda.set_device(local_rank)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=120))
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    def allmax(x):
+        if dist is None:
+            return x
+        t = torch.tensor([x], dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    ctx = api.Context(local_rank)
+    peak_tflops, _ = ctx.fp32_peak()
+    s = api.Snelly(workload_scene(args), context=ctx)
+    s.seed = 1 + rank
+    if args.kernel:
+        s.pathtracer.kernelMode = N.KERNEL_WAVEFRONT if args.kernel == "wavefront" else N.KERNEL_MEGA
+    s.render(0)  # compile, allocate, seed
+    W, H = s.width, s.height
+    samples_per_step = W * H * int(round(s.pathtracer.maxSamplesPerFrame))
+    stream = torch.cuda.ExternalStream(ctx.stream())
+    jid = s.job_id()
+    for _ in range(args.warmup):
+        ctx.advance(jid, 1)
+    ctx.sync()
+    torch.cuda.synchronize()
+
+    # ---- device-resident throughput ------------------------------------------------------------
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    clocks = ClockSampler(local_rank)
+    clocks.start()
+    time.sleep(0.3)
+    barrier()
+    torch.cuda.synchronize()
+    launches0 = ctx.launch_count()
+    for k in range(args.steps):
+        ctx.flush_l2(256 << 20)  # evict L2 between timed steps (outside the events)
+        starts[k].record(stream)
+        ctx.advance(jid, 1)
+        ends[k].record(stream)
+    ctx.sync()
+    torch.cuda.synchronize()
+    barrier()
+    launches = ctx.launch_count() - launches0 - args.steps  # minus the flushes
+    clk = clocks.stop()
+    step_ms = [a.elapsed_time(b) for a, b in zip(starts, ends)]
+    total_ms = allmax(sum(step_ms))
+    value = world * samples_per_step * args.steps / (total_ms / 1000.0)
+
+    # ---- end to end through the public API ----------------------------------------------------
+    pinned = torch.empty((H, W, 4), dtype=torch.float32, pin_memory=True).numpy()
+    h2d = ctypes.sizeof(N.SnellyParams) + max(4, len(s.scene_uniforms()) * 4)
+    barrier()
+    t0 = time.perf_counter()
+    for k in range(args.steps):
+        s.render(1)
+        s.readback(out=pinned)
+    e2e_s = allmax(time.perf_counter() - t0)
+    e2e_value = world * samples_per_step * args.steps / e2e_s
+    assert np.isfinite(pinned).all()
+
+    if rank == 0:
+        from snelly_b200.testing import HostSnelly
+        host = HostSnelly(workload_scene(args))
+        fpp, spp_special, counted = flops_per_path(host)
+        per_launch_ms = statistics.mean(step_ms)
+        achieved = fpp * samples_per_step / (per_launch_ms / 1000.0) / 1e12
+        kname = "pt_frame_mega" if (args.kernel or "mega") == "mega" else "pt_wavefront"
+        cpu = None if args.no_cpu_baseline else cpu_baseline(host, args.cpu_seconds)
+        out = {
+            "metric": METRIC, "value": value, "unit": "path samples/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (procedural SDF scene, seeded camera; no dataset)",
+            "config": {"workload": WORKLOAD, "width": W, "height": H, "spp_per_step": 1, "image_spp": 64,
+                       "max_bounces": 8, "max_march_steps": 512, "dispersive": True,
+                       "kernel": args.kernel or "mega", "math": "fast",
+                       "l2": "flushed between timed steps (256 MiB write)", "parallelism": f"replicas x{world}"},
+            "e2e": {"value": e2e_value, "unit": "path samples/s", "h2d_bytes_per_step": h2d,
+                    "d2h_bytes_per_step": W * H * 16},
+            "gpu_launches": int(launches),
+            "roofline": {"bound": "fp32", "achieved": achieved, "peak": peak_tflops, "unit": "TFLOP/s",
+                         "frac": achieved / peak_tflops, "traffic": traffic_from_profiles(kname),
+                         "flops_per_path": fpp, "special_ops_per_path": spp_special,
+                         "peak_source": "measured FFMA microbenchmark in this run (snelly_measure_fp32_peak)"},
+            "clocks": clk,
+            "cpu_baseline": cpu,
+        }
+        print(json.dumps(out), flush=True)
+    if dist is not None:
+        dist.destroy_process_group()
+
+
+def main():
+    args = parse()
+    rank = int(os.environ.get("RANK", 0))
+    world = int(os.environ.get("WORLD_SIZE", 1))
+    local_rank = int(os.environ.get("LOCAL_RANK", 0))
+    if args.impl == "reference":
+        reference_arm(args, rank)
+        return
+    gpu_arm(args, rank, world, local_rank)
+
+
+if __name__ == "__main__":
+    main()

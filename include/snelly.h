@@ -175,6 +175,10 @@ int snelly_measure_fp32_peak(snelly_ctx* ctx, double* tflops, double* ms_out);
 /* Overwrite `bytes` of scratch memory on the context's stream, evicting L2 between timings. */
 int snelly_flush_l2(snelly_ctx* ctx, size_t bytes);
 
+/* The wavelength-sampling table a job uses for `s`: SNELLY_ICDF_SAMPLES (4096) floats, the inverse
+ * CDF of the emission spectrum over 390..750 nm (js/spectra.js:28-61). */
+int snelly_inverse_cdf(const snelly_spectrum* s, float* out);
+
 /* sizeof of the ABI structs, for bindings to check their layouts: 0 SnellyParams,
  * 1 snelly_render_desc, 2 snelly_scene_opts, 3 snelly_uniform, 4 snelly_spectrum. */
 size_t snelly_abi_sizeof(int which);

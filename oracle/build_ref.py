@@ -132,10 +132,17 @@ def shader_source(scene_glsl, opts, diele_model, ncoeffs):
     return src
 
 
+def workload_key(scene_glsl, opts, diele_model, ncoeffs):
+    """Identity of a reference build: scene source + compile-time options + dielectric model."""
+    return hashlib.sha1((scene_glsl + repr(bytes(opts)) + f"{diele_model}/{ncoeffs}").encode()).hexdigest()[:16]
+
+
 class RefLib:
     """The reference shader for one scene + options, compiled for the CPU."""
 
-    def __init__(self, scene_glsl, opts, diele_model, ncoeffs):
+    def __init__(self, scene_glsl, opts, diele_model, ncoeffs, name=None):
+        """Build (needs the reference checkout) into oracle/_ref/<hash>, or, with `name`, into
+        oracle/_ref/<name> together with a key file so that load() finds it without the reference."""
         from snelly_b200 import _native
         src = shader_source(scene_glsl, opts, diele_model, ncoeffs)
         cpp = _native.glsl_to_cpp(src, "RefShader", "  vec4 gl_FragCoord;\n")
@@ -143,17 +150,44 @@ class RefLib:
         h = hashlib.sha1(cpp.encode())
         for f in (os.path.join(HERE, "ref_harness.cpp"), os.path.join(ROOT, "snelly_b200", "csrc", "glslcompat.h")):
             h.update(open(f, "rb").read())
-        d = os.path.join(OUT, h.hexdigest()[:16])
+        d = os.path.join(OUT, name if name else h.hexdigest()[:16])
         so = os.path.join(d, "libref.so")
+        stamp = os.path.join(d, "build.sha1")
+        if name and (not os.path.exists(stamp) or open(stamp).read() != h.hexdigest()):
+            if os.path.exists(so):
+                os.remove(so)
         if not os.path.exists(so):
             os.makedirs(d, exist_ok=True)
             with open(os.path.join(d, "ref_shader.inc"), "w") as f:
                 f.write(cpp)
-            cmd = ["g++", "-O3", "-march=native", "-ffp-contract=off", "-fno-fast-math", "-fopenmp", "-std=c++17",
+            # portable AVX2 target: the library may run on another machine's host CPU
+            cmd = ["g++", "-O3", "-march=x86-64-v3", "-ffp-contract=off", "-fno-fast-math", "-fopenmp", "-std=c++17",
                    "-shared", "-fPIC", "-w", "-I" + os.path.join(ROOT, "snelly_b200", "csrc"), "-I" + d,
                    os.path.join(HERE, "ref_harness.cpp"), "-o", so + ".tmp"]
             subprocess.run(cmd, check=True)
             os.replace(so + ".tmp", so)
+            with open(stamp, "w") as f:
+                f.write(h.hexdigest())
+            with open(os.path.join(d, "workload.key"), "w") as f:
+                f.write(workload_key(scene_glsl, opts, diele_model, ncoeffs))
+        self._load(so, cpp)
+
+    @classmethod
+    def load(cls, name, scene_glsl, opts, diele_model, ncoeffs):
+        """A named prebuilt reference library (no reference checkout needed), or None if absent or
+        built for another workload."""
+        d = os.path.join(OUT, name)
+        so, inc, keyf = (os.path.join(d, f) for f in ("libref.so", "ref_shader.inc", "workload.key"))
+        if not (os.path.exists(so) and os.path.exists(inc) and os.path.exists(keyf)):
+            return None
+        if open(keyf).read() != workload_key(scene_glsl, opts, diele_model, ncoeffs):
+            return None
+        self = cls.__new__(cls)
+        self.cpp = open(inc).read()
+        self._load(so, self.cpp)
+        return self
+
+    def _load(self, so, cpp):
         self.path = so
         L = ctypes.CDLL(so)
         vp, i32, sz = ctypes.c_void_p, ctypes.c_int, ctypes.c_size_t
@@ -216,8 +250,9 @@ class RefLib:
         return mean, rng
 
 
-def ref_for(snelly):
-    """RefLib + table bindings for a host-mirror Snelly object."""
+def ref_for(snelly, name=None, prebuilt_only=False):
+    """RefLib + table bindings for a host-mirror Snelly object. With `name`, use (or create) the
+    named build in oracle/_ref/<name>; prebuilt_only: never build (returns None if absent)."""
     p, keep = O.host_params(snelly)
     xyz, icdf = keep
     metal_n = np.asarray(list(p.metalN), np.float32)
@@ -228,7 +263,12 @@ def ref_for(snelly):
         "iorTex": (metal_n.ctypes.data, 64, 1, 1, 1),
         "kTex": (metal_k.ctypes.data, 64, 1, 1, 1),
     }
-    lib = RefLib(snelly.sceneObj.shader(), snelly.scene_opts(), p.dieleModel, p.dieleNumCoeffs)
+    args = (snelly.sceneObj.shader(), snelly.scene_opts(), p.dieleModel, p.dieleNumCoeffs)
+    lib = RefLib.load(name, *args) if name else None
+    if lib is None:
+        if prebuilt_only or not os.path.isdir(os.path.join(REF_ROOT, "shaders")):
+            return None
+        lib = RefLib(*args, name=name)
     return lib, p, tables, (xyz, icdf, metal_n, metal_k)
 
 

@@ -149,6 +149,7 @@ class OracleLib:
     """A compiled oracle for one scene string and one set of compile-time options."""
 
     def __init__(self, glsl, opts, count_ops=False):
+        self.count_ops = count_ops
         full, defs = assemble(glsl, opts)
         cpp = _translate(full)
         self.cpp = cpp
@@ -176,11 +177,23 @@ class OracleLib:
         L.oracle_rand.argtypes = [vp]
         L.oracle_rand.restype = ctypes.c_float
         L.oracle_uniform_block_size.restype = ctypes.c_size_t
+        L.oracle_counts.argtypes = [vp, vp]
         self.lib = L
+
+    def counts(self):
+        """(FP32 ops, special-function ops) tallied on this thread since the last call."""
+        a, b = ctypes.c_uint64(), ctypes.c_uint64()
+        self.lib.oracle_counts(ctypes.byref(a), ctypes.byref(b))
+        return a.value, b.value
 
     @staticmethod
     def _sources_digest():
         h = hashlib.sha1()
+        try:  # builds use -march=native: key them by the host CPU as well
+            flags = [l for l in open("/proc/cpuinfo") if l.startswith(("flags", "model name"))][:2]
+            h.update("".join(flags).encode())
+        except OSError:
+            pass
         for f in ("pt_oracle.h", "pt_oracle_bsdf.inc", "pt_oracle_integrator.inc", "oracle_main.cpp", "counted.h"):
             p = os.path.join(HERE, f)
             if os.path.exists(p):
@@ -227,3 +240,19 @@ def host_params(snelly):
     p.xyzTable = xyz.ctypes.data
     p.icdfTable = icdf.ctypes.data
     return p, keep
+
+
+def flops_per_path(snelly, pixels=2000, frames=2, seed=5):
+    """Algorithmic FP32 operations per path sample of a workload, counted by the oracle's
+    counting build on a fixed random subset of its pixels (single thread). Returns
+    (flops per path sample, special ops per path sample, samples counted)."""
+    lib = OracleLib(snelly.sceneObj.shader(), snelly.scene_opts(), count_ops=True)
+    n = snelly.width * snelly.height
+    pix = np.sort(np.random.RandomState(seed).choice(n, min(pixels, n), replace=False))
+    p, keep = host_params(snelly)
+    ub = pack_uniforms(lib.cpp, snelly.scene_uniforms())
+    lib.counts()
+    lib.render(p, ub, snelly.width, snelly.height, pix, frames, lib.seed(snelly.seed, pix), threads=1)
+    f, sp = lib.counts()
+    samples = len(pix) * frames * snelly.scene_opts().max_samples_per_frame
+    return f / samples, sp / samples, samples

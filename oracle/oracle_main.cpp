@@ -8,10 +8,10 @@
 #include <omp.h>
 #endif
 
-#include "glslcompat.h"
 #ifdef ORACLE_COUNT_OPS
-#include "counted.h"
+#include "counted.h"  // must precede glslcompat.h: it supplies gfloat
 #endif
+#include "glslcompat.h"
 namespace glsl {
 #include SCENE_INC
 }
@@ -59,6 +59,18 @@ float oracle_rand(uint32_t* st) {
 }
 
 size_t oracle_uniform_block_size(void) { return sizeof(glsl::SceneUniforms); }
+
+// Operation tallies of the calling thread (counting builds; zero otherwise).
+void oracle_counts(uint64_t* flops, uint64_t* special) {
+#ifdef ORACLE_COUNT_OPS
+  *flops = glsl::op_counts().flops;
+  *special = glsl::op_counts().special;
+  glsl::op_counts() = glsl::OpCounts{0, 0};
+#else
+  *flops = 0;
+  *special = 0;
+#endif
+}
 
 // Render `frames` frames for the n pixels listed in `pixels` (indices y*width + x, row 0 at the
 // bottom). rng: 4 lanes per listed pixel, in/out. xyz_sum: 3 doubles per listed pixel, the sum of

@@ -131,6 +131,7 @@ def lib():
         "snelly_measure_fp32_peak": (i32, [vp, P(ctypes.c_double), P(ctypes.c_double)]),
         "snelly_flush_l2": (i32, [vp, sz]),
         "snelly_abi_sizeof": (sz, [i32]),
+        "snelly_inverse_cdf": (i32, [P(Spectrum), vp]),
         "snelly_compile_check": (i32, [ctypes.c_char_p, P(SceneOpts), ctypes.c_char_p, sz, P(sz)]),
         "snelly_glsl_to_cpp": (i32, [ctypes.c_char_p, ctypes.c_char_p, ctypes.c_char_p, ctypes.c_char_p, sz]),
     }

@@ -422,6 +422,7 @@ class Snelly:
         self._scene_key = None
         self._job = None
         self.seed = 1
+        self.fp64 = False  # also accumulate in FP64 (precision study)
         self.initScene()
 
     # js/snelly.js:209-291
@@ -572,7 +573,7 @@ class Snelly:
         d.seed = int(self.seed)
         d.params = self.uniform_params()
         d.spectrum = self.spectrumObj.native()
-        d.accum_fp64 = 0
+        d.accum_fp64 = 1 if getattr(self, "fp64", False) else 0
         return d
 
     # -- progressive rendering ---------------------------------------------------------------------
@@ -600,12 +601,16 @@ class Snelly:
         if hasattr(self.sceneObj, "postframeCallback"):
             self.sceneObj.postframeCallback(self, None)
 
-    def readback(self):
+    def readback(self, out=None):
         """(H, W, 4) float32 array: mean X, Y, Z and sample count; row 0 is the bottom row."""
-        return self._ctx.readback(self._job, self.width, self.height)
+        return self._ctx.readback(self._job, self.width, self.height, out=out)
 
     def job_id(self):
         return self._job
+
+    def readback_state(self):
+        """(rng (n,4) uint32, Kahan sums (n,4), compensations (n,4), FP64 sums (n,4) or None)."""
+        return self._ctx.readback_state(self._job, self.width, self.height, fp64=getattr(self, "fp64", False))
 
 
 # ---------------------------------------------------------------------------------------------

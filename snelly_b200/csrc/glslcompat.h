@@ -129,6 +129,32 @@ struct sw4 {
   template <class T> GLSL_FN sw4& operator/=(const T& t);
 };
 
+// Single components. With a counting scalar (which has constructors and so cannot live in an
+// anonymous struct) each component is a one-element view convertible to a reference to its
+// scalar; with float they are plain struct members.
+template <int N, int A>
+struct sw1 {
+  gfloat d[N];
+  GLSL_FN operator gfloat&() { return d[A]; }
+  GLSL_FN operator const gfloat&() const { return d[A]; }
+  GLSL_FN sw1& operator=(gfloat v) { d[A] = v; return *this; }
+  GLSL_FN sw1& operator=(const sw1& o) { d[A] = o.d[A]; return *this; }
+  GLSL_FN sw1& operator+=(gfloat v) { d[A] = d[A] + v; return *this; }
+  GLSL_FN sw1& operator-=(gfloat v) { d[A] = d[A] - v; return *this; }
+  GLSL_FN sw1& operator*=(gfloat v) { d[A] = d[A] * v; return *this; }
+  GLSL_FN sw1& operator/=(gfloat v) { d[A] = d[A] / v; return *this; }
+};
+#ifdef GLSL_SCALAR_DEFINED
+#define GLSL_COMPONENTS2 sw1<2, 0> x, r, s; sw1<2, 1> y, g, t;
+#define GLSL_COMPONENTS3 sw1<3, 0> x, r, s; sw1<3, 1> y, g, t; sw1<3, 2> z, b, p;
+#define GLSL_COMPONENTS4 sw1<4, 0> x, r, s; sw1<4, 1> y, g, t; sw1<4, 2> z, b, p; sw1<4, 3> w, a, q;
+#else
+#define GLSL_COMPONENTS2 struct { gfloat x, y; }; struct { gfloat r, g; }; struct { gfloat s, t; };
+#define GLSL_COMPONENTS3 struct { gfloat x, y, z; }; struct { gfloat r, g, b; }; struct { gfloat s, t, p; };
+#define GLSL_COMPONENTS4 \
+  struct { gfloat x, y, z, w; }; struct { gfloat r, g, b, a; }; struct { gfloat s, t, p, q; };
+#endif
+
 #if defined(__GNUC__) && !defined(__CUDACC_RTC__)
 #pragma GCC diagnostic push
 #pragma GCC diagnostic ignored "-Wpedantic"
@@ -137,9 +163,7 @@ struct sw4 {
 struct vec2 {
   union {
     gfloat d[2];
-    struct { gfloat x, y; };
-    struct { gfloat r, g; };
-    struct { gfloat s, t; };
+    GLSL_COMPONENTS2
 #define GLSL_SWIZZLE_STORAGE 2
 #include "glsl_swizzles.inc"
 #undef GLSL_SWIZZLE_STORAGE
@@ -166,9 +190,7 @@ struct vec2 {
 struct vec3 {
   union {
     gfloat d[3];
-    struct { gfloat x, y, z; };
-    struct { gfloat r, g, b; };
-    struct { gfloat s, t, p; };
+    GLSL_COMPONENTS3
 #define GLSL_SWIZZLE_STORAGE 3
 #include "glsl_swizzles.inc"
 #undef GLSL_SWIZZLE_STORAGE
@@ -196,9 +218,7 @@ struct vec3 {
 struct vec4 {
   union {
     gfloat d[4];
-    struct { gfloat x, y, z, w; };
-    struct { gfloat r, g, b, a; };
-    struct { gfloat s, t, p, q; };
+    GLSL_COMPONENTS4
 #define GLSL_SWIZZLE_STORAGE 4
 #include "glsl_swizzles.inc"
 #undef GLSL_SWIZZLE_STORAGE

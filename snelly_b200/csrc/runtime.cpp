@@ -780,6 +780,13 @@ int snelly_sync(snelly_ctx* ctx) {
   return SNELLY_OK;
 }
 
+int snelly_inverse_cdf(const snelly_spectrum* s, float* out) {
+  if (!s || !out) return fail(SNELLY_EINVAL, "null argument to snelly_inverse_cdf");
+  std::vector<float> v = inverse_cdf(*s);
+  memcpy(out, v.data(), v.size() * sizeof(float));
+  return SNELLY_OK;
+}
+
 size_t snelly_abi_sizeof(int which) {
   switch (which) {
     case 0: return sizeof(SnellyParams);

@@ -20,6 +20,12 @@ class PlainSphere:
 
     width, height, spp = 256, 256, 16
 
+    def __init__(self, width=None, height=None):
+        if width:
+            self.width = width
+        if height:
+            self.height = height
+
     def init(self, snelly):
         r = snelly.getRenderer()
         r.width, r.height = self.width, self.height
@@ -79,18 +85,19 @@ class DispersiveFractal:
 
     width, height, spp = 1920, 1080, 64
 
-    def __init__(self, width=None, height=None, iterations=5, seed=2):
+    def __init__(self, width=None, height=None, iterations=5, seed=2, dispersive=True):
         if width:
             self.width = width
         if height:
             self.height = height
         self.iterations = iterations
         self.seed = seed
+        self.dispersive = dispersive
 
     def init(self, snelly):
         r = snelly.getRenderer()
         r.width, r.height = self.width, self.height
-        r.dispersive = True
+        r.dispersive = self.dispersive
         r.interactive = False
         r.maxBounces = 8
         r.maxMarchSteps = 512
@@ -232,4 +239,159 @@ float SDF_SURFACE(vec3 X)
         return 1.0e-4
 
 
-SCENES = {"c0": PlainSphere, "c1": DispersiveFractal, "c2": VolumetricSubsurface}
+class AtmosphereLights:
+    """Coverage scene: homogeneous atmosphere with multiple scattering, fake fog, sphere light,
+    sun and sky over a metal sphere, a glass box with absorption and a diffuse ground (RGB mode,
+    thin-lens camera). Exercises PT:971-1457 and the sphere-light paths."""
+
+    width, height, spp = 64, 48, 4
+
+    def __init__(self, width=None, height=None, dispersive=False):
+        if width:
+            self.width = width
+        if height:
+            self.height = height
+        self.dispersive = dispersive
+
+    def init(self, snelly):
+        r = snelly.getRenderer()
+        r.width, r.height = self.width, self.height
+        r.dispersive = self.dispersive
+        r.interactive = False
+        r.maxBounces = 5
+        r.maxAtmosphereScatters = 3
+        r.maxMarchSteps = 200
+        r.skyPower = math.log10(0.7)
+        r.sunPower = math.log10(5.0)
+        r.sunAngularSize = 6.0
+        r.sunLatitude = 35.0
+        r.sunLongitude = 60.0
+        r.sphereLightPower = math.log10(40.0)
+        r.sphereLightRadius = 0.3
+        r.sphereLightPosition = [-1.2, 1.6, 0.6]
+        r.sphereLightColor = [1.0, 0.8, 0.6]
+        r.envMapTransitionAngle = 60.0
+        r.skyTintUp = [0.6, 0.7, 1.0]
+        r.skyTintDown = [0.9, 0.8, 0.6]
+        cam = snelly.getCamera()
+        cam.fov = 50.0
+        cam.position.set(0.3, 1.4, 4.5)
+        cam.aperture = -4.0
+        cam.focalDistance = math.log10(4.3)
+        snelly.getControls().target.set(0.0, 0.2, 0.0)
+        m = snelly.getMaterials()
+        m.loadMetal("Copper").roughness = 0.08
+        d = m.loadDielectric("Glass (BK7)")
+        d.roughness = 0.05
+        d.absorptionColor = [0.6, 0.9, 0.8]
+        d.absorptionScale = 2.0
+        s = m.loadSurface()
+        s.diffuseAlbedo = [0.7, 0.65, 0.6]
+        s.specAlbedo = [0.3, 0.3, 0.3]
+        s.roughness = 0.25
+        v = m.loadVolume()
+        v.scatteringColor = [0.35, 0.4, 0.5]
+        v.absorptionColor = [0.05, 0.05, 0.08]
+        v.lof10_mfp = 0.6
+        v.anisotropy = 0.3
+        v.atmosphereMinY = -1.0
+        v.atmosphereMaxY = 3.0
+        v.fogEnable = True
+        v.fogMFP = 1.0
+        v.fogMaxOpticalDepth = 0.5
+
+    def shader(self):
+        return """
+float SDF_METAL(vec3 X) { return length(X - vec3(0.9, 0.0, 0.0)) - 0.6; }
+float SDF_DIELECTRIC(vec3 X)
+{
+    vec3 q = abs(X - vec3(-0.8, 0.0, 0.2)) - vec3(0.45, 0.6, 0.45);
+    return min(max(q.x, max(q.y, q.z)), 0.0) + length(max(q, 0.0)) - 0.05;
+}
+float SDF_SURFACE(vec3 X) { return X.y + 0.6; }
+"""
+
+
+class HooksAndMaps:
+    """Coverage scene: every material hook of the scene API (diffuse / specular / roughness /
+    subsurface albedo hooks, metal and dielectric hooks, normal maps on all three materials),
+    INIT() state and scene uniforms, a custom primary-ray hook using rand(), a monochromatic
+    spectrum (dispersive mode)."""
+
+    width, height, spp = 48, 48, 4
+
+    def __init__(self, width=None, height=None):
+        if width:
+            self.width = width
+        if height:
+            self.height = height
+
+    def init(self, snelly):
+        from .api import MonochromaticSpectrum
+        r = snelly.getRenderer()
+        r.width, r.height = self.width, self.height
+        r.dispersive = True
+        r.interactive = False
+        r.maxBounces = 4
+        r.maxMarchSteps = 160
+        r.skyPower = 0.0
+        r.sunPower = math.log10(3.0)
+        r.sunLatitude = 60.0
+        cam = snelly.getCamera()
+        cam.fov = 40.0
+        cam.position.set(0.0, 1.0, 4.0)
+        snelly.getControls().target.set(0.0, 0.0, 0.0)
+        m = snelly.getMaterials()
+        m.loadMetal("Silver").roughness = 0.1
+        m.loadDielectric("Water").roughness = 0.02
+        s = m.loadSurface()
+        s.diffuseAlbedo = [0.8, 0.3, 0.2]
+        s.specAlbedo = [0.2, 0.2, 0.2]
+        s.roughness = 0.3
+        s.subsurface = 0.5
+        s.subsurfaceMFP = 0.1
+        s.subsurfaceAlbedoRGB = [0.8, 0.8, 0.7]
+        snelly.addSpectrum(MonochromaticSpectrum("mono", "550 nm", 550.0))
+        snelly.loadSpectrum("mono")
+
+    def shader(self):
+        return """
+uniform float ripple;
+uniform vec3 tint;
+mat2 spin;
+void INIT() { float a = 0.3 * ripple; spin = mat2(cos(a), sin(a), -sin(a), cos(a)); }
+float SDF_SURFACE(vec3 X) { return min(X.y + 1.0, length(X - vec3(-1.1, -0.4, 0.0)) - 0.6); }
+float SDF_METAL(vec3 X) { vec3 p = X - vec3(1.1, -0.3, 0.0); p.xz = spin * p.xz; return length(max(abs(p) - vec3(0.4), 0.0)) - 0.1; }
+float SDF_DIELECTRIC(vec3 X) { return length(X - vec3(0.0, -0.3, 0.3)) - 0.5; }
+vec3 SURFACE_DIFFUSE_REFLECTANCE(in vec3 C, in vec3 X, in vec3 N, in vec3 V)
+{
+    float c = mod(floor(2.0*X.x) + floor(2.0*X.z), 2.0);
+    return mix(C, tint, c);
+}
+vec3 SURFACE_SPECULAR_REFLECTANCE(in vec3 C, in vec3 X, in vec3 N, in vec3 V) { return C * (0.5 + 0.5*abs(N.y)); }
+float SURFACE_ROUGHNESS(in float roughness, in vec3 X, in vec3 N) { return roughness * (1.0 + 0.5*sin(3.0*X.x)); }
+vec3 SUBSURFACE_ALBEDO(in vec3 C, in vec3 X, in vec3 N) { return C.zyx; }
+vec3 METAL_SPECULAR_REFLECTANCE(in vec3 C, in vec3 X, in vec3 N, in vec3 V) { return vec3(1.0, 0.9, 0.8) * C; }
+float METAL_ROUGHNESS(in float roughness, in vec3 X, in vec3 N) { return roughness + 0.05*fract(X.y*3.0); }
+vec3 DIELECTRIC_SPECULAR_REFLECTANCE(in vec3 C, in vec3 X, in vec3 N, in vec3 V) { return vec3(0.95); }
+float DIELECTRIC_ROUGHNESS(in float roughness, in vec3 X, in vec3 N) { return roughness; }
+vec3 DIELECTRIC_ABSORPTION(vec3 absorption_ui, vec3 X) { return absorption_ui + vec3(0.2, 0.05, 0.0); }
+vec3 SURFACE_NORMAL_MAP(in vec3 X, in vec3 N) { return vec3(0.1*sin(8.0*X.x), 0.1*cos(8.0*X.z), 1.0); }
+vec3 METAL_NORMAL_MAP(in vec3 X, in vec3 N) { return vec3(0.05*sin(20.0*X.y), 0.0, 1.0); }
+vec3 DIELECTRIC_NORMAL_MAP(in vec3 X, in vec3 N) { return vec3(0.0, 0.08*sin(12.0*X.x), 1.0); }
+void CONSTRUCT_PRIMARY_RAY(in vec2 pixel, inout vec4 rnd, inout vec3 primaryStart, inout vec3 primaryDir)
+{
+    vec2 ndc = -1.0 + 2.0*(pixel/vec2(48.0, 48.0));
+    float jitter = 0.002 * (rand(rnd) - 0.5);
+    primaryStart = vec3(0.0, 1.0, 4.0);
+    primaryDir = normalize(vec3(0.36*ndc.x + jitter, 0.36*ndc.y - 0.25, -1.0));
+}
+"""
+
+    def syncShader(self, snelly, shader):
+        shader.uniformF("ripple", 1.5)
+        shader.uniform3Fv("tint", [0.1, 0.6, 0.2])
+
+
+SCENES = {"c0": PlainSphere, "c1": DispersiveFractal, "c2": VolumetricSubsurface, "atmosphere": AtmosphereLights,
+          "hooks": HooksAndMaps}

@@ -1,0 +1,69 @@
+"""Generate the golden fixtures of tests/golden/ from the reference itself.
+
+Run in a checkout that has the reference at /root/reference (or $SNELLY_REFERENCE):
+    python tests/golden/make_golden.py
+
+* pt_<case>.npz: the reference's own path tracer shader (shaders/pathtracer-fragment-shader.glsl,
+  built for the CPU by oracle/build_ref.py) rendering a small image of one of the package's
+  scenes: inputs (scene case, size, frames, seed, the initial per-pixel RNG lanes) and outputs
+  (per-pixel running mean X, Y, Z, N after `frames` frames, final RNG lanes).
+* cie_csv.npy: the CIE XYZ table recomputed from scripts/color/lin2012xyz2e_fine_7sf.csv as
+  scripts/color/cie.py does (linear interpolation to 1024 samples over 390..750 nm, both ends
+  included), to pin the table in snelly_b200/data/materials.json.
+"""
+import csv
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, ROOT)
+sys.path.insert(0, os.path.join(ROOT, "oracle"))
+
+from snelly_b200 import scenes  # noqa: E402
+from snelly_b200.testing import HostSnelly  # noqa: E402
+import build_ref  # noqa: E402
+import oracle  # noqa: E402
+
+CASES = {
+    "c0": (lambda: scenes.PlainSphere(64, 64), 8),
+    "c1": (lambda: scenes.DispersiveFractal(64, 36), 4),
+    "c1_rgb": (lambda: scenes.DispersiveFractal(48, 27, dispersive=False), 3),
+    "c2": (lambda: scenes.VolumetricSubsurface(32, 32), 2),
+    "atmosphere": (lambda: scenes.AtmosphereLights(64, 48), 3),
+    "atmosphere_disp": (lambda: scenes.AtmosphereLights(32, 24, dispersive=True), 2),
+    "hooks": (lambda: scenes.HooksAndMaps(48, 48), 3),
+}
+SEED = 1
+
+
+def make_pt(name):
+    factory, frames = CASES[name]
+    h = HostSnelly(factory())
+    ref, p, tables, keep = build_ref.ref_for(h)
+    lib = oracle.OracleLib(h.sceneObj.shader(), h.scene_opts())
+    pix = np.arange(h.width * h.height)
+    rng0 = lib.seed(SEED, pix)
+    mean, rng = ref.render(p, h.scene_uniforms(), tables, h.width, h.height, pix, frames, rng0)
+    np.savez_compressed(os.path.join(HERE, f"pt_{name}.npz"), case=name, width=h.width, height=h.height,
+                        frames=frames, seed=SEED, rng0=rng0, mean=mean, rng=rng)
+    print(f"pt_{name}: {h.width}x{h.height}, {frames} frames, mean XYZ {mean[:, :3].mean(0)}")
+
+
+def make_cie():
+    path = os.path.join(build_ref.REF_ROOT, "scripts", "color", "lin2012xyz2e_fine_7sf.csv")
+    rows = [r for r in csv.reader(open(path))]
+    lam = np.array([float(r[0]) for r in rows])
+    xyz = np.array([[float(r[1]), float(r[2]), float(r[3])] for r in rows])
+    l_res = 390.0 + (750.0 - 390.0) / 1023.0 * np.arange(1024)
+    out = np.stack([np.interp(l_res, lam, xyz[:, c]) for c in range(3)], 1)
+    np.save(os.path.join(HERE, "cie_csv.npy"), out)
+    print("cie_csv: 1024 x 3")
+
+
+if __name__ == "__main__":
+    make_cie()
+    for n in CASES:
+        make_pt(n)

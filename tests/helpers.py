@@ -1,0 +1,58 @@
+"""Shared test helpers: golden fixtures, oracle builds, GPU renders."""
+import os
+
+import numpy as np
+
+from snelly_b200 import scenes
+from snelly_b200.testing import HostSnelly
+
+GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+
+CASES = {
+    "c0": lambda: scenes.PlainSphere(64, 64),
+    "c1": lambda: scenes.DispersiveFractal(64, 36),
+    "c1_rgb": lambda: scenes.DispersiveFractal(48, 27, dispersive=False),
+    "c2": lambda: scenes.VolumetricSubsurface(32, 32),
+    "atmosphere": lambda: scenes.AtmosphereLights(64, 48),
+    "atmosphere_disp": lambda: scenes.AtmosphereLights(32, 24, dispersive=True),
+    "hooks": lambda: scenes.HooksAndMaps(48, 48),
+}
+
+
+def golden(name):
+    return dict(np.load(os.path.join(GOLDEN, f"pt_{name}.npz")))
+
+
+def oracle_for(host):
+    import oracle
+    return oracle.OracleLib(host.sceneObj.shader(), host.scene_opts())
+
+
+def oracle_render(host, pixels, frames, rng0=None, threads=0):
+    import oracle
+    lib = oracle_for(host)
+    if rng0 is None:
+        rng0 = lib.seed(host.seed, pixels)
+    p, keep = oracle.host_params(host)
+    ub = oracle.pack_uniforms(lib.cpp, host.scene_uniforms())
+    return lib.render(p, ub, host.width, host.height, pixels, frames, rng0, threads)
+
+
+def gpu_render(ctx, scene, frames, seed=1, math_mode=None, kernel_mode=None, fp64=False):
+    """Render `frames` frames of `scene` through the scene API on the GPU; returns the Snelly
+    object and its (H, W, 4) mean image."""
+    from snelly_b200 import api
+    from snelly_b200 import _native as N
+    s = api.Snelly(scene, context=ctx)
+    s.seed = seed
+    if math_mode is not None:
+        s.pathtracer.mathMode = math_mode
+    if kernel_mode is not None:
+        s.pathtracer.kernelMode = kernel_mode
+    s.fp64 = fp64
+    s.render(frames)
+    return s, s.readback()
+
+
+def host(name):
+    return HostSnelly(CASES[name]())

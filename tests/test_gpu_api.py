@@ -1,0 +1,93 @@
+"""C ABI behaviour on the GPU: progressive frames, checkpoint/resume, errors and budgets."""
+import ctypes
+
+import numpy as np
+import pytest
+
+from helpers import gpu_render
+from snelly_b200 import _native as N
+from snelly_b200 import api, scenes
+
+pytestmark = pytest.mark.gpu
+
+
+def test_progressive_frames_equal_single_render(gpu_ctx):
+    a, img_a = gpu_render(gpu_ctx, scenes.PlainSphere(64, 64), 8)
+    b = api.Snelly(scenes.PlainSphere(64, 64), context=gpu_ctx)
+    b.render(3)
+    b.render(5)
+    img_b = b.readback()
+    np.testing.assert_array_equal(img_a, img_b)
+
+
+def test_checkpoint_resume_is_exact(gpu_ctx):
+    a, _ = gpu_render(gpu_ctx, scenes.DispersiveFractal(64, 36), 6)
+    full = a.readback()
+    b, _ = gpu_render(gpu_ctx, scenes.DispersiveFractal(64, 36), 3)
+    rng, acc, comp, _ = b.readback_state()
+    sid = b.compileShaders()
+    desc = b.render_desc(3)
+    jid = gpu_ctx.restore(sid, desc, rng, acc, comp)
+    resumed = gpu_ctx.readback(jid, 64, 36)
+    np.testing.assert_array_equal(full, resumed)
+
+
+def test_budget_refusal_leaves_context_usable():
+    ctx = api.Context(0, hbm_budget=64 << 20)
+    s = api.Snelly(scenes.PlainSphere(2048, 2048), context=ctx)
+    with pytest.raises(N.SnellyError) as e:
+        s.render(1)
+    assert e.value.code == -3  # ENOMEM_BUDGET
+    s2 = api.Snelly(scenes.PlainSphere(32, 32), context=ctx)
+    s2.render(2)
+    assert np.isfinite(s2.readback()).all()
+    ctx.close()
+
+
+def test_errors_are_reported(gpu_ctx):
+    L = N.lib()
+    with pytest.raises(N.SnellyError) as e:
+        gpu_ctx.readback(987654, 4, 4)
+    assert e.value.code == -7
+    opts = N.SceneOpts(3, 64, 1, 1, 0, 0, 0, 0, 0, 0, 1)
+    with pytest.raises(N.SnellyError) as e:
+        gpu_ctx.create_scene("float SDF_SURFACE(vec3 X) { return length(X) - ; }", opts)
+    assert e.value.code == -2 and "error" in str(e.value)
+    with pytest.raises(N.SnellyError) as e:
+        gpu_ctx.create_scene("float f(vec3 X) { return 1.0; }", opts)
+    assert e.value.code == -2
+    sid = gpu_ctx.create_scene("uniform float R; float SDF_SURFACE(vec3 X) { return length(X) - R; }", opts)
+    with pytest.raises(N.SnellyError) as e:
+        gpu_ctx.set_uniforms(sid, {"nope": (N.U_FLOAT, [1.0])})
+    assert e.value.code == -7
+    with pytest.raises(N.SnellyError) as e:
+        gpu_ctx.set_uniforms(sid, {"R": (N.U_VEC3, [1.0, 2.0, 3.0])})
+    assert e.value.code == -1
+    d = N.RenderDesc()
+    d.width, d.height, d.frames = 0, 4, 1
+    with pytest.raises(N.SnellyError) as e:
+        gpu_ctx.render(sid, d)
+    assert e.value.code == -1
+
+
+def test_cancel_and_poll(gpu_ctx):
+    s = api.Snelly(scenes.PlainSphere(128, 128), context=gpu_ctx)
+    s.render(4)
+    jid = s.job_id()
+    try:
+        gpu_ctx.readback(jid, 128, 128, poll=True)
+    except N.SnellyError as e:
+        assert e.code == -4  # EBUSY while frames run
+    gpu_ctx.sync()
+    img = gpu_ctx.readback(jid, 128, 128, poll=True)
+    assert (img[..., 3] == 4).all()
+    gpu_ctx.cancel(jid)
+    with pytest.raises(N.SnellyError) as e:
+        gpu_ctx.readback(jid, 128, 128)
+    assert e.value.code == -8
+
+
+def test_native_kernels_ran(gpu_ctx):
+    before = gpu_ctx.launch_count()
+    gpu_render(gpu_ctx, scenes.PlainSphere(32, 32), 3)
+    assert gpu_ctx.launch_count() >= before + 4  # seed + 3 frames + resolve
