@@ -148,6 +148,13 @@ int snelly_render(snelly_ctx* ctx, uint64_t scene_id, const snelly_render_desc* 
 /* Enqueue more frames on an existing job (progressive accumulation). */
 int snelly_advance(snelly_ctx* ctx, uint64_t job_id, int frames);
 
+/* Enqueue frames[i] more frames on each job_ids[i], batched: for every frame, the jobs that share
+ * a scene module run in one launch (up to 32 jobs per launch, each with its own parameter slot),
+ * and the launches of different modules go to separate streams so that they overlap on the GPU.
+ * Jobs keep their per-pixel RNG streams, so each job's image is the same as when rendered alone.
+ * Path-per-thread integrator. */
+int snelly_advance_batch(snelly_ctx* ctx, const uint64_t* job_ids, const int* frames, size_t n);
+
 #define SNELLY_READ_WAIT 1 /* block until the job's enqueued frames are done */
 #define SNELLY_READ_POLL 2 /* return SNELLY_EBUSY if not done */
 /* Mean XYZ and sample count per pixel: width*height*4 floats (X, Y, Z, N). */
@@ -168,6 +175,11 @@ int snelly_sync(snelly_ctx* ctx);
 void* snelly_stream(snelly_ctx* ctx);
 /* Kernel launches issued by this context so far (instrumentation). */
 uint64_t snelly_launch_count(snelly_ctx* ctx);
+
+/* Statistics of a job's image after the frames enqueued so far (waits for them): out5 = the sums
+ * over pixels of the per-pixel mean X, Y, Z and of Y^2, and the total sample count. Used by the
+ * serving loop's noise criterion. Deterministic (fixed-order two-pass reduction in FP64). */
+int snelly_image_stats(snelly_ctx* ctx, uint64_t job_id, double* out5);
 
 /* Measured FP32 FMA throughput of this GPU (TFLOP/s), from an FMA-chain microbenchmark; the
  * roofline denominator of the path tracer. ms_out: best kernel time of 5 runs. */

@@ -28,7 +28,8 @@ typedef struct SnellyParams {
   float camFovy, camAspect, camAperture, camFocalDistance;
   // path-tracing settings (js/renderer.js:547-559)
   float filterRadius, radianceClamp, skipProbability, shadowStrength;
-  int maxStepsIsMiss, wavelengthSamples, maxSSSSteps, pad0;
+  int maxStepsIsMiss, wavelengthSamples, maxSSSSteps;
+  int maxBounces;  // per-job bound on path vertices, <= the module's MAX_BOUNCES (0: the module's)
   float lengthScale, minLengthScale, maxLengthScale, pad1;
   // sky (js/renderer.js:562-569)
   int haveEnvMap, envMapVisible;

@@ -119,6 +119,7 @@ def lib():
         "snelly_set_texture": (i32, [vp, u64, ctypes.c_char_p, vp, i32, i32, i32, i32, i32, i32]),
         "snelly_render": (i32, [vp, u64, P(RenderDesc), P(u64)]),
         "snelly_advance": (i32, [vp, u64, i32]),
+        "snelly_advance_batch": (i32, [vp, P(u64), P(i32), sz]),
         "snelly_readback": (i32, [vp, u64, vp, sz, i32]),
         "snelly_readback_state": (i32, [vp, u64, vp, vp, vp, vp]),
         "snelly_restore": (i32, [vp, u64, P(RenderDesc), vp, vp, vp, P(u64)]),
@@ -130,6 +131,7 @@ def lib():
         "snelly_launch_count": (u64, [vp]),
         "snelly_measure_fp32_peak": (i32, [vp, P(ctypes.c_double), P(ctypes.c_double)]),
         "snelly_flush_l2": (i32, [vp, sz]),
+        "snelly_image_stats": (i32, [vp, u64, vp]),
         "snelly_abi_sizeof": (sz, [i32]),
         "snelly_inverse_cdf": (i32, [P(Spectrum), vp]),
         "snelly_compile_check": (i32, [ctypes.c_char_p, P(SceneOpts), ctypes.c_char_p, sz, P(sz)]),

@@ -536,6 +536,8 @@ class Snelly:
         p.minLengthScale = max(self.minLengthScale, 1.0e-6)
         p.shadowStrength = r.shadowStrength
         p.maxSSSSteps = int(r.maxSSSSteps)
+        jb = getattr(r, "jobMaxBounces", None)  # per-job limit below the module's bound
+        p.maxBounces = int(round(jb if jb else r.maxBounces))
         p.maxStepsIsMiss = 1 if r.maxStepsIsMiss else 0
         p.wavelengthSamples = int(r.wavelengthSamples)
         p.skyPower = 10.0 ** r.skyPower
@@ -696,6 +698,12 @@ class Context:
     def advance(self, jid, frames):
         N.check(self._lib.snelly_advance(self._h, jid, int(frames)))
 
+    def advance_batch(self, jobs_frames):
+        """Enqueue frames on many jobs in batched launches: {job id: frames}."""
+        ids = (ctypes.c_uint64 * len(jobs_frames))(*jobs_frames.keys())
+        fr = (ctypes.c_int * len(jobs_frames))(*jobs_frames.values())
+        N.check(self._lib.snelly_advance_batch(self._h, ids, fr, len(jobs_frames)))
+
     def readback(self, jid, width, height, out=None, poll=False):
         if out is None:
             out = np.empty((height, width, 4), np.float32)
@@ -711,6 +719,12 @@ class Context:
         N.check(self._lib.snelly_readback_state(self._h, jid, rng.ctypes.data, acc.ctypes.data, comp.ctypes.data,
                                                 acc64.ctypes.data if fp64 else None))
         return rng, acc, comp, acc64
+
+    def image_stats(self, jid):
+        """Sums over pixels of mean X, Y, Z, Y^2 and the total sample count (float64[5])."""
+        out = np.zeros(5, np.float64)
+        N.check(self._lib.snelly_image_stats(self._h, jid, out.ctypes.data))
+        return out
 
     def status(self, jid):
         a, b = ctypes.c_int(), ctypes.c_int()

@@ -2,6 +2,8 @@
 // the FP32 peak microbenchmark used as the roofline denominator, and an L2 flush for timing.
 #include <cuda_runtime.h>
 
+#include <algorithm>
+#include <mutex>
 #include <string>
 
 #include "runtime_internal.h"
@@ -23,6 +25,47 @@ __global__ void __launch_bounds__(256) ffma_peak_kernel(float* out, int iters, f
   }
   float s = ((x0 + x1) + (x2 + x3)) + ((x4 + x5) + (x6 + x7));
   if (s == 1234.5f) out[blockIdx.x] = s;  // keeps the chains live
+}
+
+// Image statistics of a job's accumulators, pass 1: per-block partial sums (in double, fixed
+// order) of the per-pixel mean X, Y, Z, of Y^2 and of the sample counts -> partial[block].
+// The per-pixel mean is the Kahan sum minus its compensation, over the count.
+constexpr int kStatsThreads = 256;
+__global__ void __launch_bounds__(kStatsThreads) image_stats_partial(const float4* __restrict__ acc,
+                                                                      const float4* __restrict__ comp, long long npix,
+                                                                      double* __restrict__ partial) {
+  __shared__ double sh[5][kStatsThreads];
+  double a[5] = {0, 0, 0, 0, 0};
+  for (long long i = (long long)blockIdx.x * kStatsThreads + threadIdx.x; i < npix; i += (long long)gridDim.x * kStatsThreads) {
+    float4 s = acc[i], c = comp[i];
+    double n = s.w;
+    if (n > 0) {
+      double x = ((double)s.x - c.x) / n, y = ((double)s.y - c.y) / n, z = ((double)s.z - c.z) / n;
+      a[0] += x;
+      a[1] += y;
+      a[2] += z;
+      a[3] += y * y;
+    }
+    a[4] += n;
+  }
+  for (int k = 0; k < 5; ++k) sh[k][threadIdx.x] = a[k];
+  __syncthreads();
+  for (int w = kStatsThreads / 2; w > 0; w >>= 1) {
+    if ((int)threadIdx.x < w)
+      for (int k = 0; k < 5; ++k) sh[k][threadIdx.x] += sh[k][threadIdx.x + w];
+    __syncthreads();
+  }
+  if (threadIdx.x < 5) partial[5 * blockIdx.x + threadIdx.x] = sh[threadIdx.x][0];
+}
+
+// Pass 2: one block folds the partials (in block order) into out[5].
+__global__ void __launch_bounds__(32) image_stats_final(const double* __restrict__ partial, int nblocks,
+                                                        double* __restrict__ out) {
+  if (threadIdx.x < 5) {
+    double t = 0;
+    for (int b = 0; b < nblocks; ++b) t += partial[5 * b + threadIdx.x];
+    out[threadIdx.x] = t;
+  }
 }
 
 __global__ void l2_flush_kernel(float4* buf, size_t n, float v) {
@@ -63,6 +106,38 @@ int snelly_measure_fp32_peak(snelly_ctx* ctx, double* tflops, double* ms_out) {
   *tflops = flops / (best * 1e-3) / 1e12;
   if (ms_out) *ms_out = best;
   c.launches += 8;
+  return SNELLY_OK;
+}
+
+// Blocks of the statistics reduction: enough to fill the GPU, at most kStatsMaxBlocks.
+constexpr int kStatsMaxBlocks = 1184;  // 8 blocks per SM on 148 SMs
+
+int snelly_image_stats(snelly_ctx* ctx, uint64_t job_id, double* out5) {
+  if (!ctx || !out5) return snelly::fail(SNELLY_EINVAL, "null argument to snelly_image_stats");
+  snelly::Context& c = *ctx->c;
+  std::lock_guard<std::mutex> lk(c.mu);
+  auto it = c.jobs.find(job_id);
+  if (it == c.jobs.end()) return snelly::fail(SNELLY_ENOTFOUND, "unknown job id");
+  snelly::Job& j = it->second;
+  long long npix = (long long)j.desc.width * j.desc.height;
+  int blocks = (int)std::min<long long>(kStatsMaxBlocks, (npix + kStatsThreads - 1) / kStatsThreads);
+  if (blocks < 1) blocks = 1;
+  // scratch: per-block partials + the result, owned by the context
+  size_t need = sizeof(double) * (5 * (size_t)kStatsMaxBlocks + 8);
+  if (c.stats_scratch.bytes < need) {
+    c.release(c.stats_scratch);
+    int rc = c.alloc(c.stats_scratch, need);
+    if (rc) return rc;
+  }
+  double* partial = (double*)c.stats_scratch.ptr;
+  double* result = partial + 5 * kStatsMaxBlocks;
+  image_stats_partial<<<blocks, kStatsThreads, 0, c.stream>>>((const float4*)j.acc.ptr, (const float4*)j.comp.ptr,
+                                                               npix, partial);
+  image_stats_final<<<1, 32, 0, c.stream>>>(partial, blocks, result);
+  c.launches += 2;
+  if (cudaMemcpyAsync(out5, result, 5 * sizeof(double), cudaMemcpyDeviceToHost, c.stream) != cudaSuccess ||
+      cudaStreamSynchronize(c.stream) != cudaSuccess)
+    return snelly::fail(SNELLY_EDEVICE, "image statistics failed");
   return SNELLY_OK;
 }
 

@@ -274,206 +274,324 @@ SD_FN void primary_ray(const SnellyParams& P, const vec2& pixel, Rng& g, vec3& s
 // Triangle-filter importance sample in [-1, 1] (PT:1928-1932).
 SD_FN float tent(float xi) { return xi < 0.5f ? sqrtf(2.0f * xi) - 1.0f : 1.0f - sqrtf(2.0f - 2.0f * xi); }
 
-// One camera path (PT:1625-1926).
-SD_FN Rad camera_path(const Ctx& c, vec3 pW, vec3 rayDir, Rng& g) {
-  const SnellyParams& P = c.P;
-  Rad L = Rad(0.0f);
-  float misSky = 1.0f, misSun = 1.0f;
-#ifdef HAS_SPHERE_LIGHT
-  float misSph = 1.0f;
-#endif
-#ifdef HAS_DIELECTRIC
-  bool inDiele = c.sc.SDF_DIELECTRIC(pW) < 0.0f;
-#endif
-  Rad thr = Rad(1.0f);
-  int atmScatters = 0;
-  (void)atmScatters;
-  for (int vertex = 0; vertex <= MAX_BOUNCES; ++vertex) {
-    if (maxc(thr) < kThroughputEps) break;
-    Hit h = march_ray(c.job, pW, rayDir, P.maxLengthScale);
-    float rayLength = P.maxLengthScale;
-    if (h.hit) {
-      rayLength = glsl::length(h.p - pW);
-    } else {
-      // escaped: environment, sun and sphere light (PT:1657-1712)
-      float segLen;
-      Rad Tr;
-#ifdef HAS_SPHERE_LIGHT
-      vec3 pLight;
-      Rad LiSph = (P.sphereLightPower < kRadianceEps) ? Rad(0.0f) : sphere_light_hit(c, pW, rayDir, pLight);
-      if (avg(LiSph) > kRadianceEps) {
-        segLen = glsl::length(pLight - pW);
-        Tr = transmittance_free(c, pW, rayDir, segLen);
-        float sp = scatter_prob(c, Tr);
-        L += thr * Tr * misSph * LiSph / (1.0f - sp);
-      } else
-#endif
-      {
-        segLen = P.maxLengthScale;
-        Tr = transmittance_free(c, pW, rayDir, segLen);
-        float sp = scatter_prob(c, Tr);
-        if (avg(Tr) > kRadianceEps) {
-          if (!(vertex == 0 && !P.envMapVisible) && misSky > 0.0f)
-            L += thr * Tr * misSky * sky_radiance(c, rayDir) / (1.0f - sp);
-          if (!(vertex == 0 && !P.sunVisibleDirectly) && misSun > 0.0f)
-            L += thr * Tr * misSun * sun_radiance(c, rayDir) / (1.0f - sp);
-        }
-      }
-#ifdef HAS_ATMOSPHERE
-      if (vertex < 2) L += thr * atm_inscatter(c, pW, rayDir, segLen, g);
-      if (atmScatters + 1 < MAX_ATMOSPHERE_SCATTERS) {
-        float sp = scatter_prob(c, Tr);
-        if (sp > rand01(g)) {
-          vec3 ps(0.0f), wo(0.0f);
-          thr *= atm_scatter_sample(c, pW, rayDir, segLen, g, ps, wo) / fmaxf(kDenomTol, sp);
-          pW = ps;
-          rayDir = wo;
-          atmScatters++;
-          continue;
-        }
-      }
-#endif
-      (void)segLen;
-      break;
-    }
+// ---- the camera path, one vertex at a time (PT:1625-1926) -----------------------------------------
+// Everything a path carries from one vertex to the next.
+struct PathState {
+  vec3 pW, rayDir;
+  Rad thr, L;
+  float misSky, misSun, misSph;
+  int atmScatters;
+  bool inDiele;
+};
 
-    Rad Tr = Rad(1.0f);
-    bool hitSphereLight = false;
-    (void)hitSphereLight;
-#ifdef HAS_SPHERE_LIGHT
-    {
-      vec3 pLight;
-      Rad LiSph = (P.sphereLightPower < kRadianceEps) ? Rad(0.0f) : sphere_light_hit(c, pW, rayDir, pLight);
-      if (avg(LiSph) > kRadianceEps) {
-        float segLen = glsl::length(pLight - pW);
-        if (segLen < rayLength) {
-          hitSphereLight = true;
-          Tr = transmittance_free(c, pW, rayDir, segLen);
-          L += thr * Tr * misSph * LiSph;
-#ifdef HAS_ATMOSPHERE
-          if (vertex < 2) L += thr * atm_inscatter(c, pW, rayDir, segLen, g);
+// Next-event estimation whose sky and sun shadow rays are traced later (wavefront stages): the
+// unoccluded contribution of each light, to be scaled by the shadow term once the ray is traced.
+struct DeferredNee {
+  vec3 org;            // shadow-ray origin (the offset vertex)
+  Rad thr;             // path throughput at the vertex
+  Rad extra;           // sphere-light term, already shadowed
+  vec3 dir[2];         // sky, sun
+  float dist[2];
+  Rad c[2];            // f * Li0 / pdf * |cos| * mis
+  Rad li[2];           // Li0 (unshadowed radiance, for the gate)
+  bool pending[2];
+  bool any;
+};
+
+SD_FN void start_path(const Ctx& c, PathState& s, const vec3& start, const vec3& dir) {
+  s.pW = start;
+  s.rayDir = dir;
+  s.thr = Rad(1.0f);
+  s.L = Rad(0.0f);
+  s.misSky = s.misSun = s.misSph = 1.0f;
+  s.atmScatters = 0;
+#ifdef HAS_DIELECTRIC
+  s.inDiele = c.sc.SDF_DIELECTRIC(start) < 0.0f;
+#else
+  (void)c;
+  s.inDiele = false;
 #endif
-        }
+}
+
+// Next-event estimation at a surface vertex with the sky and sun shadow rays deferred
+// (same random numbers in the same order as direct_surface).
+SD_FN void direct_surface_deferred(const Ctx& c, const vec3& pW, const Frame& f, const vec3& wiW, int mat, Rng& g,
+                                   float& skyPdf, float& sunPdf, float& sphPdf, const Rad& thr, DeferredNee& nd) {
+  const SnellyParams& P = c.P;
+  vec3 wiL = to_local(wiW, f);
+  nd.org = pW;
+  nd.thr = thr;
+  nd.extra = Rad(0.0f);
+  nd.pending[0] = nd.pending[1] = false;
+  if (P.skyPower > kRadianceEps) {
+    vec3 woL = sample_cosine(g, skyPdf);
+    vec3 woW = to_world(woL, f);
+    Rad Li = sky_radiance(c, woW);
+    if (avg(Li) > kRadianceEps) {
+      float bp = fmaxf(kPdfEps, bsdf_pdf(c, pW, f, wiL, woL, mat));
+      Rad fv = bsdf_eval(c, pW, f, wiL, woL, mat);
+      float w = balance(skyPdf, bp);
+      nd.c[0] = fv * Li / fmaxf(kPdfEps, skyPdf) * fabsf(glsl::dot(woW, f.n)) * w;
+      nd.li[0] = Li;
+      nd.dir[0] = woW;
+      nd.dist[0] = P.maxLengthScale;
+      nd.pending[0] = true;
+    }
+  }
+  if (P.sunPower > kRadianceEps) {
+    vec3 woW = sample_sun_dir(c, g, sunPdf);
+    vec3 woL = to_local(woW, f);
+    Rad Li = woL.z < 0.0f ? Rad(0.0f) : sun_radiance(c, woW);
+    if (avg(Li) > kRadianceEps) {
+      float bp = fmaxf(kPdfEps, bsdf_pdf(c, pW, f, wiL, woL, mat));
+      Rad fv = bsdf_eval(c, pW, f, wiL, woL, mat);
+      float w = balance(sunPdf, bp);
+      nd.c[1] = fv * Li / fmaxf(kPdfEps, sunPdf) * fabsf(glsl::dot(woW, f.n)) * w;
+      nd.li[1] = Li;
+      nd.dir[1] = woW;
+      nd.dist[1] = P.maxLengthScale;
+      nd.pending[1] = true;
+    }
+  }
+#ifdef HAS_SPHERE_LIGHT
+  if (P.sphereLightPower > kRadianceEps &&
+      glsl::dot(pW - v3(P.sphereLightPosition), f.n) <= P.sphereLightRadius) {
+    vec3 pHit;
+    Rad Li = sample_sphere_light(c, g, pW, pHit, sphPdf);
+    if (avg(Li) > kRadianceEps) {
+      float dist = fmaxf(0.0f, glsl::length(pHit - pW) - 3.0f * P.minLengthScale);
+      vec3 woW = glsl::normalize(pHit - pW);
+      vec3 woL = to_local(woW, f);
+      Li = shadow_scale(c, Li, transmittance(c, pW, woW, dist));
+      if (avg(Li) > kRadianceEps) {
+        float bp = fmaxf(kPdfEps, bsdf_pdf(c, pW, f, wiL, woL, mat));
+        Rad fv = bsdf_eval(c, pW, f, wiL, woL, mat);
+        float w = balance(sphPdf, bp);
+        nd.extra = fv * Li / fmaxf(kPdfEps, sphPdf) * fabsf(glsl::dot(woW, f.n)) * w;
       }
     }
+  }
+#else
+  (void)sphPdf;
 #endif
-#ifdef HAS_DIELECTRIC
-    if (inDiele) thr *= glsl::exp(-rayLength * diele_absorption(c, pW));  // Beer's law (PT:1740-1744)
+  nd.any = true;
+}
+
+// The deferred estimate once the shadow rays are traced: occluded[l] for each pending light.
+SD_FN Rad resolve_deferred(const Ctx& c, const DeferredNee& nd, const bool occluded[2]) {
+  Rad Ld = Rad(0.0f);
+  for (int l = 0; l < 2; ++l) {
+    if (!nd.pending[l]) continue;
+    Rad Tr = occluded[l] ? Rad(0.0f) : transmittance_free(c, nd.org, nd.dir[l], nd.dist[l]);
+    Rad sc = glsl::abs(Rad(1.0f) - c.P.shadowStrength * (Rad(1.0f) - Tr));
+    if (avg(nd.li[l] * sc) > kRadianceEps) Ld += nd.c[l] * sc;
+  }
+  Ld += nd.extra;
+  return nd.thr * glsl::min(Rad(c.P.radianceClamp), Ld);
+}
+
+enum { VERTEX_CONTINUE = 0, VERTEX_DONE = 1 };
+
+// Everything of one loop iteration of the camera path after the ray has been traced (`h`).
+// With `nd` non-null the surface vertex's sky/sun next-event estimate is deferred into it.
+SD_FN int vertex_step(const Ctx& c, PathState& s, const Hit& h, int vertex, Rng& g, DeferredNee* nd) {
+  const SnellyParams& P = c.P;
+  (void)vertex;
+  float rayLength = P.maxLengthScale;
+  if (h.hit) {
+    rayLength = glsl::length(h.p - s.pW);
+  } else {
+    // escaped: environment, sun and sphere light (PT:1657-1712)
+    float segLen;
+    Rad Tr;
+#ifdef HAS_SPHERE_LIGHT
+    vec3 pLight;
+    Rad LiSph = (P.sphereLightPower < kRadianceEps) ? Rad(0.0f) : sphere_light_hit(c, s.pW, s.rayDir, pLight);
+    if (avg(LiSph) > kRadianceEps) {
+      segLen = glsl::length(pLight - s.pW);
+      Tr = transmittance_free(c, s.pW, s.rayDir, segLen);
+      float sp = scatter_prob(c, Tr);
+      s.L += s.thr * Tr * s.misSph * LiSph / (1.0f - sp);
+    } else
 #endif
+    {
+      segLen = P.maxLengthScale;
+      Tr = transmittance_free(c, s.pW, s.rayDir, segLen);
+      float sp = scatter_prob(c, Tr);
+      if (avg(Tr) > kRadianceEps) {
+        if (!(vertex == 0 && !P.envMapVisible) && s.misSky > 0.0f)
+          s.L += s.thr * Tr * s.misSky * sky_radiance(c, s.rayDir) / (1.0f - sp);
+        if (!(vertex == 0 && !P.sunVisibleDirectly) && s.misSun > 0.0f)
+          s.L += s.thr * Tr * s.misSun * sun_radiance(c, s.rayDir) / (1.0f - sp);
+      }
+    }
 #ifdef HAS_ATMOSPHERE
-    if (vertex < 2) L += thr * atm_inscatter(c, pW, rayDir, rayLength, g);
-    if (!hitSphereLight) Tr = transmittance_free(c, pW, rayDir, rayLength);
-    if (atmScatters + 1 < MAX_ATMOSPHERE_SCATTERS) {
+    if (vertex < 2) s.L += s.thr * atm_inscatter(c, s.pW, s.rayDir, segLen, g);
+    if (s.atmScatters + 1 < MAX_ATMOSPHERE_SCATTERS) {
       float sp = scatter_prob(c, Tr);
       if (sp > rand01(g)) {
         vec3 ps(0.0f), wo(0.0f);
-        thr *= atm_scatter_sample(c, pW, rayDir, rayLength, g, ps, wo) / fmaxf(kDenomTol, sp);
-        pW = ps;
-        rayDir = wo;
-        atmScatters++;
-        continue;
+        s.thr *= atm_scatter_sample(c, s.pW, s.rayDir, segLen, g, ps, wo) / fmaxf(kDenomTol, sp);
+        s.pW = ps;
+        s.rayDir = wo;
+        s.atmScatters++;
+        return VERTEX_CONTINUE;
       }
-      thr /= fmaxf(kDenomTol, 1.0f - sp);
-    }
-    if (hitSphereLight) break;
-    thr *= transmittance_free(c, pW, rayDir, rayLength);
-#endif
-    (void)Tr;
-
-    // surface interaction (PT:1782-1794)
-    pW = h.p;
-    vec3 nW = sdf_normal(c.job, pW, h.mat);
-    vec3 ngW = nW;
-    Frame fr = make_frame(nW);
-#ifdef HAS_NORMALMAP
-    nW = perturb_normal(c, pW, fr, h.mat);
-    if (glsl::dot(nW, rayDir) > 0.0f && h.mat != MAT_DIELE) nW = 2.0f * ngW * glsl::dot(ngW, nW) - nW;
-    fr = make_frame(nW);
-#endif
-
-    // surface scatter or subsurface walk (PT:1796-1811)
-    bool doSSS = false;
-    float probSSS = 0.0f;
-    Rad ssAlb = Rad(0.0f);
-    (void)ssAlb;
-#ifdef HAS_SURFACE
-    if (P.subsurfaceMFP > 0.0f) {
-      ssAlb = subsurf_albedo(c, pW, fr.n);
-      float wd = (1.0f - P.subsurface) * avg(surf_diffuse(c, pW, fr.n, -rayDir));
-      float ws = avg(surf_specular(c, pW, fr.n, -rayDir));
-      float wss = P.subsurface * avg(ssAlb) * 3.0f;
-      float tot = wd + ws + wss;
-      probSSS = wss / (tot + kDenomTol);
-      probSSS = glsl::clamp(probSSS, 0.0f, 1.0f - kPdfEps);
-      doSSS = rand01(g) < probSSS;
     }
 #endif
-    if (!doSSS) {
-      vec3 wiW = -rayDir;
-      vec3 wiL = to_local(wiW, fr);
-      vec3 woL(0.0f);  // an uninitialised local in the reference (PT:1820), zero under WebGL
-      float bsdfPdf = 0.0f;
-      Rad f = bsdf_sample(c, pW, fr, wiL, h.mat, woL, bsdfPdf, g);
-      vec3 woW = to_world(woL, fr);
+    (void)segLen;
+    return VERTEX_DONE;
+  }
+
+  Rad Tr = Rad(1.0f);
+  bool hitSphereLight = false;
+  (void)hitSphereLight;
+  (void)Tr;
+#ifdef HAS_SPHERE_LIGHT
+  {
+    vec3 pLight;
+    Rad LiSph = (P.sphereLightPower < kRadianceEps) ? Rad(0.0f) : sphere_light_hit(c, s.pW, s.rayDir, pLight);
+    if (avg(LiSph) > kRadianceEps) {
+      float segLen = glsl::length(pLight - s.pW);
+      if (segLen < rayLength) {
+        hitSphereLight = true;
+        Tr = transmittance_free(c, s.pW, s.rayDir, segLen);
+        s.L += s.thr * Tr * s.misSph * LiSph;
+#ifdef HAS_ATMOSPHERE
+        if (vertex < 2) s.L += s.thr * atm_inscatter(c, s.pW, s.rayDir, segLen, g);
+#endif
+      }
+    }
+  }
+#endif
 #ifdef HAS_DIELECTRIC
-      if (h.mat == MAT_DIELE && glsl::dot(wiW, ngW) * glsl::dot(woW, ngW) < 0.0f) inDiele = !inDiele;
+  if (s.inDiele) s.thr *= glsl::exp(-rayLength * diele_absorption(c, s.pW));  // Beer's law (PT:1740-1744)
+#endif
+#ifdef HAS_ATMOSPHERE
+  if (vertex < 2) s.L += s.thr * atm_inscatter(c, s.pW, s.rayDir, rayLength, g);
+  if (!hitSphereLight) Tr = transmittance_free(c, s.pW, s.rayDir, rayLength);
+  if (s.atmScatters + 1 < MAX_ATMOSPHERE_SCATTERS) {
+    float sp = scatter_prob(c, Tr);
+    if (sp > rand01(g)) {
+      vec3 ps(0.0f), wo(0.0f);
+      s.thr *= atm_scatter_sample(c, s.pW, s.rayDir, rayLength, g, ps, wo) / fmaxf(kDenomTol, sp);
+      s.pW = ps;
+      s.rayDir = wo;
+      s.atmScatters++;
+      return VERTEX_CONTINUE;
+    }
+    s.thr /= fmaxf(kDenomTol, 1.0f - sp);
+  }
+  if (hitSphereLight) return VERTEX_DONE;
+  s.thr *= transmittance_free(c, s.pW, s.rayDir, rayLength);
+#endif
+
+  // surface interaction (PT:1782-1794)
+  s.pW = h.p;
+  vec3 nW = sdf_normal(c.job, s.pW, h.mat);
+  vec3 ngW = nW;
+  Frame fr = make_frame(nW);
+#ifdef HAS_NORMALMAP
+  nW = perturb_normal(c, s.pW, fr, h.mat);
+  if (glsl::dot(nW, s.rayDir) > 0.0f && h.mat != MAT_DIELE) nW = 2.0f * ngW * glsl::dot(ngW, nW) - nW;
+  fr = make_frame(nW);
+#endif
+
+  // surface scatter or subsurface walk (PT:1796-1811)
+  bool doSSS = false;
+  float probSSS = 0.0f;
+  Rad ssAlb = Rad(0.0f);
+  (void)ssAlb;
+#ifdef HAS_SURFACE
+  if (P.subsurfaceMFP > 0.0f) {
+    ssAlb = subsurf_albedo(c, s.pW, fr.n);
+    float wd = (1.0f - P.subsurface) * avg(surf_diffuse(c, s.pW, fr.n, -s.rayDir));
+    float ws = avg(surf_specular(c, s.pW, fr.n, -s.rayDir));
+    float wss = P.subsurface * avg(ssAlb) * 3.0f;
+    float tot = wd + ws + wss;
+    probSSS = wss / (tot + kDenomTol);
+    probSSS = glsl::clamp(probSSS, 0.0f, 1.0f - kPdfEps);
+    doSSS = rand01(g) < probSSS;
+  }
+#endif
+  if (!doSSS) {
+    vec3 wiW = -s.rayDir;
+    vec3 wiL = to_local(wiW, fr);
+    vec3 woL(0.0f);  // an uninitialised local in the reference (PT:1820), zero under WebGL
+    float bsdfPdf = 0.0f;
+    Rad f = bsdf_sample(c, s.pW, fr, wiL, h.mat, woL, bsdfPdf, g);
+    vec3 woW = to_world(woL, fr);
+#ifdef HAS_DIELECTRIC
+    if (h.mat == MAT_DIELE && glsl::dot(wiW, ngW) * glsl::dot(woW, ngW) < 0.0f) s.inDiele = !s.inDiele;
 #endif
 #ifdef HAS_VOLUME_EMISSION
-      L += thr * vol_emission(c, pW);
+    s.L += s.thr * vol_emission(c, s.pW);
 #endif
-      rayDir = woW;
-      pW += ngW * glsl::sign(glsl::dot(rayDir, ngW)) * 3.0f * P.minLengthScale;
-      float skyPdf = 0.0f, sunPdf = 0.0f, sphPdf = 0.0f;
-#ifdef HAS_DIELECTRIC
-      if (!inDiele)
-#endif
-        L += thr * direct_surface(c, pW, fr, wiW, h.mat, g, skyPdf, sunPdf, sphPdf);
-      Rad fop = glsl::min(Rad(P.radianceClamp), f / fmaxf(kPdfEps, bsdfPdf));
-      thr *= fop * fabsf(glsl::dot(woW, nW)) / fmaxf(kPdfEps, 1.0f - probSSS);
-      misSky = balance(bsdfPdf, skyPdf);
-      misSun = balance(bsdfPdf, sunPdf);
-#ifdef HAS_SPHERE_LIGHT
-      misSph = balance(bsdfPdf, sphPdf);
-#endif
+    s.rayDir = woW;
+    s.pW += ngW * glsl::sign(glsl::dot(s.rayDir, ngW)) * 3.0f * P.minLengthScale;
+    float skyPdf = 0.0f, sunPdf = 0.0f, sphPdf = 0.0f;
+    if (!s.inDiele) {
+      if (nd) direct_surface_deferred(c, s.pW, fr, wiW, h.mat, g, skyPdf, sunPdf, sphPdf, s.thr, *nd);
+      else s.L += s.thr * direct_surface(c, s.pW, fr, wiW, h.mat, g, skyPdf, sunPdf, sphPdf);
     }
-#ifdef HAS_SURFACE
-    else {
-      // subsurface random walk to a new vertex (PT:1866-1918)
-      Rad dAlbEntry = surf_diffuse(c, pW, fr.n, -rayDir);
-      (void)dAlbEntry;
-      Rad walkThr = Rad(0.0f);
-      vec3 pExit(0.0f);
-      Frame fw = fr;
-      fw.n = ngW;  // geometric normal for the entry (the tangents stay those of the shading frame)
-      if (!sss_walk(c, pW, fw, g, ssAlb, walkThr, pExit)) break;
-      pW = pExit;
-      nW = sdf_normal(c.job, pExit, MAT_SURFA);
-      Frame fe = make_frame(nW);
-      float bsdfPdf = 0.0f;
-      vec3 dExit = sample_cosine(g, bsdfPdf);
-      vec3 woW = to_world(dExit, fe);
-      rayDir = woW;
-      thr *= walkThr;
-      float skyPdf = 0.0f, sunPdf = 0.0f, sphPdf = 0.0f;
-      Rad dAlbExit = surf_diffuse(c, pW, nW, -rayDir);
-#ifdef HAS_DIELECTRIC
-      if (!inDiele)
-#endif
-        L += thr * sss_exit_radiance(c, pExit, fe, g, dAlbExit, skyPdf, sunPdf, sphPdf);
-      misSky = balance(bsdfPdf, skyPdf);
-      misSun = balance(bsdfPdf, sunPdf);
+    Rad fop = glsl::min(Rad(P.radianceClamp), f / fmaxf(kPdfEps, bsdfPdf));
+    s.thr *= fop * fabsf(glsl::dot(woW, nW)) / fmaxf(kPdfEps, 1.0f - probSSS);
+    s.misSky = balance(bsdfPdf, skyPdf);
+    s.misSun = balance(bsdfPdf, sunPdf);
 #ifdef HAS_SPHERE_LIGHT
-      misSph = balance(bsdfPdf, sphPdf);
+    s.misSph = balance(bsdfPdf, sphPdf);
 #endif
-      Rad lobe = glsl::mix(Rad(1.0f), dAlbExit, P.subsurfaceDiffuseWeight) / kPi;
-      Rad fop = glsl::min(Rad(P.radianceClamp), lobe / fmaxf(kPdfEps, bsdfPdf));
-      thr *= fop * fabsf(glsl::dot(woW, nW)) / fmaxf(kPdfEps, probSSS);
-      pW += nW * glsl::sign(glsl::dot(rayDir, nW)) * 3.0f * P.minLengthScale;
-    }
-#endif
-    if (maxc(thr) < kThroughputEps) break;
   }
-  return L;
+#ifdef HAS_SURFACE
+  else {
+    // subsurface random walk to a new vertex (PT:1866-1918)
+    Rad walkThr = Rad(0.0f);
+    vec3 pExit(0.0f);
+    Frame fw = fr;
+    fw.n = ngW;  // geometric normal for the entry (the tangents stay those of the shading frame)
+    if (!sss_walk(c, s.pW, fw, g, ssAlb, walkThr, pExit)) return VERTEX_DONE;
+    s.pW = pExit;
+    nW = sdf_normal(c.job, pExit, MAT_SURFA);
+    Frame fe = make_frame(nW);
+    float bsdfPdf = 0.0f;
+    vec3 dExit = sample_cosine(g, bsdfPdf);
+    vec3 woW = to_world(dExit, fe);
+    s.rayDir = woW;
+    s.thr *= walkThr;
+    float skyPdf = 0.0f, sunPdf = 0.0f, sphPdf = 0.0f;
+    Rad dAlbExit = surf_diffuse(c, s.pW, nW, -s.rayDir);
+    if (!s.inDiele) s.L += s.thr * sss_exit_radiance(c, pExit, fe, g, dAlbExit, skyPdf, sunPdf, sphPdf);
+    s.misSky = balance(bsdfPdf, skyPdf);
+    s.misSun = balance(bsdfPdf, sunPdf);
+#ifdef HAS_SPHERE_LIGHT
+    s.misSph = balance(bsdfPdf, sphPdf);
+#endif
+    Rad lobe = glsl::mix(Rad(1.0f), dAlbExit, P.subsurfaceDiffuseWeight) / kPi;
+    Rad fop = glsl::min(Rad(P.radianceClamp), lobe / fmaxf(kPdfEps, bsdfPdf));
+    s.thr *= fop * fabsf(glsl::dot(woW, nW)) / fmaxf(kPdfEps, probSSS);
+    s.pW += nW * glsl::sign(glsl::dot(s.rayDir, nW)) * 3.0f * P.minLengthScale;
+  }
+#endif
+  if (maxc(s.thr) < kThroughputEps) return VERTEX_DONE;
+  return VERTEX_CONTINUE;
+}
+
+// The loop bound on vertices: the module's MAX_BOUNCES, or a smaller per-job value.
+SD_FN int max_bounces(const SnellyParams& P) {
+  return (P.maxBounces > 0 && P.maxBounces < MAX_BOUNCES) ? P.maxBounces : MAX_BOUNCES;
+}
+
+// One camera path, path-per-thread (PT:1625-1926).
+SD_FN Rad camera_path(const Ctx& c, vec3 pW, vec3 rayDir, Rng& g) {
+  PathState s;
+  start_path(c, s, pW, rayDir);
+  const int maxb = max_bounces(c.P);
+  for (int vertex = 0; vertex <= maxb; ++vertex) {
+    if (maxc(s.thr) < kThroughputEps) break;
+    Hit h = march_ray(c.job, s.pW, s.rayDir, c.P.maxLengthScale);
+    if (vertex_step(c, s, h, vertex, g, nullptr) == VERTEX_DONE) break;
+  }
+  return s.L;
 }
 
 // Wavelength for this pixel and frame (PT:1936-1947): the inverse CDF of the emission spectrum

@@ -17,3 +17,36 @@ typedef struct JobRec {
   int slot;              // index into the module's constant-memory parameter banks
   int mode;              // SNELLY_MODE_*
 } JobRec;
+
+// Wavefront path state and queues of one job (structure of arrays, one element per path =
+// pixel of the frame; device pointers). Layout shared with the host (wavefront.cpp).
+#define WF_A 0      // active-path queue counts [2] (ping-pong by iteration parity)
+#define WF_S 2      // shadow-ray queue counts [2]
+#define WF_Q 4      // shade-queue segment counts [2][4]
+#define WF_HEAD 12  // extend work heads, one per iteration
+#define WF_COUNTERS 96
+typedef struct WfBuffers {
+  float4* pos;      // path vertex pW (xyz)
+  float4* dir;      // ray direction (xyz)
+  float4* thr;      // throughput (Rad in xyz)
+  float4* rad;      // accumulated radiance L
+  float4* cmf;      // rgb colour-matching weights (xyz), wavelength (w)
+  float4* mis;      // MIS weights sky, sun, sphere
+  float4* xyzw;     // XYZ weights of the wavelength (xyz)
+  int4* info;       // vertex, atmosphere scatters, flags, unused
+  uint4* rng;       // RNG lanes during the frame
+  float4* hit;      // continuation hit position (xyz), encoded material + hit flag (w)
+  float4* nee_org;  // shadow-ray origin
+  float4* nee_thr;  // throughput at the vertex of the pending estimate
+  float4* nee_extra;  // sphere-light term (already shadowed)
+  float4* nee_dir[2];  // sky, sun shadow directions (xyz) and lengths (w)
+  float4* nee_c[2];    // unoccluded contributions
+  float4* nee_li[2];   // unshadowed radiance (gate)
+  unsigned char* shadow;  // occlusion result per shadow ray (2 per path)
+  int* qa[2];       // active-path queues
+  int* qs[2];       // shadow-ray queues (path * 2 + light)
+  int* qshade;      // shade queue, 4 segments of `paths` entries: finish/miss, surface, metal, dielectric
+  int* cnt;         // counters (WF_*)
+  int paths;
+  int pixel_begin;
+} WfBuffers;

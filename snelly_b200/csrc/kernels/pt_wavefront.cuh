@@ -1,0 +1,392 @@
+// pt_wavefront.cuh - wavefront integrator: the camera path of pt_integrator.cuh split into stages
+// over queues of rays and paths in HBM (one job per launch, one sample per pixel per frame).
+//
+//   generate: camera rays (wavelength, jitter, primary ray) for every pixel -> active queue.
+//   extend  : persistent warps trace the continuation rays of the active paths and the pending
+//             shadow rays of the previous vertex. A lane that finishes a ray takes the next one
+//             from a global work head (warp-aggregated atomics), so warps stay full however
+//             uneven the sphere-tracing step counts are. Hits are appended to per-material
+//             segments of the shade queue (misses and finishing paths first).
+//   shade   : per path: resolve the previous vertex's deferred next-event estimate with the
+//             shadow results, then run the vertex (vertex_step) with the sky/sun shadow rays
+//             deferred; continuing paths and new shadow rays go to the next iteration's queues,
+//             finished paths add their XYZ to the pixel's Kahan sums.
+// The host launches generate once and (extend, shade) MAX_BOUNCES + 2 times per frame; the queue
+// counters ping-pong by iteration parity, so the sequence needs no host synchronisation.
+#pragma once
+#include "pt_integrator.cuh"
+#include "pt_launch.h"
+
+#ifndef WF_CHUNK
+#define WF_CHUNK 8  // march steps between refills
+#endif
+#define WF_FULL 0xffffffffu
+
+namespace sdev {
+
+enum { WF_INDIELE = 1, WF_FINISHING = 2, WF_NEE = 4, WF_NEE_SKY = 8, WF_NEE_SUN = 16 };
+
+#ifdef DISPERSION_ENABLED
+SD_FN Rad ld_rad(const float4& v) { return v.x; }
+SD_FN float4 st_rad(const Rad& r) { return make_float4(r, 0.0f, 0.0f, 0.0f); }
+#else
+SD_FN Rad ld_rad(const float4& v) { return vec3(v.x, v.y, v.z); }
+SD_FN float4 st_rad(const Rad& r) { return make_float4(r.x, r.y, r.z, 0.0f); }
+#endif
+SD_FN vec3 ld3(const float4& v) { return vec3(v.x, v.y, v.z); }
+SD_FN float4 st3(const vec3& v, float w = 0.0f) { return make_float4(v.x, v.y, v.z, w); }
+SD_FN unsigned lanemask_lt() { return (1u << (threadIdx.x & 31)) - 1u; }
+
+// Warp-aggregated append: every lane calls it; lanes with `on` get consecutive slots.
+SD_FN int warp_append(int* counter, bool on) {
+  unsigned m = __ballot_sync(WF_FULL, on);
+  if (!m) return -1;
+  int leader = __ffs(m) - 1;
+  int base = 0;
+  if ((int)(threadIdx.x & 31) == leader) base = atomicAdd(counter, __popc(m));
+  base = __shfl_sync(WF_FULL, base, leader);
+  return on ? base + __popc(m & lanemask_lt()) : -1;
+}
+
+SD_FN float enc_hit(bool hit, int mat) { return __int_as_float((hit ? 1 : 0) | ((mat + 1) << 1)); }
+SD_FN void dec_hit(float w, bool& hit, int& mat) {
+  int v = __float_as_int(w);
+  hit = v & 1;
+  mat = (v >> 1) - 1;
+}
+
+// Final contribution of a path: XYZ added to the pixel's Kahan sums, RNG written back.
+SD_FN void finish_path(const JobRec& J, const WfBuffers& B, int path, const Rad& L, const vec3& xyzw, const Rng& g) {
+  long long i = (long long)B.pixel_begin + path;
+#ifdef DISPERSION_ENABLED
+  vec3 c = xyzw * (L / float(MAX_SAMPLES_PER_FRAME));
+#else
+  (void)xyzw;
+  vec3 c = rgb_to_xyz(L / float(MAX_SAMPLES_PER_FRAME));
+#endif
+  float4 s = J.acc[i], cp = J.comp[i];
+  float y, t;
+  y = c.x - cp.x; t = s.x + y; cp.x = (t - s.x) - y; s.x = t;
+  y = c.y - cp.y; t = s.y + y; cp.y = (t - s.y) - y; s.y = t;
+  y = c.z - cp.z; t = s.z + y; cp.z = (t - s.z) - y; s.z = t;
+  s.w += 1.0f;
+  J.acc[i] = s;
+  J.comp[i] = cp;
+  if (J.acc64) {
+    J.acc64[4 * i + 0] += double(c.x);
+    J.acc64[4 * i + 1] += double(c.y);
+    J.acc64[4 * i + 2] += double(c.z);
+    J.acc64[4 * i + 3] += 1.0;
+  }
+  J.rng[i] = make_uint4(g.s[0], g.s[1], g.s[2], g.s[3]);
+}
+
+}  // namespace sdev
+
+extern "C" __global__ void __launch_bounds__(SNELLY_BLOCK) snelly_wf_generate(const JobRec* __restrict__ jobs,
+                                                                           const SnellyParams* __restrict__ gparams,
+                                                                           WfBuffers B) {
+  using namespace sdev;
+  const JobRec& J = jobs[0];
+  int path = blockIdx.x * blockDim.x + threadIdx.x;
+  if (path == 0) {
+    B.cnt[WF_A + 0] = B.paths;
+    for (int k = 1; k < WF_COUNTERS; ++k) B.cnt[k] = 0;
+  }
+  if (path >= B.paths) return;
+  long long i = (long long)B.pixel_begin + path;
+  const SnellyParams& P = c_params[0];
+  uint4 r4 = J.rng[i];
+  Rng g;
+  g.s[0] = r4.x; g.s[1] = r4.y; g.s[2] = r4.z; g.s[3] = r4.w;
+  Scene sc(uniforms_of(0));
+  sc.INIT();
+  Ctx c{P, gparams, sc, 0, 0.0f, vec3(0.0f), Frame()};
+  const int W = J.width;
+  const int x = int(i % W), y = int(i / W);
+  vec3 xyzw = pick_wavelength(c, g);
+  c.sun = make_frame(v3(P.sunDir));
+  float jx = 0.5f * P.filterRadius * tent(rand01(g));
+  float jy = 0.5f * P.filterRadius * tent(rand01(g));
+  vec3 start, dir;
+  primary_ray_hook(c, vec2(float(x) + 0.5f, float(y) + 0.5f) + vec2(jx, jy), g, start, dir);
+  PathState s;
+  start_path(c, s, start, dir);
+  B.pos[path] = st3(s.pW);
+  B.dir[path] = st3(s.rayDir);
+  B.thr[path] = st_rad(s.thr);
+  B.rad[path] = st_rad(s.L);
+  B.cmf[path] = st3(c.cmf, c.lambda);
+  B.mis[path] = make_float4(1.0f, 1.0f, 1.0f, 0.0f);
+  B.xyzw[path] = st3(xyzw);
+  B.info[path] = make_int4(0, 0, s.inDiele ? WF_INDIELE : 0, 0);
+  B.rng[path] = make_uint4(g.s[0], g.s[1], g.s[2], g.s[3]);
+  B.qa[0][path] = path;
+}
+
+// Trace the active continuation rays and the pending shadow rays of iteration `it`.
+extern "C" __global__ void __launch_bounds__(SNELLY_BLOCK) snelly_wf_extend(WfBuffers B, int it) {
+  using namespace sdev;
+  const SnellyParams& P = c_params[0];
+  Scene sc(uniforms_of(0));
+  sc.INIT();
+  int* cnt = B.cnt;
+  const int cur = it & 1, nxt = cur ^ 1;
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    cnt[WF_A + nxt] = 0;
+    cnt[WF_S + nxt] = 0;
+  }
+  const int nA = cnt[WF_A + cur], nS = cnt[WF_S + cur];
+  const int total = nA + nS;
+  const int* qa = B.qa[cur];
+  const int* qs = B.qs[cur];
+  int* qcnt = cnt + WF_Q + 4 * cur;
+  const float minMarch = P.minLengthScale;
+  const float maxLen = P.maxLengthScale;
+
+  bool has = false, exhausted = false;
+  int path = 0, sidx = -1;  // sidx >= 0: a shadow ray
+  vec3 o(0.0f), d(0.0f);
+  float t = 0.0f, sgn = 1.0f, maxd = 0.0f;
+  int n = 0;
+  for (;;) {
+    // ---- refill idle lanes ----------------------------------------------------------------
+    bool want = !has && !exhausted;
+    unsigned need = __ballot_sync(WF_FULL, want);
+    bool done = false, res_hit = false, finishing = false;
+    int res_mat = MAT_INVAL;
+    if (need) {
+      int leader = __ffs(need) - 1;
+      int base = 0;
+      if ((int)(threadIdx.x & 31) == leader) base = atomicAdd(cnt + WF_HEAD + it, __popc(need));
+      base = __shfl_sync(WF_FULL, base, leader);
+      if (want) {
+        int w = base + __popc(need & lanemask_lt());
+        if (w >= total) {
+          exhausted = true;
+        } else if (w < nA) {
+          path = qa[w];
+          sidx = -1;
+          if (B.info[path].z & WF_FINISHING) {
+            finishing = true;
+            done = true;
+          } else {
+            o = ld3(B.pos[path]);
+            d = ld3(B.dir[path]);
+            maxd = maxLen;
+            has = true;
+          }
+        } else {
+          sidx = qs[w - nA];
+          path = sidx >> 1;
+          o = ld3(B.nee_org[path]);
+          float4 dd = B.nee_dir[sidx & 1][path];
+          d = ld3(dd);
+          maxd = dd.w;
+          has = true;
+        }
+        if (has) {  // first distance at the ray origin (PT:888-900)
+          float sdf = 1.0e20f;
+#ifdef HAS_SURFACE
+          sdf = fminf(sdf, fabsf(sc.SDF_SURFACE(o)));
+#endif
+#ifdef HAS_METAL
+          sdf = fminf(sdf, fabsf(sc.SDF_METAL(o)));
+#endif
+#ifdef HAS_DIELECTRIC
+          sdf = fminf(sdf, fabsf(sc.SDF_DIELECTRIC(o)));
+#endif
+          sgn = glsl::sign(sdf);
+          t = sgn * sdf;
+          n = 0;
+          if (fabsf(t) >= maxd) {
+            done = true;
+            res_hit = false;
+          }
+        }
+      }
+    }
+    // ---- march (PT:901-919) ------------------------------------------------------------------
+    for (int k = 0; k < WF_CHUNK && has && !done; ++k) {
+      vec3 p = o + t * d;
+      float sdf = 1.0e20f;
+      int m = MAT_INVAL;
+#ifdef HAS_SURFACE
+      {
+        float dd = fabsf(sc.SDF_SURFACE(p));
+        if (dd < minMarch) m = MAT_SURFA;
+        sdf = fminf(sdf, dd);
+      }
+#endif
+#ifdef HAS_METAL
+      if (m == MAT_INVAL) {
+        float dd = fabsf(sc.SDF_METAL(p));
+        if (dd < minMarch) m = MAT_METAL;
+        sdf = fminf(sdf, dd);
+      }
+#endif
+#ifdef HAS_DIELECTRIC
+      if (m == MAT_INVAL) {
+        float dd = fabsf(sc.SDF_DIELECTRIC(p));
+        if (dd < minMarch) m = MAT_DIELE;
+        sdf = fminf(sdf, dd);
+      }
+#endif
+      if (m != MAT_INVAL) {
+        done = true;
+        res_hit = true;
+        res_mat = m;
+        break;
+      }
+      t += sgn * sdf;
+      if (fabsf(t) >= maxd) {
+        done = true;
+        res_hit = false;
+        break;
+      }
+      if (++n >= MAX_MARCH_STEPS) {  // out of steps: a hit at the zero position unless maxStepsIsMiss
+        done = true;
+        res_hit = !P.maxStepsIsMiss;
+        res_mat = MAT_INVAL;
+        t = 0.0f;
+        o = vec3(0.0f);
+        d = vec3(0.0f);
+        break;
+      }
+    }
+    // ---- results ---------------------------------------------------------------------------
+    bool cont_result = done && sidx < 0;
+    int seg = -1;
+    if (cont_result) {
+      if (!finishing) B.hit[path] = st3(o + t * d, enc_hit(res_hit, res_mat));
+      seg = (finishing || !res_hit) ? 0 : (res_mat == MAT_SURFA ? 1 : (res_mat == MAT_METAL ? 2 : (res_mat == MAT_DIELE ? 3 : 0)));
+    }
+    if (done && sidx >= 0) B.shadow[sidx] = res_hit ? 1 : 0;
+    for (int sgi = 0; sgi < 4; ++sgi) {
+      int slot = warp_append(qcnt + sgi, seg == sgi);
+      if (slot >= 0) B.qshade[sgi * B.paths + slot] = path;
+    }
+    if (done) has = false;
+    if (__all_sync(WF_FULL, exhausted && !has)) break;
+  }
+}
+
+// Shade every path the extend stage of iteration `it` queued.
+extern "C" __global__ void __launch_bounds__(SNELLY_BLOCK) snelly_wf_shade(const JobRec* __restrict__ jobs,
+                                                                        const SnellyParams* __restrict__ gparams,
+                                                                        WfBuffers B, int it) {
+  using namespace sdev;
+  const JobRec& J = jobs[0];
+  const SnellyParams& P = c_params[0];
+  int* cnt = B.cnt;
+  const int cur = it & 1, nxt = cur ^ 1;
+  const int* qc = cnt + WF_Q + 4 * cur;
+  const int n0 = qc[0], n1 = qc[1], n2 = qc[2], n3 = qc[3];
+  const int total = n0 + n1 + n2 + n3;
+  if (blockIdx.x == 0 && threadIdx.x == 0)
+    for (int k = 0; k < 4; ++k) cnt[WF_Q + 4 * nxt + k] = 0;
+  Scene sc(uniforms_of(0));
+  sc.INIT();
+  const int stride = gridDim.x * blockDim.x;
+  for (int base = blockIdx.x * blockDim.x; base < total; base += stride) {
+    int w = base + threadIdx.x;
+    bool valid = w < total;
+    int path = 0;
+    bool push_active = false;
+    int push_shadow = 0;  // bit 0: sky, bit 1: sun
+    if (valid) {
+      int seg = w < n0 ? 0 : (w < n0 + n1 ? 1 : (w < n0 + n1 + n2 ? 2 : 3));
+      int off = w - (seg == 0 ? 0 : (seg == 1 ? n0 : (seg == 2 ? n0 + n1 : n0 + n1 + n2)));
+      path = B.qshade[seg * B.paths + off];
+      int4 info = B.info[path];
+      float4 cm = B.cmf[path];
+      Ctx c{P, gparams, sc, 0, cm.w, ld3(cm), make_frame(v3(P.sunDir))};
+      PathState s;
+      s.pW = ld3(B.pos[path]);
+      s.rayDir = ld3(B.dir[path]);
+      s.thr = ld_rad(B.thr[path]);
+      s.L = ld_rad(B.rad[path]);
+      float4 mw = B.mis[path];
+      s.misSky = mw.x;
+      s.misSun = mw.y;
+      s.misSph = mw.z;
+      s.atmScatters = info.y;
+      s.inDiele = info.z & WF_INDIELE;
+      uint4 r4 = B.rng[path];
+      Rng g;
+      g.s[0] = r4.x; g.s[1] = r4.y; g.s[2] = r4.z; g.s[3] = r4.w;
+      int flags = info.z;
+      if (flags & WF_NEE) {  // the previous vertex's next-event estimate, now that its shadows are traced
+        DeferredNee nd;
+        nd.org = ld3(B.nee_org[path]);
+        nd.thr = ld_rad(B.nee_thr[path]);
+        nd.extra = ld_rad(B.nee_extra[path]);
+        bool occ[2] = {false, false};
+        for (int l = 0; l < 2; ++l) {
+          nd.pending[l] = flags & (l == 0 ? WF_NEE_SKY : WF_NEE_SUN);
+          if (nd.pending[l]) {
+            float4 dd = B.nee_dir[l][path];
+            nd.dir[l] = ld3(dd);
+            nd.dist[l] = dd.w;
+            nd.c[l] = ld_rad(B.nee_c[l][path]);
+            nd.li[l] = ld_rad(B.nee_li[l][path]);
+            occ[l] = B.shadow[2 * path + l];
+          }
+        }
+        s.L += resolve_deferred(c, nd, occ);
+        flags &= ~(WF_NEE | WF_NEE_SKY | WF_NEE_SUN);
+      }
+      bool finished;
+      if (flags & WF_FINISHING) {
+        finished = true;
+      } else {
+        float4 hw = B.hit[path];
+        Hit h;
+        h.p = ld3(hw);
+        dec_hit(hw.w, h.hit, h.mat);
+        int vertex = info.x;
+        DeferredNee nd;
+        nd.any = false;
+        int r = vertex_step(c, s, h, vertex, g, &nd);
+        ++vertex;
+        finished = r == VERTEX_DONE || vertex > max_bounces(P) || maxc(s.thr) < kThroughputEps;
+        if (nd.any) {
+          flags |= WF_NEE;
+          B.nee_org[path] = st3(nd.org);
+          B.nee_thr[path] = st_rad(nd.thr);
+          B.nee_extra[path] = st_rad(nd.extra);
+          for (int l = 0; l < 2; ++l)
+            if (nd.pending[l]) {
+              flags |= (l == 0 ? WF_NEE_SKY : WF_NEE_SUN);
+              B.nee_dir[l][path] = st3(nd.dir[l], nd.dist[l]);
+              B.nee_c[l][path] = st_rad(nd.c[l]);
+              B.nee_li[l][path] = st_rad(nd.li[l]);
+              push_shadow |= 1 << l;
+            }
+          if (finished) flags |= WF_FINISHING;  // one more pass to resolve the shadows
+          finished = false;
+        }
+        info.x = vertex;
+      }
+      s.inDiele ? (flags |= WF_INDIELE) : (flags &= ~WF_INDIELE);
+      if (finished) {
+        finish_path(J, B, path, s.L, ld3(B.xyzw[path]), g);
+      } else {
+        B.pos[path] = st3(s.pW);
+        B.dir[path] = st3(s.rayDir);
+        B.thr[path] = st_rad(s.thr);
+        B.rad[path] = st_rad(s.L);
+        B.mis[path] = make_float4(s.misSky, s.misSun, s.misSph, 0.0f);
+        B.info[path] = make_int4(info.x, s.atmScatters, flags, 0);
+        B.rng[path] = make_uint4(g.s[0], g.s[1], g.s[2], g.s[3]);
+        push_active = true;
+      }
+    }
+    int slot = warp_append(cnt + WF_A + nxt, push_active);
+    if (slot >= 0) B.qa[nxt][slot] = path;
+    for (int l = 0; l < 2; ++l) {
+      int ss = warp_append(cnt + WF_S + nxt, (push_shadow >> l) & 1);
+      if (ss >= 0) B.qs[nxt][ss] = 2 * path + l;
+    }
+  }
+}

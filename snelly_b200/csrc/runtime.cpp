@@ -381,12 +381,122 @@ int Context::enqueue_frames(Job& j, int frames) {
   return SNELLY_OK;
 }
 
+// Batched frames (see snelly_advance_batch). Jobs are grouped by module; each group gets a lane
+// (stream + device tables); per frame, one launch covers the group's jobs that still need frames.
+int Context::advance_batch(const std::vector<Job*>& js, const std::vector<int>& frames) {
+  std::map<Module*, std::vector<size_t>> groups;
+  for (size_t k = 0; k < js.size(); ++k)
+    if (frames[k] > 0) groups[js[k]->scene->module.get()].push_back(k);
+  // all earlier work on the main stream (job seeding, single-job frames) comes first
+  cudaEvent_t start;
+  RT_TRY(cudaEventCreateWithFlags(&start, cudaEventDisableTiming));
+  RT_TRY(cudaEventRecord(start, stream));
+  size_t lane_idx = 0;
+  for (auto& g : groups) {
+    Module& m = *g.first;
+    std::vector<size_t>& idx = g.second;
+    // one lane per module: its constant-memory slots are reused chunk after chunk, in order
+    for (size_t c0 = 0; c0 < idx.size(); c0 += SNELLY_MAX_BATCH) {
+      if (lane_idx >= lanes.size()) {
+        BatchLane L;
+        RT_TRY(cudaStreamCreateWithFlags(&L.stream, cudaStreamNonBlocking));
+        RT_TRY(cudaEventCreateWithFlags(&L.done, cudaEventDisableTiming));
+        int rc = alloc(L.recs, SNELLY_MAX_BATCH * sizeof(JobRec) + 4 * (SNELLY_MAX_BATCH + 1) + 256);
+        if (!rc) rc = alloc(L.gparams, SNELLY_MAX_BATCH * sizeof(SnellyParams));
+        if (rc) return rc;
+        lanes.push_back(L);
+      }
+      BatchLane& L = lanes[lane_idx];
+      if (c0 == 0) RT_TRY(cudaStreamWaitEvent(L.stream, start, 0));
+      size_t c1 = std::min(idx.size(), c0 + SNELLY_MAX_BATCH);
+      int maxf = 0;
+      for (size_t q = c0; q < c1; ++q) maxf = std::max(maxf, frames[idx[q]]);
+      // parameter slots: one per job of the chunk
+      for (size_t q = c0; q < c1; ++q) {
+        Job& j = *js[idx[q]];
+        int slot = (int)(q - c0);
+        RT_TRY(cudaMemcpyAsync(m.c_params + slot * sizeof(SnellyParams), &j.params, sizeof(SnellyParams),
+                               cudaMemcpyHostToDevice, L.stream));
+        size_t ub = std::min(j.ublock.size(), m.slot_uniform_bytes);
+        if (ub)
+          RT_TRY(cudaMemcpyAsync(m.c_uniforms + slot * m.slot_uniform_bytes, j.ublock.data(), ub,
+                                 cudaMemcpyHostToDevice, L.stream));
+        RT_TRY(cudaMemcpyAsync((char*)L.gparams.ptr + slot * sizeof(SnellyParams), &j.params, sizeof(SnellyParams),
+                               cudaMemcpyHostToDevice, L.stream));
+      }
+      for (int f = 0; f < maxf; ++f) {
+        std::vector<JobRec> recs;
+        std::vector<int> bs(1, 0);
+        for (size_t q = c0; q < c1; ++q) {
+          Job& j = *js[idx[q]];
+          if (frames[idx[q]] <= f) continue;
+          JobRec r{};
+          r.rng = (uint4*)j.rng.ptr;
+          r.acc = (float4*)j.acc.ptr;
+          r.comp = (float4*)j.comp.ptr;
+          r.acc64 = (double*)j.acc64.ptr;
+          r.out = (float4*)j.out.ptr;
+          r.seed = j.desc.seed;
+          r.width = j.desc.width;
+          r.height = j.desc.height;
+          r.pixel_begin = 0;
+          r.pixel_count = j.desc.width * j.desc.height;
+          r.slot = (int)(q - c0);
+          r.mode = j.desc.mode;
+          recs.push_back(r);
+          bs.push_back(bs.back() + (r.pixel_count + SNELLY_BLOCK - 1) / SNELLY_BLOCK);
+        }
+        // the tables are rewritten for every frame: the copy is ordered after the previous launch
+        RT_TRY(cudaMemcpyAsync(L.recs.ptr, recs.data(), recs.size() * sizeof(JobRec), cudaMemcpyHostToDevice, L.stream));
+        char* bsp = (char*)L.recs.ptr + SNELLY_MAX_BATCH * sizeof(JobRec);
+        RT_TRY(cudaMemcpyAsync(bsp, bs.data(), bs.size() * sizeof(int), cudaMemcpyHostToDevice, L.stream));
+        void* recp = L.recs.ptr;
+        void* bsv = bsp;
+        int nj = (int)recs.size();
+        void* gp = L.gparams.ptr;
+        void* args[] = {&recp, &bsv, &nj, &gp};
+        RT_TRY(cudaLaunchKernel((const void*)m.f_frame_mega, dim3((unsigned)bs.back()), dim3(SNELLY_BLOCK), args, 0,
+                                L.stream));
+        launches++;
+      }
+      // resolve each job once at the end of the batch (single-job launches on the lane)
+      for (size_t q = c0; q < c1; ++q) {
+        Job& j = *js[idx[q]];
+        void* tables = j.tables.ptr;
+        void* bstart = (char*)j.tables.ptr + 128;
+        int one = 1;
+        void* rargs[] = {&tables, &bstart, &one};
+        RT_TRY(cudaLaunchKernel((const void*)m.f_resolve, dim3((unsigned)j.blocks), dim3(SNELLY_BLOCK), rargs, 0,
+                                L.stream));
+        launches++;
+        j.frames_enqueued += frames[idx[q]];
+      }
+    }
+    BatchLane& L = lanes[lane_idx];
+    RT_TRY(cudaEventRecord(L.done, L.stream));
+    RT_TRY(cudaStreamWaitEvent(stream, L.done, 0));
+    ++lane_idx;
+  }
+  // later main-stream work (and every job's completion event) is ordered after all lanes
+  for (size_t k = 0; k < js.size(); ++k) RT_TRY(cudaEventRecord(js[k]->done, stream));
+  cudaEventDestroy(start);
+  return SNELLY_OK;
+}
+
 Context::~Context() {
   cudaStreamSynchronize(stream);
+  for (auto& L : lanes) {
+    cudaStreamSynchronize(L.stream);
+    release(L.recs);
+    release(L.gparams);
+    cudaEventDestroy(L.done);
+    cudaStreamDestroy(L.stream);
+  }
   for (auto& kv : jobs) free_job(kv.second);
   for (auto& kv : scenes)
     for (auto& t : kv.second.textures) release(t.second);
   release(xyz);
+  release(stats_scratch);
   for (auto& kv : module_cache) cudaLibraryUnload(kv.second->lib);
   cudaStreamDestroy(stream);
 }
@@ -480,7 +590,10 @@ int snelly_create_scene(snelly_ctx* ctx, const char* glsl, const snelly_scene_op
     return rc;
   }
   s.opts = o;
-  s.kernel_mode = o.kernel_mode == SNELLY_KERNEL_WAVEFRONT ? SNELLY_KERNEL_WAVEFRONT : SNELLY_KERNEL_MEGA;
+  // The wavefront integrator serves one sample per pixel per frame (the reference default);
+  // more samples per frame consume one pixel's RNG stream sequentially and use the per-pixel kernel.
+  s.kernel_mode = (o.kernel_mode == SNELLY_KERNEL_WAVEFRONT && o.max_samples_per_frame == 1) ? SNELLY_KERNEL_WAVEFRONT
+                                                                                              : SNELLY_KERNEL_MEGA;
   std::string nvlog;
   rc = c.compile_module(program_source(s.src), o.math_mode, &s.module, &nvlog);
   if (log && log_cap) snprintf(log, log_cap, "%s", rc ? t_last_error.c_str() : nvlog.c_str());
@@ -688,6 +801,26 @@ int snelly_advance(snelly_ctx* ctx, uint64_t job_id, int frames) {
   if (it == c.jobs.end()) return fail(SNELLY_ENOTFOUND, "unknown job id");
   if (it->second.cancelled) return fail(SNELLY_ECANCELLED, "job was cancelled");
   return c.enqueue_frames(it->second, frames);
+}
+
+int snelly_advance_batch(snelly_ctx* ctx, const uint64_t* job_ids, const int* frames, size_t n) {
+  if (!ctx || (n && (!job_ids || !frames))) return fail(SNELLY_EINVAL, "null argument to snelly_advance_batch");
+  Context& c = *ctx->c;
+  std::lock_guard<std::mutex> lk(c.mu);
+  std::vector<Job*> js;
+  std::vector<int> fs;
+  for (size_t k = 0; k < n; ++k) {
+    auto it = c.jobs.find(job_ids[k]);
+    if (it == c.jobs.end()) return fail(SNELLY_ENOTFOUND, "unknown job id in batch");
+    if (it->second.cancelled) return fail(SNELLY_ECANCELLED, "cancelled job in batch");
+    if (frames[k] < 0) return fail(SNELLY_EINVAL, "frames must be >= 0");
+    if (it->second.desc.mode != SNELLY_MODE_PT) return fail(SNELLY_EINVAL, "batches run the path tracer only");
+    for (Job* q : js)
+      if (q == &it->second) return fail(SNELLY_EINVAL, "job listed twice in batch");
+    js.push_back(&it->second);
+    fs.push_back(frames[k]);
+  }
+  return c.advance_batch(js, fs);
 }
 
 static int wait_job(Context& c, Job& j, int flags) {

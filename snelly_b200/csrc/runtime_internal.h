@@ -9,6 +9,7 @@
 #include <vector>
 
 #include "glsl_transform.h"
+#include "kernels/pt_launch.h"
 #include "snelly.h"
 
 #ifndef SNELLY_MAX_BATCH
@@ -63,10 +64,19 @@ struct Job {
   std::vector<unsigned char> ublock;
   DevBuf rng, acc, comp, acc64, out, icdf, env, gparams, tables;
   DevBuf wf;  // wavefront path state and queues
+  WfBuffers wfb{};
   int blocks = 0;
   int frames_enqueued = 0;
   bool cancelled = false;
   cudaEvent_t done = nullptr;
+};
+
+// Device-side tables of a batched launch, one set per batch stream.
+struct BatchLane {
+  cudaStream_t stream = nullptr;
+  cudaEvent_t done = nullptr;
+  DevBuf recs;     // JobRec[SNELLY_MAX_BATCH] + block starts
+  DevBuf gparams;  // SnellyParams[SNELLY_MAX_BATCH]
 };
 
 struct Context {
@@ -82,6 +92,8 @@ struct Context {
   uint64_t next_id = 0;
   uint64_t launches = 0;
   std::string csrc_dir, kernel_dir, include_dir, cache_dir;
+  std::vector<BatchLane> lanes;  // batch streams (created on first use)
+  DevBuf stats_scratch;          // image-statistics partial sums
 
   ~Context();
   int alloc(DevBuf& b, size_t bytes);
@@ -91,6 +103,7 @@ struct Context {
   int upload_slot(Job& j, int slot);
   int single_job_tables(Job& j);
   int enqueue_frames(Job& j, int frames);
+  int advance_batch(const std::vector<Job*>& jobs, const std::vector<int>& frames);
   void free_job(Job& j);
   // wavefront integrator (wavefront.cpp)
   int alloc_wavefront(Job& j);

@@ -56,8 +56,7 @@ def test_null_arguments_rejected():
     assert L.snelly_shutdown(None) == -1
 
 
-@pytest.mark.parametrize("name", sorted(scenes.SCENES))
-@pytest.mark.parametrize("math_mode", [N.MATH_FAST, N.MATH_STRICT])
+@pytest.mark.parametrize("name,math_mode", [(n, N.MATH_FAST) for n in sorted(scenes.SCENES)] + [("c1", N.MATH_STRICT)])
 def test_every_scene_compiles_for_sm100a(name, math_mode):
     h = HostSnelly(scenes.SCENES[name]())
     opts = h.scene_opts()
