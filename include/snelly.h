@@ -159,6 +159,17 @@ int snelly_advance_batch(snelly_ctx* ctx, const uint64_t* job_ids, const int* fr
 #define SNELLY_READ_POLL 2 /* return SNELLY_EBUSY if not done */
 /* Mean XYZ and sample count per pixel: width*height*4 floats (X, Y, Z, N). */
 int snelly_readback(snelly_ctx* ctx, uint64_t job_id, float* out_xyzn, size_t bytes, int flags);
+/* Mean values per pixel of a first-hit job: NORMALS and AO give mean XYZ and the frame count;
+ * PICK gives (first-hit distance or maxLengthScale on a miss, material id, 0, 1) for the ray
+ * through the centre of each pixel (pick-fragment-shader.glsl at every pixel). */
+
+/* First-hit distance and material id (-1 none, 0 dielectric, 1 metal, 2 surface) along the
+ * pinhole camera ray through pixel coordinate (x, y) of a desc->width x desc->height frame, in
+ * gl_FragCoord units: Renderer.prototype.pick (js/renderer.js:398-461, pick-fragment-shader.glsl).
+ * A miss gives maxLengthScale. desc->params supplies the camera; frames/mode are ignored.
+ * Synchronous. */
+int snelly_pick(snelly_ctx* ctx, uint64_t scene_id, const snelly_render_desc* desc, float x, float y, float* distance,
+                float* material);
 /* Complete progressive state (for checkpoint/resume): RNG lanes (4 uint32 per pixel), Kahan sums
  * and compensations (4 floats each per pixel); acc64 (4 doubles per pixel) when enabled, else
  * may be NULL. Waits for the job. */
@@ -196,7 +207,8 @@ int snelly_inverse_cdf(const snelly_spectrum* s, float* out);
 size_t snelly_abi_sizeof(int which);
 
 /* Translate and compile a scene for sm_100a without a device (no module is loaded): a build and
- * test-time check. The NVRTC log goes to `log`, the cubin size to cubin_bytes. */
+ * test-time check. The NVRTC log, with the assembler's per-kernel register, spill and shared
+ * memory report, goes to `log`; the cubin size to cubin_bytes. */
 int snelly_compile_check(const char* scene_glsl, const snelly_scene_opts* opts, char* log, size_t log_cap,
                          size_t* cubin_bytes);
 

@@ -1,7 +1,8 @@
-"""Build the reference's own path tracer shader as a CPU library: oracle/_ref/<key>/libref.so.
+"""Build the reference's own fragment shaders as CPU libraries: oracle/_ref/<key>/libref.so.
 
 TEST INFRASTRUCTURE (the recipe for the reference build). Reads
-shaders/pathtracer-fragment-shader.glsl from a checkout of the reference, applies the same
+shaders/pathtracer-fragment-shader.glsl (or the normals, ao or pick program) from a checkout of
+the reference, applies the same
 source substitutions the reference host applies before compiling it (Renderer.compileShaders,
 js/renderer.js:217-316, via GLU.applyShaderReplacements, js/gl.js:157-168), including the
 __IOR_FUNC__ code that the material objects generate (the JS string builders of
@@ -113,8 +114,14 @@ float K_METAL(float wavelength_nm)
 MODEL_NAMES = {0: "abbe", 1: "sellmeier", 2: "sellmeier2", 3: "polyanskiy", 4: "cauchy"}
 
 
-def shader_source(scene_glsl, opts, diele_model, ncoeffs):
-    src = open(os.path.join(REF_ROOT, "shaders", "pathtracer-fragment-shader.glsl")).read()
+PROGRAMS = ("pathtracer", "normals", "ao", "pick")
+
+
+def shader_source(scene_glsl, opts, diele_model, ncoeffs, program="pathtracer"):
+    """The fragment shader of `program` with the host's substitutions applied (the same set for
+    every program, js/renderer.js:287-316)."""
+    assert program in PROGRAMS
+    src = open(os.path.join(REF_ROOT, "shaders", f"{program}-fragment-shader.glsl")).read()
     full, defs = O.assemble(scene_glsl, opts)
     # the reference host's #define block, without the loop bounds (those are substituted)
     defines = "\n".join(l for l in defs.splitlines() if not l.startswith("#define MAX_"))
@@ -132,22 +139,26 @@ def shader_source(scene_glsl, opts, diele_model, ncoeffs):
     return src
 
 
-def workload_key(scene_glsl, opts, diele_model, ncoeffs):
-    """Identity of a reference build: scene source + compile-time options + dielectric model."""
-    return hashlib.sha1((scene_glsl + repr(bytes(opts)) + f"{diele_model}/{ncoeffs}").encode()).hexdigest()[:16]
+def workload_key(scene_glsl, opts, diele_model, ncoeffs, program="pathtracer"):
+    """Identity of a reference build: scene source + compile-time options + dielectric model
+    (+ the program, for the first-hit programs)."""
+    tag = "" if program == "pathtracer" else "/" + program
+    return hashlib.sha1((scene_glsl + repr(bytes(opts)) + f"{diele_model}/{ncoeffs}{tag}").encode()).hexdigest()[:16]
 
 
 class RefLib:
     """The reference shader for one scene + options, compiled for the CPU."""
 
-    def __init__(self, scene_glsl, opts, diele_model, ncoeffs, name=None):
+    def __init__(self, scene_glsl, opts, diele_model, ncoeffs, name=None, program="pathtracer"):
         """Build (needs the reference checkout) into oracle/_ref/<hash>, or, with `name`, into
-        oracle/_ref/<name> together with a key file so that load() finds it without the reference."""
+        oracle/_ref/<name> together with a key file so that load() finds it without the reference.
+        `program`: the fragment shader to build (pathtracer, normals, ao or pick)."""
         from snelly_b200 import _native
-        src = shader_source(scene_glsl, opts, diele_model, ncoeffs)
+        self.program = program
+        src = shader_source(scene_glsl, opts, diele_model, ncoeffs, program)
         cpp = _native.glsl_to_cpp(src, "RefShader", "  vec4 gl_FragCoord;\n")
         self.cpp = cpp
-        h = hashlib.sha1(cpp.encode())
+        h = hashlib.sha1(cpp.encode() + program.encode())
         for f in (os.path.join(HERE, "ref_harness.cpp"), os.path.join(ROOT, "snelly_b200", "csrc", "glslcompat.h")):
             h.update(open(f, "rb").read())
         d = os.path.join(OUT, name if name else h.hexdigest()[:16])
@@ -164,25 +175,28 @@ class RefLib:
             cmd = ["g++", "-O3", "-march=x86-64-v3", "-ffp-contract=off", "-fno-fast-math", "-fopenmp", "-std=c++17",
                    "-shared", "-fPIC", "-w", "-I" + os.path.join(ROOT, "snelly_b200", "csrc"), "-I" + d,
                    os.path.join(HERE, "ref_harness.cpp"), "-o", so + ".tmp"]
+            if program == "pick":
+                cmd.insert(1, "-DREF_PICK")
             subprocess.run(cmd, check=True)
             os.replace(so + ".tmp", so)
             with open(stamp, "w") as f:
                 f.write(h.hexdigest())
             with open(os.path.join(d, "workload.key"), "w") as f:
-                f.write(workload_key(scene_glsl, opts, diele_model, ncoeffs))
+                f.write(workload_key(scene_glsl, opts, diele_model, ncoeffs, program))
         self._load(so, cpp)
 
     @classmethod
-    def load(cls, name, scene_glsl, opts, diele_model, ncoeffs):
+    def load(cls, name, scene_glsl, opts, diele_model, ncoeffs, program="pathtracer"):
         """A named prebuilt reference library (no reference checkout needed), or None if absent or
         built for another workload."""
         d = os.path.join(OUT, name)
         so, inc, keyf = (os.path.join(d, f) for f in ("libref.so", "ref_shader.inc", "workload.key"))
         if not (os.path.exists(so) and os.path.exists(inc) and os.path.exists(keyf)):
             return None
-        if open(keyf).read() != workload_key(scene_glsl, opts, diele_model, ncoeffs):
+        if open(keyf).read() != workload_key(scene_glsl, opts, diele_model, ncoeffs, program):
             return None
         self = cls.__new__(cls)
+        self.program = program
         self.cpp = open(inc).read()
         self._load(so, self.cpp)
         return self
@@ -191,8 +205,12 @@ class RefLib:
         self.path = so
         L = ctypes.CDLL(so)
         vp, i32, sz = ctypes.c_void_p, ctypes.c_int, ctypes.c_size_t
-        L.ref_render.argtypes = [vp, sz, sz, sz, i32, i32, vp, i32, i32, vp, vp, i32]
-        L.ref_render.restype = i32
+        if self.program == "pick":
+            L.ref_pick.argtypes = [vp, sz, sz, i32, vp, i32, vp, i32]
+            L.ref_pick.restype = i32
+        else:
+            L.ref_render.argtypes = [vp, sz, sz, sz, i32, i32, vp, i32, i32, vp, vp, i32]
+            L.ref_render.restype = i32
         L.ref_block_size.restype = sz
         self.lib = L
         self.layout, self.size = self._layout(cpp)
@@ -236,6 +254,17 @@ class RefLib:
                 buf[off:off + 32] = struct.pack("<Q6i", ptr, w, h, ch, 0, linear, 0)
         return bytes(buf)
 
+    def pick(self, params, scene_calls, tables, width, pixels, threads=0):
+        """The pick program at the centre of each listed pixel: (n, 2) distance and material."""
+        pixels = np.ascontiguousarray(pixels, np.int32)
+        out = np.zeros((len(pixels), 4), np.float32)
+        blk = self.block(params, scene_calls, tables)
+        ub = ctypes.create_string_buffer(blk, len(blk))
+        rc = self.lib.ref_pick(ub, len(blk), self.layout["mousePick"][1], int(width), pixels.ctypes.data, len(pixels),
+                               out.ctypes.data, int(threads))
+        assert rc == 0
+        return out[:, :2].copy()
+
     def render(self, params, scene_calls, tables, width, height, pixels, frames, rng, threads=0):
         pixels = np.ascontiguousarray(pixels, np.int32)
         n = len(pixels)
@@ -250,9 +279,10 @@ class RefLib:
         return mean, rng
 
 
-def ref_for(snelly, name=None, prebuilt_only=False):
+def ref_for(snelly, name=None, prebuilt_only=False, program="pathtracer"):
     """RefLib + table bindings for a host-mirror Snelly object. With `name`, use (or create) the
-    named build in oracle/_ref/<name>; prebuilt_only: never build (returns None if absent)."""
+    named build in oracle/_ref/<name>; prebuilt_only: never build (returns None if absent);
+    program: which fragment shader (pathtracer, normals, ao, pick)."""
     p, keep = O.host_params(snelly)
     xyz, icdf = keep
     metal_n = np.asarray(list(p.metalN), np.float32)
@@ -264,11 +294,11 @@ def ref_for(snelly, name=None, prebuilt_only=False):
         "kTex": (metal_k.ctypes.data, 64, 1, 1, 1),
     }
     args = (snelly.sceneObj.shader(), snelly.scene_opts(), p.dieleModel, p.dieleNumCoeffs)
-    lib = RefLib.load(name, *args) if name else None
+    lib = RefLib.load(name, *args, program=program) if name else None
     if lib is None:
         if prebuilt_only or not os.path.isdir(os.path.join(REF_ROOT, "shaders")):
             return None
-        lib = RefLib(*args, name=name)
+        lib = RefLib(*args, name=name, program=program)
     return lib, p, tables, (xyz, icdf, metal_n, metal_k)
 
 

@@ -173,6 +173,8 @@ class OracleLib:
         vp, i32 = ctypes.c_void_p, ctypes.c_int
         L.oracle_render.argtypes = [vp, vp, i32, i32, vp, i32, i32, vp, vp, vp, i32]
         L.oracle_render.restype = i32
+        L.oracle_firsthit.argtypes = [vp, vp, i32, i32, i32, vp, i32, i32, vp, vp, vp, i32]
+        L.oracle_firsthit.restype = i32
         L.oracle_seed.argtypes = [ctypes.c_uint64, ctypes.c_uint64, vp]
         L.oracle_rand.argtypes = [vp]
         L.oracle_rand.restype = ctypes.c_float
@@ -194,7 +196,8 @@ class OracleLib:
             h.update("".join(flags).encode())
         except OSError:
             pass
-        for f in ("pt_oracle.h", "pt_oracle_bsdf.inc", "pt_oracle_integrator.inc", "oracle_main.cpp", "counted.h"):
+        for f in ("pt_oracle.h", "pt_oracle_bsdf.inc", "pt_oracle_integrator.inc", "fh_oracle.inc", "oracle_main.cpp",
+                  "counted.h"):
             p = os.path.join(HERE, f)
             if os.path.exists(p):
                 h.update(open(p, "rb").read())
@@ -220,6 +223,23 @@ class OracleLib:
         rc = self.lib.oracle_render(ctypes.byref(params), ub, int(width), int(height), pixels.ctypes.data, n,
                                     int(frames), rng.ctypes.data, xyz.ctypes.data, mean.ctypes.data, int(threads))
         assert rc == 0
+        return xyz, mean, rng
+
+    def firsthit(self, mode, params, uniforms, width, height, pixels, frames, rng=None, threads=0):
+        """First-hit programs: mode 1 normals, 2 ambient occlusion (returns xyz_sum, running mean,
+        final rng as render() does), 3 pick (returns (n, 2) distance and material at the pixel
+        centres)."""
+        pixels = np.ascontiguousarray(pixels, np.int32)
+        n = len(pixels)
+        rng = np.ascontiguousarray(rng if rng is not None else np.ones((n, 4)), np.uint32).copy()
+        xyz = np.zeros((n, 3), np.float64)
+        mean = np.zeros((n, 4), np.float32)
+        ub = ctypes.create_string_buffer(bytes(uniforms), max(1, len(uniforms)))
+        rc = self.lib.oracle_firsthit(ctypes.byref(params), ub, int(mode), int(width), int(height), pixels.ctypes.data,
+                                      n, int(frames), rng.ctypes.data, xyz.ctypes.data, mean.ctypes.data, int(threads))
+        assert rc == 0
+        if mode == 3:
+            return mean[:, :2].copy()
         return xyz, mean, rng
 
 

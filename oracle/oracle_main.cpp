@@ -111,4 +111,64 @@ int oracle_render(const SnellyParams* P, const void* uniforms, int width, int he
   return 0;
 }
 
+// One frame per call of the first-hit programs for the listed pixels: mode 1 normals
+// (NM:293-345), 2 ambient occlusion (AO:395-488), both updating rng, xyz_sum and the running mean
+// as oracle_render does; mode 3 pick (PK:133-152) at each pixel centre, writing
+// (distance, material, 0, 0) to mean (rng and xyz_sum untouched).
+int oracle_firsthit(const SnellyParams* P, const void* uniforms, int mode, int width, int height, const int* pixels,
+                    int n, int frames, uint32_t* rng, double* xyz_sum, float* mean, int threads) {
+  (void)height;
+  if (mode < 1 || mode > 3) return -1;
+  const glsl::SceneUniforms& U = *reinterpret_cast<const glsl::SceneUniforms*>(uniforms);
+#ifdef _OPENMP
+  if (threads > 0) omp_set_num_threads(threads);
+#pragma omp parallel for schedule(dynamic, 16)
+#endif
+  for (int k = 0; k < n; ++k) {
+    int idx = pixels[k];
+    int x = idx % width, y = idx / width;
+    glsl::vec2 pixel(float(x) + 0.5f, float(y) + 0.5f);
+    if (mode == 3) {
+      glsl::Scene sc(U);
+      sc.INIT();
+      oracle::Invocation inv(*P, sc);
+      glsl::vec2 r = inv.pick(pixel);
+      mean[4 * k + 0] = glsl::s_tofloat(r.x);
+      mean[4 * k + 1] = glsl::s_tofloat(r.y);
+      mean[4 * k + 2] = 0.0f;
+      mean[4 * k + 3] = 0.0f;
+      continue;
+    }
+    glsl::vec4 rnd((float)rng[4 * k + 0], (float)rng[4 * k + 1], (float)rng[4 * k + 2], (float)rng[4 * k + 3]);
+    for (int f = 0; f < frames; ++f) {
+      glsl::Scene sc(U);
+      oracle::Invocation inv(*P, sc);
+      glsl::vec3 c;
+      bool skipped = false;
+      if (mode == 1) {
+        sc.INIT();
+        c = inv.normals(pixel, rnd);
+      } else {
+        // AO:397-414: the interactive-mode skip comes before INIT()
+        c = inv.ao_frame(pixel, rnd, skipped);
+      }
+      if (skipped) continue;
+      float cx = glsl::s_tofloat(c.x), cy = glsl::s_tofloat(c.y), cz = glsl::s_tofloat(c.z);
+      xyz_sum[3 * k + 0] += (double)cx;
+      xyz_sum[3 * k + 1] += (double)cy;
+      xyz_sum[3 * k + 2] += (double)cz;
+      float oldN = mean[4 * k + 3], newN = oldN + 1.0f;
+      mean[4 * k + 0] = (oldN * mean[4 * k + 0] + cx) / newN;
+      mean[4 * k + 1] = (oldN * mean[4 * k + 1] + cy) / newN;
+      mean[4 * k + 2] = (oldN * mean[4 * k + 2] + cz) / newN;
+      mean[4 * k + 3] = newN;
+    }
+    rng[4 * k + 0] = (uint32_t)glsl::s_tofloat(rnd.x);
+    rng[4 * k + 1] = (uint32_t)glsl::s_tofloat(rnd.y);
+    rng[4 * k + 2] = (uint32_t)glsl::s_tofloat(rnd.z);
+    rng[4 * k + 3] = (uint32_t)glsl::s_tofloat(rnd.w);
+  }
+  return 0;
+}
+
 }  // extern "C"

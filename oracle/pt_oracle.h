@@ -1,5 +1,6 @@
 // pt_oracle.h - CPU oracle: a sequential restatement of the reference's spectral path tracer,
-// shaders/pathtracer-fragment-shader.glsl (cited PT:line), for checking the CUDA path tracer.
+// shaders/pathtracer-fragment-shader.glsl (cited PT:line), and of its first-hit programs
+// (fh_oracle.inc), for checking the CUDA kernels.
 //
 // TEST INFRASTRUCTURE. This file is compiled only into the oracle library that tests and the
 // benchmark's CPU-baseline leg load; the product never includes or links it.
@@ -243,6 +244,7 @@ struct Invocation {
 
 #include "pt_oracle_bsdf.inc"
 #include "pt_oracle_integrator.inc"
+#include "fh_oracle.inc"
 };
 
 }  // namespace oracle

@@ -1,5 +1,6 @@
-// ref_harness.cpp - runs the reference's own path tracer fragment shader (translated to C++ by
-// oracle/build_ref.py into ref_shader.inc) once per pixel and frame on the CPU.
+// ref_harness.cpp - runs one of the reference's own fragment shaders (translated to C++ by
+// oracle/build_ref.py into ref_shader.inc) once per pixel and frame on the CPU: the path tracer,
+// normals and ambient-occlusion programs through ref_render, the pick program through ref_pick.
 //
 // TEST INFRASTRUCTURE: part of the oracle/_ref build recipe.
 #include <cstdint>
@@ -15,6 +16,35 @@ namespace glsl {
 }
 
 extern "C" size_t ref_block_size(void) { return sizeof(glsl::RefShaderUniforms); }
+
+#ifdef REF_PICK
+// The pick program (built with -DREF_PICK): one invocation per listed pixel with mousePick at the
+// pixel centre; out: gbuf_pick (distance, material, 0, 0) per pixel.
+extern "C" int ref_pick(const void* block, size_t block_bytes, size_t off_mouse, int width, const int* pixels, int n,
+                        float* out, int threads) {
+  if (block_bytes != sizeof(glsl::RefShaderUniforms)) return -1;
+#ifdef _OPENMP
+  if (threads > 0) omp_set_num_threads(threads);
+#endif
+#pragma omp parallel
+  {
+    std::vector<unsigned char> local(block_bytes + 16);
+    unsigned char* lb = local.data();
+#pragma omp for schedule(dynamic, 16)
+    for (int k = 0; k < n; ++k) {
+      std::memcpy(lb, block, block_bytes);
+      int idx = pixels[k], x = idx % width, y = idx / width;
+      float mp[2] = {float(x) + 0.5f, float(y) + 0.5f};
+      std::memcpy(lb + off_mouse, mp, sizeof mp);
+      glsl::RefShader sh(*reinterpret_cast<const glsl::RefShaderUniforms*>(lb));
+      sh.gl_FragCoord = glsl::vec4(0.5f, 0.5f, 0.5f, 1.0f);
+      sh.main();
+      for (int c = 0; c < 4; ++c) out[4 * k + c] = sh.gbuf_pick[c];
+    }
+  }
+  return 0;
+}
+#else
 
 // block: the uniform block (samplers included); off_radiance / off_rng: offsets of the Radiance
 // and RngData sampler records, re-pointed for each pixel at a 1x1 NEAREST texture holding that
@@ -61,3 +91,4 @@ extern "C" int ref_render(const void* block, size_t block_bytes, size_t off_radi
   }
   return 0;
 }
+#endif  // REF_PICK

@@ -122,6 +122,8 @@ def lib():
         "snelly_advance_batch": (i32, [vp, P(u64), P(i32), sz]),
         "snelly_readback": (i32, [vp, u64, vp, sz, i32]),
         "snelly_readback_state": (i32, [vp, u64, vp, vp, vp, vp]),
+        "snelly_pick": (i32, [vp, u64, P(RenderDesc), ctypes.c_float, ctypes.c_float, P(ctypes.c_float),
+                              P(ctypes.c_float)]),
         "snelly_restore": (i32, [vp, u64, P(RenderDesc), vp, vp, vp, P(u64)]),
         "snelly_job_status": (i32, [vp, u64, P(i32), P(i32)]),
         "snelly_cancel": (i32, [vp, u64]),

@@ -402,6 +402,21 @@ class Renderer:
     def getSPP(self):
         return self.spp
 
+    def pick(self, xPick, yPick):
+        """First-hit distance and material along the camera ray through pixel coordinate
+        (xPick, yPick) of the frame (Renderer.prototype.pick, js/renderer.js:398-461)."""
+        return self._snelly.pick(xPick, yPick)
+
+    def focusAt(self, x, y):
+        """Set the camera's focal distance to the first hit under the frame fraction (x, y)
+        (Renderer.prototype.focusAt, js/renderer.js:391-396, whose body reads undefined names and
+        never sets the focal distance; this does what its documentation states)."""
+        s = self._snelly
+        hit = self.pick(x * s.width, y * s.height)
+        if hit["material"] >= 0:
+            s.camera.focalDistance = math.log10(max(hit["distance"], 1.0e-30) / max(s.lengthScale, 1.0e-30))
+        return hit
+
 
 class Snelly:
     """The application facade of js/snelly.js, headless: one GPU context and one scene."""
@@ -571,7 +586,8 @@ class Snelly:
         d = N.RenderDesc()
         d.width, d.height = int(self.width), int(self.height)
         d.frames = int(frames)
-        d.mode = {"pt": N.MODE_PT, "normals": N.MODE_NORMALS, "ao": N.MODE_AO}.get(self.pathtracer.renderMode, N.MODE_PT)
+        d.mode = {"pt": N.MODE_PT, "normals": N.MODE_NORMALS, "ao": N.MODE_AO,
+                  "pick": N.MODE_PICK}.get(self.pathtracer.renderMode, N.MODE_PT)
         d.seed = int(self.seed)
         d.params = self.uniform_params()
         d.spectrum = self.spectrumObj.native()
@@ -602,6 +618,14 @@ class Snelly:
         r.spp += frames * int(round(r.maxSamplesPerFrame))
         if hasattr(self.sceneObj, "postframeCallback"):
             self.sceneObj.postframeCallback(self, None)
+
+    def pick(self, xPick, yPick):
+        """Renderer.pick: {"distance", "material"} of the first hit along the pinhole ray through
+        pixel coordinate (xPick, yPick) (gl_FragCoord units; a miss gives maxLengthScale and -1)."""
+        sid = self.compileShaders()
+        self._ctx.set_uniforms(sid, self.scene_uniforms())
+        d, m = self._ctx.pick(sid, self.render_desc(1), xPick, yPick)
+        return {"distance": d, "material": m}
 
     def readback(self, out=None):
         """(H, W, 4) float32 array: mean X, Y, Z and sample count; row 0 is the bottom row."""
@@ -703,6 +727,12 @@ class Context:
         ids = (ctypes.c_uint64 * len(jobs_frames))(*jobs_frames.keys())
         fr = (ctypes.c_int * len(jobs_frames))(*jobs_frames.values())
         N.check(self._lib.snelly_advance_batch(self._h, ids, fr, len(jobs_frames)))
+
+    def pick(self, sid, desc, x, y):
+        d, m = ctypes.c_float(), ctypes.c_float()
+        N.check(self._lib.snelly_pick(self._h, sid, ctypes.byref(desc), float(x), float(y), ctypes.byref(d),
+                                      ctypes.byref(m)))
+        return d.value, m.value
 
     def readback(self, jid, width, height, out=None, poll=False):
         if out is None:

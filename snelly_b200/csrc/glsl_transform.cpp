@@ -282,6 +282,26 @@ std::string rewrite_tokens(const std::vector<Tok>& t, size_t b, size_t e) {
             }
           }
         }
+        // GLSL evaluates call arguments left to right; C++ leaves the order of constructor
+        // arguments unspecified. Vector/matrix constructors whose arguments call rand() (the
+        // one side-effecting call scenes make) become braced initialisations, which are
+        // evaluated in order.
+        {
+          static const std::set<std::string> ctors = {"vec2", "vec3", "vec4", "mat2", "mat3", "mat4"};
+          size_t j = next_sig(t, i + 1);
+          if (ctors.count(s) && j < e && t[j].k == T_PUNCT && t[j].s == "(") {
+            size_t jc = match_close(t, j);
+            bool calls_rand = false;
+            for (size_t q = j + 1; q < jc && q < e; ++q)
+              if (t[q].k == T_IDENT && t[q].s == "rand") calls_rand = true;
+            if (calls_rand && jc < e) {
+              out += name + "{";
+              replace_close.insert(jc);
+              i = j;
+              break;
+            }
+          }
+        }
         out += name;
         if (pending_ref) {
           // the first identifier after out/inout (skipping const) is the parameter type

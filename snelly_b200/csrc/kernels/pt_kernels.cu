@@ -111,6 +111,7 @@ extern "C" __global__ void __launch_bounds__(SNELLY_BLOCK) snelly_frame_mega(con
 }
 
 #include "pt_wavefront.cuh"
+#include "pt_firsthit.cuh"
 
 // Mean XYZ and sample count per pixel into `out` (float4), for readback.
 extern "C" __global__ void __launch_bounds__(SNELLY_BLOCK) snelly_resolve(const JobRec* __restrict__ jobs, const int* __restrict__ block_start,

@@ -3,6 +3,12 @@
 
 #define SNELLY_BLOCK 128  // threads per block of the per-pixel kernels
 
+// Render modes (the values of SNELLY_MODE_* in snelly.h).
+#define JOB_MODE_PT 0
+#define JOB_MODE_NORMALS 1
+#define JOB_MODE_AO 2
+#define JOB_MODE_PICK 3
+
 // One job's slice of a batched launch. Pointers are device addresses of the job's SoA buffers.
 typedef struct JobRec {
   uint4* rng;            // 4 LCG lanes per pixel
@@ -16,6 +22,8 @@ typedef struct JobRec {
   int pixel_count;       // pixels covered by this launch
   int slot;              // index into the module's constant-memory parameter banks
   int mode;              // SNELLY_MODE_*
+  int pick_at;           // pick mode: trace the single pixel coordinate (pick_x, pick_y)
+  float pick_x, pick_y;  // (gl_FragCoord units of a frame of params.resolution)
 } JobRec;
 
 // Wavefront path state and queues of one job (structure of arrays, one element per path =

@@ -17,8 +17,8 @@
 #include "pt_integrator.cuh"
 #include "pt_launch.h"
 
-#ifndef WF_CHUNK
-#define WF_CHUNK 8  // march steps between refills
+#ifndef WF_REFILL
+#define WF_REFILL 4  // idle lanes of a warp that trigger a refill from the work head
 #endif
 #define WF_FULL 0xffffffffu
 
@@ -125,6 +125,11 @@ extern "C" __global__ void __launch_bounds__(SNELLY_BLOCK) snelly_wf_generate(co
 }
 
 // Trace the active continuation rays and the pending shadow rays of iteration `it`.
+//
+// Every pass of the loop evaluates the scene SDFs once for every lane that holds a ray; a ray's
+// first evaluation (at its origin, which fixes the marching sign, PT:888-900) is such a pass too,
+// so refilled lanes march in step with the rest of the warp. Idle lanes are refilled from the
+// global work head when at least WF_REFILL of them are idle, or when none of the warp is busy.
 extern "C" __global__ void __launch_bounds__(SNELLY_BLOCK) snelly_wf_extend(WfBuffers B, int it) {
   using namespace sdev;
   const SnellyParams& P = c_params[0];
@@ -144,18 +149,19 @@ extern "C" __global__ void __launch_bounds__(SNELLY_BLOCK) snelly_wf_extend(WfBu
   const float minMarch = P.minLengthScale;
   const float maxLen = P.maxLengthScale;
 
-  bool has = false, exhausted = false;
+  bool has = false, exhausted = false, first = false;
   int path = 0, sidx = -1;  // sidx >= 0: a shadow ray
   vec3 o(0.0f), d(0.0f);
   float t = 0.0f, sgn = 1.0f, maxd = 0.0f;
   int n = 0;
   for (;;) {
-    // ---- refill idle lanes ----------------------------------------------------------------
-    bool want = !has && !exhausted;
-    unsigned need = __ballot_sync(WF_FULL, want);
     bool done = false, res_hit = false, finishing = false;
     int res_mat = MAT_INVAL;
-    if (need) {
+    // ---- refill idle lanes ----------------------------------------------------------------
+    const bool want = !has && !exhausted;
+    const unsigned need = __ballot_sync(WF_FULL, want);
+    const unsigned busy = __ballot_sync(WF_FULL, has);
+    if (need && (__popc(need) >= WF_REFILL || !busy)) {
       int leader = __ffs(need) - 1;
       int base = 0;
       if ((int)(threadIdx.x & 31) == leader) base = atomicAdd(cnt + WF_HEAD + it, __popc(need));
@@ -175,6 +181,7 @@ extern "C" __global__ void __launch_bounds__(SNELLY_BLOCK) snelly_wf_extend(WfBu
             d = ld3(B.dir[path]);
             maxd = maxLen;
             has = true;
+            first = true;
           }
         } else {
           sidx = qs[w - nA];
@@ -184,89 +191,79 @@ extern "C" __global__ void __launch_bounds__(SNELLY_BLOCK) snelly_wf_extend(WfBu
           d = ld3(dd);
           maxd = dd.w;
           has = true;
-        }
-        if (has) {  // first distance at the ray origin (PT:888-900)
-          float sdf = 1.0e20f;
-#ifdef HAS_SURFACE
-          sdf = fminf(sdf, fabsf(sc.SDF_SURFACE(o)));
-#endif
-#ifdef HAS_METAL
-          sdf = fminf(sdf, fabsf(sc.SDF_METAL(o)));
-#endif
-#ifdef HAS_DIELECTRIC
-          sdf = fminf(sdf, fabsf(sc.SDF_DIELECTRIC(o)));
-#endif
-          sgn = glsl::sign(sdf);
-          t = sgn * sdf;
-          n = 0;
-          if (fabsf(t) >= maxd) {
-            done = true;
-            res_hit = false;
-          }
+          first = true;
         }
       }
     }
-    // ---- march (PT:901-919) ------------------------------------------------------------------
-    for (int k = 0; k < WF_CHUNK && has && !done; ++k) {
-      vec3 p = o + t * d;
+    // ---- one sphere-tracing step (PT:888-919) -------------------------------------------------
+    if (has) {
+      const vec3 p = first ? o : o + t * d;
       float sdf = 1.0e20f;
       int m = MAT_INVAL;
 #ifdef HAS_SURFACE
       {
         float dd = fabsf(sc.SDF_SURFACE(p));
-        if (dd < minMarch) m = MAT_SURFA;
+        if (!first && dd < minMarch) m = MAT_SURFA;
         sdf = fminf(sdf, dd);
       }
 #endif
 #ifdef HAS_METAL
       if (m == MAT_INVAL) {
         float dd = fabsf(sc.SDF_METAL(p));
-        if (dd < minMarch) m = MAT_METAL;
+        if (!first && dd < minMarch) m = MAT_METAL;
         sdf = fminf(sdf, dd);
       }
 #endif
 #ifdef HAS_DIELECTRIC
       if (m == MAT_INVAL) {
         float dd = fabsf(sc.SDF_DIELECTRIC(p));
-        if (dd < minMarch) m = MAT_DIELE;
+        if (!first && dd < minMarch) m = MAT_DIELE;
         sdf = fminf(sdf, dd);
       }
 #endif
-      if (m != MAT_INVAL) {
+      if (first) {  // the distance at the origin fixes the marching sign and the first step
+        first = false;
+        sgn = glsl::sign(sdf);
+        t = sgn * sdf;
+        n = 0;
+        if (fabsf(t) >= maxd) {
+          done = true;
+          res_hit = false;
+        }
+      } else if (m != MAT_INVAL) {
         done = true;
         res_hit = true;
         res_mat = m;
-        break;
-      }
-      t += sgn * sdf;
-      if (fabsf(t) >= maxd) {
-        done = true;
-        res_hit = false;
-        break;
-      }
-      if (++n >= MAX_MARCH_STEPS) {  // out of steps: a hit at the zero position unless maxStepsIsMiss
-        done = true;
-        res_hit = !P.maxStepsIsMiss;
-        res_mat = MAT_INVAL;
-        t = 0.0f;
-        o = vec3(0.0f);
-        d = vec3(0.0f);
-        break;
+      } else {
+        t += sgn * sdf;
+        if (fabsf(t) >= maxd) {
+          done = true;
+          res_hit = false;
+        } else if (++n >= MAX_MARCH_STEPS) {  // out of steps: a hit at the zero position unless maxStepsIsMiss
+          done = true;
+          res_hit = !P.maxStepsIsMiss;
+          res_mat = MAT_INVAL;
+          t = 0.0f;
+          o = vec3(0.0f);
+          d = vec3(0.0f);
+        }
       }
     }
     // ---- results ---------------------------------------------------------------------------
-    bool cont_result = done && sidx < 0;
-    int seg = -1;
-    if (cont_result) {
-      if (!finishing) B.hit[path] = st3(o + t * d, enc_hit(res_hit, res_mat));
-      seg = (finishing || !res_hit) ? 0 : (res_mat == MAT_SURFA ? 1 : (res_mat == MAT_METAL ? 2 : (res_mat == MAT_DIELE ? 3 : 0)));
+    if (__any_sync(WF_FULL, done)) {
+      const bool cont_result = done && sidx < 0;
+      int seg = -1;
+      if (cont_result) {
+        if (!finishing) B.hit[path] = st3(o + t * d, enc_hit(res_hit, res_mat));
+        seg = (finishing || !res_hit) ? 0 : (res_mat == MAT_SURFA ? 1 : (res_mat == MAT_METAL ? 2 : (res_mat == MAT_DIELE ? 3 : 0)));
+      }
+      if (done && sidx >= 0) B.shadow[sidx] = res_hit ? 1 : 0;
+      for (int sgi = 0; sgi < 4; ++sgi) {
+        int slot = warp_append(qcnt + sgi, seg == sgi);
+        if (slot >= 0) B.qshade[sgi * B.paths + slot] = path;
+      }
+      if (done) has = false;
     }
-    if (done && sidx >= 0) B.shadow[sidx] = res_hit ? 1 : 0;
-    for (int sgi = 0; sgi < 4; ++sgi) {
-      int slot = warp_append(qcnt + sgi, seg == sgi);
-      if (slot >= 0) B.qshade[sgi * B.paths + slot] = path;
-    }
-    if (done) has = false;
     if (__all_sync(WF_FULL, exhausted && !has)) break;
   }
 }

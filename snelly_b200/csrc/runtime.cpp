@@ -343,6 +343,9 @@ int Context::single_job_tables(Job& j) {
   r.pixel_count = j.desc.width * j.desc.height;
   r.slot = 0;
   r.mode = j.desc.mode;
+  r.pick_at = j.pick_at;
+  r.pick_x = j.pick_x;
+  r.pick_y = j.pick_y;
   int bs[2] = {0, (r.pixel_count + SNELLY_BLOCK - 1) / SNELLY_BLOCK};
   RT_TRY(cudaMemcpyAsync(j.tables.ptr, &r, sizeof r, cudaMemcpyHostToDevice, stream));
   RT_TRY(cudaMemcpyAsync((char*)j.tables.ptr + 128, bs, sizeof bs, cudaMemcpyHostToDevice, stream));
@@ -692,8 +695,14 @@ int snelly_set_texture(snelly_ctx* ctx, uint64_t scene_id, const char* name, con
   return SNELLY_OK;
 }
 
+// A one-pixel job of snelly_pick: the pixel coordinate and the frame it belongs to.
+struct PickAt {
+  float x, y;
+  int width, height;
+};
+
 static int start_job(Context& c, uint64_t scene_id, const snelly_render_desc* desc, const uint32_t* rng,
-                     const float* acc, const float* comp, uint64_t* job_id) {
+                     const float* acc, const float* comp, uint64_t* job_id, const PickAt* pick = nullptr) {
   auto it = c.scenes.find(scene_id);
   if (it == c.scenes.end()) return fail(SNELLY_ENOTFOUND, "unknown scene id");
   if (desc->width < 1 || desc->height < 1 || (long long)desc->width * desc->height > (1ll << 30))
@@ -713,6 +722,13 @@ static int start_job(Context& c, uint64_t scene_id, const snelly_render_desc* de
   j.params = desc->params;
   j.params.resolution[0] = (float)desc->width;
   j.params.resolution[1] = (float)desc->height;
+  if (pick) {
+    j.params.resolution[0] = (float)pick->width;
+    j.params.resolution[1] = (float)pick->height;
+    j.pick_at = 1;
+    j.pick_x = pick->x;
+    j.pick_y = pick->y;
+  }
   j.ublock = s.ublock;
   size_t npix = (size_t)desc->width * desc->height;
   int rc;
@@ -749,7 +765,8 @@ static int start_job(Context& c, uint64_t scene_id, const snelly_render_desc* de
   if (cudaEventCreateWithFlags(&j.done, cudaEventDisableTiming) != cudaSuccess)
     return bail(fail(SNELLY_EDEVICE, "event creation failed"));
   if ((rc = c.single_job_tables(j))) return bail(rc);
-  if (s.kernel_mode == SNELLY_KERNEL_WAVEFRONT && (rc = c.alloc_wavefront(j))) return bail(rc);
+  if (s.kernel_mode == SNELLY_KERNEL_WAVEFRONT && desc->mode == SNELLY_MODE_PT && (rc = c.alloc_wavefront(j)))
+    return bail(rc);
   if (rng) {
     if (cudaMemcpy(j.rng.ptr, rng, npix * 16, cudaMemcpyHostToDevice) != cudaSuccess ||
         cudaMemcpy(j.acc.ptr, acc, npix * 16, cudaMemcpyHostToDevice) != cudaSuccess ||
@@ -853,6 +870,35 @@ int snelly_readback(snelly_ctx* ctx, uint64_t job_id, float* out, size_t bytes, 
   return SNELLY_OK;
 }
 
+int snelly_pick(snelly_ctx* ctx, uint64_t scene_id, const snelly_render_desc* desc, float x, float y, float* distance,
+                float* material) {
+  if (!ctx || !desc || !distance || !material) return fail(SNELLY_EINVAL, "null argument to snelly_pick");
+  if (desc->width < 1 || desc->height < 1) return fail(SNELLY_EINVAL, "bad image size");
+  Context& c = *ctx->c;
+  std::lock_guard<std::mutex> lk(c.mu);
+  snelly_render_desc d = *desc;
+  d.width = d.height = 1;
+  d.frames = 1;
+  d.mode = SNELLY_MODE_PICK;
+  d.accum_fp64 = 0;
+  PickAt pa{x, y, desc->width, desc->height};
+  uint64_t id = 0;
+  int rc = start_job(c, scene_id, &d, nullptr, nullptr, nullptr, &id, &pa);
+  if (rc) return rc;
+  Job& j = c.jobs[id];
+  float r[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+  rc = wait_job(c, j, SNELLY_READ_WAIT);
+  if (!rc && (cudaMemcpyAsync(r, j.out.ptr, sizeof r, cudaMemcpyDeviceToHost, c.stream) != cudaSuccess ||
+              cudaStreamSynchronize(c.stream) != cudaSuccess))
+    rc = fail(SNELLY_EDEVICE, "pick readback failed");
+  c.free_job(j);
+  c.jobs.erase(id);
+  if (rc) return rc;
+  *distance = r[0];
+  *material = r[1];
+  return SNELLY_OK;
+}
+
 int snelly_readback_state(snelly_ctx* ctx, uint64_t job_id, uint32_t* rng, float* acc, float* comp, double* acc64) {
   if (!ctx) return fail(SNELLY_EINVAL, "ctx is null");
   Context& c = *ctx->c;
@@ -949,7 +995,9 @@ int snelly_compile_check(const char* glsl, const snelly_scene_opts* opts, char* 
   std::string inc = env ? std::string(env) + "/../../include" : dir + "/../include";
   std::vector<char> cubin;
   std::string lg;
-  rc = nvrtc_cubin(program_source(ss), nvrtc_options(csrc + "/kernels", csrc, inc, opts->math_mode), &cubin, &lg);
+  std::vector<std::string> nopts = nvrtc_options(csrc + "/kernels", csrc, inc, opts->math_mode);
+  nopts.push_back("--ptxas-options=-v");  // the log then lists registers, spills and shared memory per kernel
+  rc = nvrtc_cubin(program_source(ss), nopts, &cubin, &lg);
   if (log && log_cap) snprintf(log, log_cap, "%s", rc ? t_last_error.c_str() : lg.c_str());
   if (cubin_bytes) *cubin_bytes = cubin.size();
   return rc;

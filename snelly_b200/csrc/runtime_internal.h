@@ -12,6 +12,11 @@
 #include "kernels/pt_launch.h"
 #include "snelly.h"
 
+static_assert(JOB_MODE_PT == SNELLY_MODE_PT && JOB_MODE_NORMALS == SNELLY_MODE_NORMALS &&
+                  JOB_MODE_AO == SNELLY_MODE_AO && JOB_MODE_PICK == SNELLY_MODE_PICK,
+              "kernel render-mode values follow the ABI's");
+static_assert(sizeof(JobRec) <= 128, "a single-job table holds one JobRec before the block starts at byte 128");
+
 #ifndef SNELLY_MAX_BATCH
 #define SNELLY_MAX_BATCH 32
 #endif
@@ -66,6 +71,8 @@ struct Job {
   DevBuf wf;  // wavefront path state and queues
   WfBuffers wfb{};
   int blocks = 0;
+  int pick_at = 0;           // a one-pixel pick job (snelly_pick)
+  float pick_x = 0.0f, pick_y = 0.0f;
   int frames_enqueued = 0;
   bool cancelled = false;
   cudaEvent_t done = nullptr;

@@ -7,6 +7,10 @@ Run in a checkout that has the reference at /root/reference (or $SNELLY_REFERENC
   built for the CPU by oracle/build_ref.py) rendering a small image of one of the package's
   scenes: inputs (scene case, size, frames, seed, the initial per-pixel RNG lanes) and outputs
   (per-pixel running mean X, Y, Z, N after `frames` frames, final RNG lanes).
+* fh_<case>.npz: the reference's first-hit programs (shaders/normals-fragment-shader.glsl,
+  ao-fragment-shader.glsl, pick-fragment-shader.glsl, built the same way) on the same scenes:
+  normals and AO running means and RNG lanes after a few frames, pick distance and material at
+  every pixel centre. `python tests/golden/make_golden.py fh` regenerates only these.
 * cie_csv.npy: the CIE XYZ table recomputed from scripts/color/lin2012xyz2e_fine_7sf.csv as
   scripts/color/cie.py does (linear interpolation to 1024 samples over 390..750 nm, both ends
   included), to pin the table in snelly_b200/data/materials.json.
@@ -52,6 +56,30 @@ def make_pt(name):
     print(f"pt_{name}: {h.width}x{h.height}, {frames} frames, mean XYZ {mean[:, :3].mean(0)}")
 
 
+FH_CASES = ("c0", "c1", "c2", "atmosphere", "hooks")
+FH_FRAMES = 3
+
+
+def make_firsthit(name):
+    """fh_<case>.npz: the reference's normals and ambient-occlusion programs (FH_FRAMES frames,
+    running mean and final RNG lanes) and its pick program at every pixel centre."""
+    factory, _ = CASES[name]
+    h = HostSnelly(factory())
+    lib = oracle.OracleLib(h.sceneObj.shader(), h.scene_opts())
+    pix = np.arange(h.width * h.height)
+    rng0 = lib.seed(SEED, pix)
+    out = dict(case=name, width=h.width, height=h.height, frames=FH_FRAMES, seed=SEED, rng0=rng0)
+    for prog in ("normals", "ao"):
+        ref, p, tables, keep = build_ref.ref_for(h, program=prog)
+        mean, rng = ref.render(p, h.scene_uniforms(), tables, h.width, h.height, pix, FH_FRAMES, rng0)
+        out[prog + "_mean"] = mean
+        out[prog + "_rng"] = rng
+    ref, p, tables, keep = build_ref.ref_for(h, program="pick")
+    out["pick"] = ref.pick(p, h.scene_uniforms(), tables, h.width, pix)
+    np.savez_compressed(os.path.join(HERE, f"fh_{name}.npz"), **out)
+    print(f"fh_{name}: {h.width}x{h.height}, normals/ao {FH_FRAMES} frames, pick hits {(out['pick'][:, 1] >= 0).mean():.3f}")
+
+
 def make_cie():
     path = os.path.join(build_ref.REF_ROOT, "scripts", "color", "lin2012xyz2e_fine_7sf.csv")
     rows = [r for r in csv.reader(open(path))]
@@ -64,6 +92,12 @@ def make_cie():
 
 
 if __name__ == "__main__":
-    make_cie()
+    only = sys.argv[1:]
+    if not only or "cie" in only:
+        make_cie()
     for n in CASES:
-        make_pt(n)
+        if not only or "pt" in only:
+            make_pt(n)
+    for n in FH_CASES:
+        if not only or "fh" in only:
+            make_firsthit(n)

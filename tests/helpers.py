@@ -19,8 +19,26 @@ CASES = {
 }
 
 
+FH_CASES = ("c0", "c1", "c2", "atmosphere", "hooks")
+
+
 def golden(name):
     return dict(np.load(os.path.join(GOLDEN, f"pt_{name}.npz")))
+
+
+def golden_fh(name):
+    return dict(np.load(os.path.join(GOLDEN, f"fh_{name}.npz")))
+
+
+def oracle_firsthit(host, mode, pixels, frames, rng0=None, threads=0):
+    """The oracle's first-hit programs (mode 1 normals, 2 AO, 3 pick) for the listed pixels."""
+    import oracle
+    lib = oracle_for(host)
+    if rng0 is None and mode != 3:
+        rng0 = lib.seed(host.seed, pixels)
+    p, keep = oracle.host_params(host)
+    ub = oracle.pack_uniforms(lib.cpp, host.scene_uniforms())
+    return lib.firsthit(mode, p, ub, host.width, host.height, pixels, frames, rng0, threads)
 
 
 def oracle_for(host):

@@ -3,7 +3,7 @@ and its building blocks: RNG, seeding, inverse CDF, tables."""
 import numpy as np
 import pytest
 
-from helpers import CASES, GOLDEN, golden, host, oracle_for, oracle_render
+from helpers import CASES, FH_CASES, GOLDEN, golden, golden_fh, host, oracle_firsthit, oracle_for, oracle_render
 
 
 @pytest.mark.parametrize("name", sorted(CASES))
@@ -16,6 +16,21 @@ def test_oracle_matches_reference_golden(name):
     xyz, mean, rng = oracle_render(h, pix, int(g["frames"]), rng0=g["rng0"])
     np.testing.assert_array_equal(rng, g["rng"])
     np.testing.assert_array_equal(mean, g["mean"])
+
+
+@pytest.mark.parametrize("name", FH_CASES)
+def test_firsthit_oracle_matches_reference_golden(name):
+    """The restatements of the normals, ambient-occlusion and pick programs reproduce the
+    reference's own shaders bit for bit (running means, RNG lanes, pick distance and material)."""
+    g = golden_fh(name)
+    h = host(name)
+    assert (h.width, h.height) == (int(g["width"]), int(g["height"]))
+    pix = np.arange(h.width * h.height)
+    for mode, prog in ((1, "normals"), (2, "ao")):
+        xyz, mean, rng = oracle_firsthit(h, mode, pix, int(g["frames"]), rng0=g["rng0"])
+        np.testing.assert_array_equal(rng, g[prog + "_rng"], err_msg=prog)
+        np.testing.assert_array_equal(mean, g[prog + "_mean"], err_msg=prog)
+    np.testing.assert_array_equal(oracle_firsthit(h, 3, pix, 1), g["pick"])
 
 
 def test_seeding_is_deterministic_and_in_range():
