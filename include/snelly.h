@@ -202,6 +202,26 @@ int snelly_flush_l2(snelly_ctx* ctx, size_t bytes);
  * CDF of the emission spectrum over 390..750 nm (js/spectra.js:28-61). */
 int snelly_inverse_cdf(const snelly_spectrum* s, float* out);
 
+/* Display transform of a job's mean image: shaders/tonemapper-fragment-shader.glsl as uploaded by
+ * Renderer.render (js/renderer.js:619-638): XYZ -> linear sRGB, gamut shift, pow(., invGamma),
+ * 2^exposure, L/(1+L), saturation, contrast, hue shift. Fields are the shader's uniforms (the
+ * host passes invGamma = 1/gamma). Output row 0 is the bottom row. RGBA8: the colour-buffer
+ * conversion clamp(c, 0, 1) * 255 rounded to nearest, 4 bytes per pixel; RGBA32F: the shader's
+ * output colour, 16 bytes per pixel. Waits for the job's enqueued frames. */
+typedef struct snelly_tonemap_params {
+  float exposure, invGamma, contrast, saturation, hueShift;
+} snelly_tonemap_params;
+#define SNELLY_TONEMAP_RGBA8 0
+#define SNELLY_TONEMAP_RGBA32F 1
+int snelly_tonemap(snelly_ctx* ctx, uint64_t job_id, const snelly_tonemap_params* params, void* out, size_t bytes,
+                   int format);
+
+/* Exhaustive device self-test of the arithmetic replacement the scene kernels' random number
+ * generator uses (no counterpart in the reference): which = 0 checks its integer-to-float
+ * conversion and its quotients against float() and __fdiv_rn for every state of each of the four
+ * lanes. *mismatches = number of differing results. */
+int snelly_selftest(snelly_ctx* ctx, int which, uint64_t* mismatches);
+
 /* sizeof of the ABI structs, for bindings to check their layouts: 0 SnellyParams,
  * 1 snelly_render_desc, 2 snelly_scene_opts, 3 snelly_uniform, 4 snelly_spectrum. */
 size_t snelly_abi_sizeof(int which);

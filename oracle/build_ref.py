@@ -114,14 +114,16 @@ float K_METAL(float wavelength_nm)
 MODEL_NAMES = {0: "abbe", 1: "sellmeier", 2: "sellmeier2", 3: "polyanskiy", 4: "cauchy"}
 
 
-PROGRAMS = ("pathtracer", "normals", "ao", "pick")
+PROGRAMS = ("pathtracer", "normals", "ao", "pick", "tonemapper")
 
 
 def shader_source(scene_glsl, opts, diele_model, ncoeffs, program="pathtracer"):
     """The fragment shader of `program` with the host's substitutions applied (the same set for
-    every program, js/renderer.js:287-316)."""
+    every program, js/renderer.js:287-316; the tonemapper gets none, js/renderer.js:358)."""
     assert program in PROGRAMS
     src = open(os.path.join(REF_ROOT, "shaders", f"{program}-fragment-shader.glsl")).read()
+    if program == "tonemapper":
+        return src
     full, defs = O.assemble(scene_glsl, opts)
     # the reference host's #define block, without the loop bounds (those are substituted)
     defines = "\n".join(l for l in defs.splitlines() if not l.startswith("#define MAX_"))
@@ -177,6 +179,8 @@ class RefLib:
                    os.path.join(HERE, "ref_harness.cpp"), "-o", so + ".tmp"]
             if program == "pick":
                 cmd.insert(1, "-DREF_PICK")
+            elif program == "tonemapper":
+                cmd.insert(1, "-DREF_TONEMAP")
             subprocess.run(cmd, check=True)
             os.replace(so + ".tmp", so)
             with open(stamp, "w") as f:
@@ -208,6 +212,9 @@ class RefLib:
         if self.program == "pick":
             L.ref_pick.argtypes = [vp, sz, sz, i32, vp, i32, vp, i32]
             L.ref_pick.restype = i32
+        elif self.program == "tonemapper":
+            L.ref_tonemap.argtypes = [vp, sz, sz, vp, i32, vp]
+            L.ref_tonemap.restype = i32
         else:
             L.ref_render.argtypes = [vp, sz, sz, sz, i32, i32, vp, i32, i32, vp, vp, i32]
             L.ref_render.restype = i32
@@ -265,6 +272,21 @@ class RefLib:
         assert rc == 0
         return out[:, :2].copy()
 
+    def tonemap(self, xyzn, uniforms):
+        """The tonemapper program on (n, 4) radiance texels with the given shader uniforms
+        {exposure, invGamma, contrast, saturation, hueShift}: (n, 4) output colours."""
+        a = np.ascontiguousarray(xyzn, np.float32).reshape(-1, 4)
+        out = np.zeros_like(a)
+        buf = bytearray(self.size)
+        for name, val in uniforms.items():
+            off = self.layout[name][1]
+            buf[off:off + 4] = np.float32(val).tobytes()
+        blk = bytes(buf)
+        ub = ctypes.create_string_buffer(blk, len(blk))
+        rc = self.lib.ref_tonemap(ub, len(blk), self.layout["Radiance"][1], a.ctypes.data, len(a), out.ctypes.data)
+        assert rc == 0
+        return out
+
     def render(self, params, scene_calls, tables, width, height, pixels, frames, rng, threads=0):
         pixels = np.ascontiguousarray(pixels, np.int32)
         n = len(pixels)
@@ -277,6 +299,13 @@ class RefLib:
                                  int(threads))
         assert rc == 0
         return mean, rng
+
+
+def tonemapper_lib():
+    """The reference's tonemapper program built for the CPU (scene-independent)."""
+    from snelly_b200 import _native
+    opts = _native.SceneOpts()
+    return RefLib("", opts, 0, 0, name="tonemapper", program="tonemapper")
 
 
 def ref_for(snelly, name=None, prebuilt_only=False, program="pathtracer"):

@@ -175,6 +175,8 @@ class OracleLib:
         L.oracle_render.restype = i32
         L.oracle_firsthit.argtypes = [vp, vp, i32, i32, i32, vp, i32, i32, vp, vp, vp, i32]
         L.oracle_firsthit.restype = i32
+        L.oracle_tonemap.argtypes = [vp, i32, vp, vp]
+        L.oracle_tonemap.restype = i32
         L.oracle_seed.argtypes = [ctypes.c_uint64, ctypes.c_uint64, vp]
         L.oracle_rand.argtypes = [vp]
         L.oracle_rand.restype = ctypes.c_float
@@ -196,8 +198,8 @@ class OracleLib:
             h.update("".join(flags).encode())
         except OSError:
             pass
-        for f in ("pt_oracle.h", "pt_oracle_bsdf.inc", "pt_oracle_integrator.inc", "fh_oracle.inc", "oracle_main.cpp",
-                  "counted.h"):
+        for f in ("pt_oracle.h", "pt_oracle_bsdf.inc", "pt_oracle_integrator.inc", "fh_oracle.inc", "tm_oracle.h",
+                  "oracle_main.cpp", "counted.h"):
             p = os.path.join(HERE, f)
             if os.path.exists(p):
                 h.update(open(p, "rb").read())
@@ -241,6 +243,15 @@ class OracleLib:
         if mode == 3:
             return mean[:, :2].copy()
         return xyz, mean, rng
+
+    def tonemap(self, xyzn, params):
+        """Display transform of (n, 4) mean XYZ pixels; params = (exposure, invGamma, contrast,
+        saturation, hueShift) as the shader receives them. Returns (n, 4) RGBA floats."""
+        a = np.ascontiguousarray(xyzn, np.float32).reshape(-1, 4)
+        out = np.zeros_like(a)
+        p = np.asarray(params, np.float32)
+        assert self.lib.oracle_tonemap(a.ctypes.data, len(a), p.ctypes.data, out.ctypes.data) == 0
+        return out
 
 
 def host_params(snelly):

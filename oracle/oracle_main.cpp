@@ -16,6 +16,7 @@ namespace glsl {
 #include SCENE_INC
 }
 #include "pt_oracle.h"
+#include "tm_oracle.h"
 
 namespace {
 
@@ -167,6 +168,17 @@ int oracle_firsthit(const SnellyParams* P, const void* uniforms, int mode, int w
     rng[4 * k + 1] = (uint32_t)glsl::s_tofloat(rnd.y);
     rng[4 * k + 2] = (uint32_t)glsl::s_tofloat(rnd.z);
     rng[4 * k + 3] = (uint32_t)glsl::s_tofloat(rnd.w);
+  }
+  return 0;
+}
+
+// The display transform (TM:36-97) of n mean XYZ pixels (4 floats each, N ignored) with the
+// shader's uniforms p = {exposure, invGamma, contrast, saturation, hueShift}; out: RGBA floats.
+int oracle_tonemap(const float* in4, int n, const float* p, float* out4) {
+  oracle::ToneMapper tm{p[0], p[1], p[2], p[3], p[4]};
+  for (int k = 0; k < n; ++k) {
+    glsl::vec4 c = tm.apply(glsl::vec3(in4[4 * k + 0], in4[4 * k + 1], in4[4 * k + 2]));
+    for (int i = 0; i < 4; ++i) out4[4 * k + i] = glsl::s_tofloat(c[i]);
   }
   return 0;
 }

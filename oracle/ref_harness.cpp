@@ -17,7 +17,28 @@ namespace glsl {
 
 extern "C" size_t ref_block_size(void) { return sizeof(glsl::RefShaderUniforms); }
 
-#ifdef REF_PICK
+#ifdef REF_TONEMAP
+// The tonemapper program (built with -DREF_TONEMAP): the Radiance texture bound to each input
+// texel in turn (1x1 NEAREST); out: g_outputColor per texel.
+extern "C" int ref_tonemap(const void* block, size_t block_bytes, size_t off_radiance, const float* in4, int n,
+                           float* out4) {
+  if (block_bytes != sizeof(glsl::RefShaderUniforms)) return -1;
+  std::vector<unsigned char> local(block_bytes + 16);
+  unsigned char* lb = local.data();
+  float rad[4];
+  glsl::sampler2D radS{rad, 1, 1, 4, 0, 0, 0};
+  std::memcpy(lb, block, block_bytes);
+  std::memcpy(lb + off_radiance, &radS, sizeof radS);
+  for (int k = 0; k < n; ++k) {
+    for (int c = 0; c < 4; ++c) rad[c] = in4[4 * k + c];
+    glsl::RefShader sh(*reinterpret_cast<const glsl::RefShaderUniforms*>(lb));
+    sh.vTexCoord = glsl::vec2(0.5f, 0.5f);
+    sh.main();
+    for (int c = 0; c < 4; ++c) out4[4 * k + c] = sh.g_outputColor[c];
+  }
+  return 0;
+}
+#elif defined(REF_PICK)
 // The pick program (built with -DREF_PICK): one invocation per listed pixel with mousePick at the
 // pixel centre; out: gbuf_pick (distance, material, 0, 0) per pixel.
 extern "C" int ref_pick(const void* block, size_t block_bytes, size_t off_mouse, int width, const int* pixels, int n,

@@ -83,6 +83,14 @@ class Spectrum(ctypes.Structure):
                 ("band_max", ctypes.c_float), ("wavelength", ctypes.c_float)]
 
 
+class TonemapParams(ctypes.Structure):
+    """snelly_tonemap_params: the tonemapper shader's uniforms."""
+    _fields_ = [(n, ctypes.c_float) for n in ("exposure", "invGamma", "contrast", "saturation", "hueShift")]
+
+
+TONEMAP_RGBA8, TONEMAP_RGBA32F = 0, 1
+
+
 class RenderDesc(ctypes.Structure):
     _fields_ = [("width", ctypes.c_int), ("height", ctypes.c_int), ("frames", ctypes.c_int), ("mode", ctypes.c_int),
                 ("seed", ctypes.c_uint64), ("params", SnellyParams), ("spectrum", Spectrum),
@@ -122,6 +130,8 @@ def lib():
         "snelly_advance_batch": (i32, [vp, P(u64), P(i32), sz]),
         "snelly_readback": (i32, [vp, u64, vp, sz, i32]),
         "snelly_readback_state": (i32, [vp, u64, vp, vp, vp, vp]),
+        "snelly_selftest": (i32, [vp, i32, P(u64)]),
+        "snelly_tonemap": (i32, [vp, u64, P(TonemapParams), vp, sz, i32]),
         "snelly_pick": (i32, [vp, u64, P(RenderDesc), ctypes.c_float, ctypes.c_float, P(ctypes.c_float),
                               P(ctypes.c_float)]),
         "snelly_restore": (i32, [vp, u64, P(RenderDesc), vp, vp, vp, P(u64)]),

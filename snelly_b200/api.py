@@ -631,6 +631,21 @@ class Snelly:
         """(H, W, 4) float32 array: mean X, Y, Z and sample count; row 0 is the bottom row."""
         return self._ctx.readback(self._job, self.width, self.height, out=out)
 
+    def tonemap_params(self):
+        """The tonemapper's uniforms as Renderer.render uploads them (js/renderer.js:623-630)."""
+        r = self.pathtracer
+        return (r.exposure, 1.0 / r.gamma, r.contrast, r.saturation, r.hueShift)
+
+    def tonemap(self, fmt=N.TONEMAP_RGBA8):
+        """The displayed image: the mean radiance through the reference's tonemapper with the
+        renderer's exposure, gamma, contrast, saturation and hue shift. (H, W, 4), row 0 bottom."""
+        return self._ctx.tonemap(self._job, self.width, self.height, self.tonemap_params(), fmt)
+
+    def screenshot(self, path):
+        """Write the displayed image to a PNG file (top row first)."""
+        from .image import write_png
+        write_png(path, self.tonemap()[::-1])
+
     def job_id(self):
         return self._job
 
@@ -727,6 +742,21 @@ class Context:
         ids = (ctypes.c_uint64 * len(jobs_frames))(*jobs_frames.keys())
         fr = (ctypes.c_int * len(jobs_frames))(*jobs_frames.values())
         N.check(self._lib.snelly_advance_batch(self._h, ids, fr, len(jobs_frames)))
+
+    def tonemap(self, jid, width, height, params, fmt=N.TONEMAP_RGBA8):
+        """The job's mean image through the display transform: (H, W, 4) uint8 (RGBA8) or float32
+        (RGBA32F); row 0 is the bottom row. params: (exposure, invGamma, contrast, saturation,
+        hueShift) as the tonemapper shader receives them."""
+        tp = N.TonemapParams(*[float(v) for v in params])
+        out = np.empty((height, width, 4), np.uint8 if fmt == N.TONEMAP_RGBA8 else np.float32)
+        N.check(self._lib.snelly_tonemap(self._h, jid, ctypes.byref(tp), out.ctypes.data, out.nbytes, int(fmt)))
+        return out
+
+    def selftest(self, which):
+        """Mismatch count of a device self-test (0: the RNG's conversions and quotients)."""
+        n = ctypes.c_uint64()
+        N.check(self._lib.snelly_selftest(self._h, int(which), ctypes.byref(n)))
+        return n.value
 
     def pick(self, sid, desc, x, y):
         d, m = ctypes.c_float(), ctypes.c_float()

@@ -11,7 +11,7 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 CUDA = os.environ.get("CUDA_HOME", "/usr/local/cuda")
-SOURCES = ["runtime.cpp", "glsl_transform.cpp", "wavefront.cpp", "aot_kernels.cu"]
+SOURCES = ["runtime.cpp", "glsl_transform.cpp", "wavefront.cpp", "aot_kernels.cu", "tonemap.cu"]
 OUT = os.path.join(HERE, "libsnelly.so")
 
 
@@ -34,8 +34,10 @@ def build(force=False, verbose=False):
     if not force and not needs_build():
         return OUT
     csrc = os.path.join(HERE, "csrc")
+    # --fmad=false: the ahead-of-time kernels restate reference formulas operation by operation
+    # (the tonemapper) or check arithmetic against IEEE results (the self-tests)
     cmd = [os.path.join(CUDA, "bin", "nvcc"), "-shared", "-Xcompiler", "-fPIC", "-O2", "-std=c++17",
-           "-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo",
+           "-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo", "--fmad=false",
            "-I" + csrc, "-I" + os.path.join(ROOT, "include"), "-I" + os.path.join(CUDA, "include"),
            "-o", OUT + ".tmp"]
     cmd += [os.path.join(csrc, s) for s in SOURCES]

@@ -1,11 +1,14 @@
 // aot_kernels.cu - scene-independent kernels compiled ahead of time for sm_100a into libsnelly:
-// the FP32 peak microbenchmark used as the roofline denominator, and an L2 flush for timing.
+// the FP32 peak microbenchmark used as the roofline denominator, an L2 flush for timing, the image
+// statistics reduction, and exhaustive self-tests of the arithmetic replacements the scene
+// kernels use (this file is compiled without fast-math, so floorf and __fdiv_rn are IEEE).
 #include <cuda_runtime.h>
 
 #include <algorithm>
 #include <mutex>
 #include <string>
 
+#include "kernels/pt_rng.cuh"
 #include "runtime_internal.h"
 #include "snelly.h"
 
@@ -66,6 +69,24 @@ __global__ void __launch_bounds__(32) image_stats_final(const double* __restrict
     for (int b = 0; b < nblocks; ++b) t += partial[5 * b + threadIdx.x];
     out[threadIdx.x] = t;
   }
+}
+
+// Self-test 0: the RNG's conversion and quotient for every state x in [0, m) of each modulus,
+// against float(x) and __fdiv_rn.
+__global__ void selftest_rng_quotients(unsigned long long* bad) {
+  const unsigned m[4] = {4194287u, 4194277u, 4194191u, 4194167u};
+  const float inv[4] = {SNELLY_RNG_INV_M0, SNELLY_RNG_INV_M1, SNELLY_RNG_INV_M2, SNELLY_RNG_INV_M3};
+  unsigned long long n = 0;
+  const unsigned stride = gridDim.x * blockDim.x;
+  for (int k = 0; k < 4; ++k) {
+    const float mf = (float)m[k];
+    for (unsigned x = blockIdx.x * blockDim.x + threadIdx.x; x < m[k]; x += stride) {
+      float xf = sdev::small_uint_to_float(x);
+      float q = sdev::quotient_small(xf, mf, inv[k]);
+      n += (xf == (float)x && __float_as_uint(q) == __float_as_uint(__fdiv_rn((float)x, mf))) ? 0 : 1;
+    }
+  }
+  if (n) atomicAdd(bad, n);
 }
 
 __global__ void l2_flush_kernel(float4* buf, size_t n, float v) {
@@ -138,6 +159,30 @@ int snelly_image_stats(snelly_ctx* ctx, uint64_t job_id, double* out5) {
   if (cudaMemcpyAsync(out5, result, 5 * sizeof(double), cudaMemcpyDeviceToHost, c.stream) != cudaSuccess ||
       cudaStreamSynchronize(c.stream) != cudaSuccess)
     return snelly::fail(SNELLY_EDEVICE, "image statistics failed");
+  return SNELLY_OK;
+}
+
+int snelly_selftest(snelly_ctx* ctx, int which, uint64_t* mismatches) {
+  if (!ctx || !mismatches) return snelly::fail(SNELLY_EINVAL, "null argument to snelly_selftest");
+  if (which != 0) return snelly::fail(SNELLY_EINVAL, "unknown self-test");
+  snelly::Context& c = *ctx->c;
+  std::lock_guard<std::mutex> lk(c.mu);
+  snelly::DevBuf cnt;
+  int rc = c.alloc(cnt, sizeof(unsigned long long));
+  if (rc) return rc;
+  unsigned long long* d = (unsigned long long*)cnt.ptr;
+  unsigned long long h = 0;
+  cudaError_t e = cudaMemsetAsync(d, 0, sizeof h, c.stream);
+  if (e == cudaSuccess) {
+    selftest_rng_quotients<<<c.sm_count * 16, 256, 0, c.stream>>>(d);
+    c.launches += 1;
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess) e = cudaMemcpyAsync(&h, d, sizeof h, cudaMemcpyDeviceToHost, c.stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(c.stream);
+  c.release(cnt);
+  if (e != cudaSuccess) return snelly::fail(SNELLY_EDEVICE, std::string("self-test: ") + cudaGetErrorString(e));
+  *mismatches = h;
   return SNELLY_OK;
 }
 

@@ -14,6 +14,7 @@
 // laid out on the GPU (kernels, queues, state in HBM) is in pt_kernels.cu.
 #pragma once
 #include "snelly_params.h"
+#include "pt_rng.cuh"
 
 #ifndef MAX_MARCH_STEPS
 #define MAX_MARCH_STEPS 256
@@ -56,38 +57,12 @@ SD_FN float avg(const vec3& v) { return (v.x + v.y + v.z) / 3.0f; }
 SD_FN float maxc(float f) { return f; }
 SD_FN float maxc(const vec3& v) { return fmaxf(fmaxf(v.x, v.y), v.z); }
 
-// ---- random numbers --------------------------------------------------------------------------
-// The reference's generator (PT:119-130) is a four-lane combined multiplicative LCG evaluated in
-// float arithmetic with Schrage's decomposition. For integer states below 2^22 every float
-// operation there is exact, so the same sequence comes out of 32-bit integer Schrage steps:
-// x' = a*(x mod q) - r*(x div q), plus m if negative. The output u = fract(x0/m0 - x1/m1 +
-// x2/m2 - x3/m3) uses IEEE round-to-nearest divisions so it is bit-identical to the reference.
-struct Rng {
-  unsigned s[4];
-};
-SD_FN unsigned schrage(unsigned x, int a, unsigned q, int r, int m) {
-  unsigned hi = x / q;
-  unsigned lo = x - hi * q;
-  int p = a * int(lo) - r * int(hi);
-  return unsigned(p < 0 ? p + m : p);
-}
-SD_FN float rand01(Rng& g) {
-  g.s[0] = schrage(g.s[0], 3423, 1225u, 1112, 4194287);
-  g.s[1] = schrage(g.s[1], 2646, 1585u, 367, 4194277);
-  g.s[2] = schrage(g.s[2], 1707, 2457u, 92, 4194191);
-  g.s[3] = schrage(g.s[3], 1999, 2098u, 265, 4194167);
-  float u0 = __fdiv_rn(float(g.s[0]), 4194287.0f);
-  float u1 = __fdiv_rn(float(g.s[1]), 4194277.0f);
-  float u2 = __fdiv_rn(float(g.s[2]), 4194191.0f);
-  float u3 = __fdiv_rn(float(g.s[3]), 4194167.0f);
-  float v = __fsub_rn(__fadd_rn(__fsub_rn(u0, u1), u2), u3);
-  return __fsub_rn(v, floorf(v));
-}
+// ---- random numbers: pt_rng.cuh (Rng, rand01) -------------------------------------------------
 
 // ---- tables (GL LINEAR + CLAMP_TO_EDGE 1-D lookups, texel centres at (i+0.5)/n) ---------------
 SD_FN float table1(const float* t, int n, float u) {
   float x = u * float(n) - 0.5f;
-  float x0 = floorf(x);
+  float x0 = glsl::s_floor(x);
   float f = x - x0;
   int i0 = int(x0), i1 = i0 + 1;
   i0 = i0 < 0 ? 0 : (i0 >= n ? n - 1 : i0);
@@ -98,7 +73,7 @@ SD_FN float table1(const float* t, int n, float u) {
 SD_FN vec3 table_xyz(const float* t, float u) {
   const int n = SNELLY_XYZ_SAMPLES;
   float x = u * float(n) - 0.5f;
-  float x0 = floorf(x);
+  float x0 = glsl::s_floor(x);
   float f = x - x0;
   int i0 = int(x0), i1 = i0 + 1;
   i0 = i0 < 0 ? 0 : (i0 >= n ? n - 1 : i0);
@@ -760,7 +735,7 @@ SD_FN vec3 sky_rgb(const Ctx& c, const vec3& dir) {
     float rot_phi = kPi * P.envMapPhiRotation / 180.0f;
     vec3 dl = to_local(dir, make_frame(pole));
     float phi = atan2f(dl.y, dl.x) + kPi + rot_phi;
-    phi -= 2.0f * kPi * floorf(phi / (2.0f * kPi));
+    phi -= 2.0f * kPi * glsl::s_floor(phi / (2.0f * kPi));
     float theta = acosf(dl.z);
     glsl::sampler2D env{P.envMap, P.envMapW, P.envMapH, 3, 2, 1, 1};
     vec4 tx = glsl::texture(env, vec2(phi / (2.0f * kPi), theta / kPi));

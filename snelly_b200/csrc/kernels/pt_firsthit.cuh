@@ -135,7 +135,7 @@ SD_FN void fh_camera(const Ctx& c, const vec2& pixel, Rng& g, vec3& start, vec3&
 SD_FN vec3 fh_env_xyz(const SnellyParams& P, const vec3& dir) {
   if (P.haveEnvMap) {
     float phi = atan2f(dir.x, dir.z) + kPi;
-    phi -= 2.0f * kPi * floorf(phi / (2.0f * kPi));
+    phi -= 2.0f * kPi * glsl::s_floor(phi / (2.0f * kPi));
     float theta = acosf(dir.y);
     glsl::sampler2D env{P.envMap, P.envMapW, P.envMapH, 3, 2, 1, 1};
     vec4 tx = glsl::texture(env, vec2(phi / (2.0f * kPi), theta / kPi));
@@ -153,7 +153,7 @@ SD_FN vec3 fh_sky_rgb(const SnellyParams& P, const vec3& dir) {
     float rot_phi = kPi * P.envMapPhiRotation / 180.0f;
     vec3 dl = to_local(dir, fh_basis(pole));
     float phi = atan2f(dl.y, dl.x) + kPi + rot_phi;
-    phi -= 2.0f * kPi * floorf(phi / (2.0f * kPi));
+    phi -= 2.0f * kPi * glsl::s_floor(phi / (2.0f * kPi));
     float theta = acosf(dl.z);
     glsl::sampler2D env{P.envMap, P.envMapW, P.envMapH, 3, 2, 1, 1};
     vec4 tx = glsl::texture(env, vec2(phi / (2.0f * kPi), theta / kPi));

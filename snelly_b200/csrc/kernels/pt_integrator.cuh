@@ -600,7 +600,7 @@ SD_FN vec3 pick_wavelength(Ctx& c, Rng& g) {
 #ifdef DISPERSION_ENABLED
   const SnellyParams& P = c.P;
   float ns = float(P.wavelengthSamples);
-  float xi = 0.1f + 0.8f * (0.5f + floorf(ns * rand01(g))) / ns;
+  float xi = 0.1f + 0.8f * (0.5f + glsl::s_floor(ns * rand01(g))) / ns;
   float w = table1(c.Pg->icdfTable, SNELLY_ICDF_SAMPLES, xi);
   c.lambda = 390.0f + (750.0f - 390.0f) * w;
   vec3 xyz = table_xyz(c.Pg->xyzTable, w);

@@ -72,7 +72,7 @@ extern "C" __global__ void __launch_bounds__(SNELLY_BLOCK) snelly_seed(const Job
 
 // One frame (MAX_SAMPLES_PER_FRAME samples) for every pixel of every job in the batch: the
 // path-per-thread kernel. Each thread runs the whole camera path of its pixel.
-extern "C" __global__ void __launch_bounds__(SNELLY_BLOCK) snelly_frame_mega(const JobRec* __restrict__ jobs,
+extern "C" __global__ void __launch_bounds__(SNELLY_BLOCK, SNELLY_MEGA_MIN_BLOCKS) snelly_frame_mega(const JobRec* __restrict__ jobs,
                                                                           const int* __restrict__ block_start, int njobs,
                                                                           const SnellyParams* __restrict__ gparams) {
   using namespace sdev;

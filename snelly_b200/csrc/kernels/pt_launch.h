@@ -2,6 +2,14 @@
 #pragma once
 
 #define SNELLY_BLOCK 128  // threads per block of the per-pixel kernels
+// Resident blocks per SM the register allocation of the path-per-thread kernel and of the
+// wavefront shade stage is held to (65536 registers / (blocks x 128 threads) per thread).
+#ifndef SNELLY_MEGA_MIN_BLOCKS
+#define SNELLY_MEGA_MIN_BLOCKS 5
+#endif
+#ifndef SNELLY_SHADE_MIN_BLOCKS
+#define SNELLY_SHADE_MIN_BLOCKS 4
+#endif
 
 // Render modes (the values of SNELLY_MODE_* in snelly.h).
 #define JOB_MODE_PT 0

@@ -18,7 +18,13 @@
 #include "pt_launch.h"
 
 #ifndef WF_REFILL
-#define WF_REFILL 4  // idle lanes of a warp that trigger a refill from the work head
+#define WF_REFILL 4  // idle lanes of a warp that trigger a refill
+#endif
+#ifndef WF_GRAB
+#define WF_GRAB 32  // work items a warp claims from the global head at a time
+#endif
+#ifndef WF_CHUNK
+#define WF_CHUNK 8  // sphere-tracing steps between refills
 #endif
 #define WF_FULL 0xffffffffu
 
@@ -126,10 +132,12 @@ extern "C" __global__ void __launch_bounds__(SNELLY_BLOCK) snelly_wf_generate(co
 
 // Trace the active continuation rays and the pending shadow rays of iteration `it`.
 //
-// Every pass of the loop evaluates the scene SDFs once for every lane that holds a ray; a ray's
-// first evaluation (at its origin, which fixes the marching sign, PT:888-900) is such a pass too,
-// so refilled lanes march in step with the rest of the warp. Idle lanes are refilled from the
-// global work head when at least WF_REFILL of them are idle, or when none of the warp is busy.
+// Every pass of the loop runs up to WF_CHUNK sphere-tracing steps, each evaluating the scene SDFs
+// once for every lane that holds a ray; a ray's first evaluation (at its origin, which fixes the
+// marching sign, PT:888-900) is such a step too, so refilled lanes march in step with the rest of
+// the warp. Idle lanes are refilled when at least WF_REFILL of them are idle, or when none of the
+// warp is busy, from a range of WF_GRAB items the warp claims from the global work head with one
+// atomic.
 extern "C" __global__ void __launch_bounds__(SNELLY_BLOCK) snelly_wf_extend(WfBuffers B, int it) {
   using namespace sdev;
   const SnellyParams& P = c_params[0];
@@ -149,31 +157,39 @@ extern "C" __global__ void __launch_bounds__(SNELLY_BLOCK) snelly_wf_extend(WfBu
   const float minMarch = P.minLengthScale;
   const float maxLen = P.maxLengthScale;
 
-  bool has = false, exhausted = false, first = false;
+  bool has = false, first = false;
   int path = 0, sidx = -1;  // sidx >= 0: a shadow ray
   vec3 o(0.0f), d(0.0f);
   float t = 0.0f, sgn = 1.0f, maxd = 0.0f;
   int n = 0;
+  // The warp's claimed range [wbase, wlim) of work items (warp-uniform); one atomic claims
+  // WF_GRAB items, handed to idle lanes over several refills.
+  int wbase = 0, wlim = 0;
+  bool wdone = false;
   for (;;) {
     bool done = false, res_hit = false, finishing = false;
     int res_mat = MAT_INVAL;
     // ---- refill idle lanes ----------------------------------------------------------------
-    const bool want = !has && !exhausted;
+    const bool want = !has;
     const unsigned need = __ballot_sync(WF_FULL, want);
     const unsigned busy = __ballot_sync(WF_FULL, has);
-    if (need && (__popc(need) >= WF_REFILL || !busy)) {
-      int leader = __ffs(need) - 1;
-      int base = 0;
-      if ((int)(threadIdx.x & 31) == leader) base = atomicAdd(cnt + WF_HEAD + it, __popc(need));
-      base = __shfl_sync(WF_FULL, base, leader);
-      if (want) {
-        int w = base + __popc(need & lanemask_lt());
-        if (w >= total) {
-          exhausted = true;
-        } else if (w < nA) {
-          path = qa[w];
+    if (!wdone && need && (__popc(need) >= WF_REFILL || !busy)) {
+      if (wbase >= wlim) {
+        int nb = 0;
+        if ((threadIdx.x & 31) == 0) nb = atomicAdd(cnt + WF_HEAD + it, WF_GRAB);
+        nb = __shfl_sync(WF_FULL, nb, 0);
+        wbase = nb;
+        wlim = min(nb + WF_GRAB, total);
+        wdone = nb >= total;
+      }
+      const int w = wbase + __popc(need & lanemask_lt());
+      wbase = min(wbase + __popc(need), wlim);
+      if (want && w < wlim) {
+        if (w < nA) {
+          const int e = qa[w];
+          path = e < 0 ? ~e : e;
           sidx = -1;
-          if (B.info[path].z & WF_FINISHING) {
+          if (e < 0) {  // the path only waits for its shadow results
             finishing = true;
             done = true;
           } else {
@@ -195,8 +211,8 @@ extern "C" __global__ void __launch_bounds__(SNELLY_BLOCK) snelly_wf_extend(WfBu
         }
       }
     }
-    // ---- one sphere-tracing step (PT:888-919) -------------------------------------------------
-    if (has) {
+    // ---- up to WF_CHUNK sphere-tracing steps (PT:888-919); a lane stops when its ray is done ----
+    for (int k = 0; k < WF_CHUNK && has && !done; ++k) {
       const vec3 p = first ? o : o + t * d;
       float sdf = 1.0e20f;
       int m = MAT_INVAL;
@@ -264,12 +280,12 @@ extern "C" __global__ void __launch_bounds__(SNELLY_BLOCK) snelly_wf_extend(WfBu
       }
       if (done) has = false;
     }
-    if (__all_sync(WF_FULL, exhausted && !has)) break;
+    if (wdone && !__any_sync(WF_FULL, has)) break;
   }
 }
 
 // Shade every path the extend stage of iteration `it` queued.
-extern "C" __global__ void __launch_bounds__(SNELLY_BLOCK) snelly_wf_shade(const JobRec* __restrict__ jobs,
+extern "C" __global__ void __launch_bounds__(SNELLY_BLOCK, SNELLY_SHADE_MIN_BLOCKS) snelly_wf_shade(const JobRec* __restrict__ jobs,
                                                                         const SnellyParams* __restrict__ gparams,
                                                                         WfBuffers B, int it) {
   using namespace sdev;
@@ -289,7 +305,7 @@ extern "C" __global__ void __launch_bounds__(SNELLY_BLOCK) snelly_wf_shade(const
     int w = base + threadIdx.x;
     bool valid = w < total;
     int path = 0;
-    bool push_active = false;
+    bool push_active = false, finishing_entry = false;
     int push_shadow = 0;  // bit 0: sky, bit 1: sun
     if (valid) {
       int seg = w < n0 ? 0 : (w < n0 + n1 ? 1 : (w < n0 + n1 + n2 ? 2 : 3));
@@ -377,10 +393,12 @@ extern "C" __global__ void __launch_bounds__(SNELLY_BLOCK) snelly_wf_shade(const
         B.info[path] = make_int4(info.x, s.atmScatters, flags, 0);
         B.rng[path] = make_uint4(g.s[0], g.s[1], g.s[2], g.s[3]);
         push_active = true;
+        finishing_entry = flags & WF_FINISHING;
       }
     }
+    // active-queue entries of paths that only wait for their shadow results are stored as ~path
     int slot = warp_append(cnt + WF_A + nxt, push_active);
-    if (slot >= 0) B.qa[nxt][slot] = path;
+    if (slot >= 0) B.qa[nxt][slot] = finishing_entry ? ~path : path;
     for (int l = 0; l < 2; ++l) {
       int ss = warp_append(cnt + WF_S + nxt, (push_shadow >> l) & 1);
       if (ss >= 0) B.qs[nxt][ss] = 2 * path + l;

@@ -299,6 +299,14 @@ int Context::compile_module(const std::string& src, int math_mode, std::shared_p
       if (f.required) return fail(SNELLY_ECOMPILE, std::string("kernel missing from module: ") + f.name);
     }
   }
+  if (m->f_wf_extend) {  // the extend stage is persistent: one wave of resident blocks
+    int nb = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, (const void*)m->f_wf_extend, SNELLY_BLOCK, 0) == cudaSuccess &&
+        nb > 0)
+      m->extend_blocks_per_sm = nb;
+    else
+      cudaGetLastError();
+  }
   size_t sz = 0;
   RT_TRY(cudaLibraryGetGlobal((void**)&m->c_params, &sz, m->lib, "c_params"));
   RT_TRY(cudaLibraryGetGlobal((void**)&m->c_uniforms, &m->c_uniforms_bytes, m->lib, "c_uniforms"));
@@ -318,7 +326,7 @@ int Context::launch(cudaKernel_t f, int blocks, int threads, void** args) {
 
 // Upload a job's parameter and uniform blocks into constant-memory slot `slot` of its module.
 int Context::upload_slot(Job& j, int slot) {
-  Module& m = *j.scene->module;
+  Module& m = *j.module;
   RT_TRY(cudaMemcpyAsync(m.c_params + slot * sizeof(SnellyParams), &j.params, sizeof(SnellyParams),
                          cudaMemcpyHostToDevice, stream));
   size_t ub = std::min(j.ublock.size(), m.slot_uniform_bytes);
@@ -355,7 +363,7 @@ int Context::single_job_tables(Job& j) {
 
 int Context::enqueue_frames(Job& j, int frames) {
   if (frames <= 0) return SNELLY_OK;
-  Module& m = *j.scene->module;
+  Module& m = *j.module;
   int rc = upload_slot(j, 0);
   if (rc) return rc;
   void* tables = j.tables.ptr;
@@ -389,7 +397,7 @@ int Context::enqueue_frames(Job& j, int frames) {
 int Context::advance_batch(const std::vector<Job*>& js, const std::vector<int>& frames) {
   std::map<Module*, std::vector<size_t>> groups;
   for (size_t k = 0; k < js.size(); ++k)
-    if (frames[k] > 0) groups[js[k]->scene->module.get()].push_back(k);
+    if (frames[k] > 0) groups[js[k]->module].push_back(k);
   // all earlier work on the main stream (job seeding, single-job frames) comes first
   cudaEvent_t start;
   RT_TRY(cudaEventCreateWithFlags(&start, cudaEventDisableTiming));
@@ -514,6 +522,7 @@ void Context::free_job(Job& j) {
   release(j.env);
   release(j.gparams);
   release(j.tables);
+  release(j.display);
   release_wavefront(j);
   if (j.done) cudaEventDestroy(j.done);
   j.done = nullptr;
@@ -717,6 +726,17 @@ static int start_job(Context& c, uint64_t scene_id, const snelly_render_desc* de
   Scene& s = it->second;
   Job j;
   j.scene = &s;
+  j.module = s.module.get();
+  if (desc->mode != SNELLY_MODE_PT) {
+    if (s.opts.math_mode == SNELLY_MATH_STRICT) {
+      s.strict_module = s.module;
+    } else if (!s.strict_module) {
+      std::string nvlog;
+      int rc0 = c.compile_module(program_source(s.src), SNELLY_MATH_STRICT, &s.strict_module, &nvlog);
+      if (rc0) return rc0;
+    }
+    j.module = s.strict_module.get();
+  }
   j.desc = *desc;
   j.desc.env_map = nullptr;
   j.params = desc->params;
@@ -778,7 +798,14 @@ static int start_job(Context& c, uint64_t scene_id, const snelly_render_desc* de
     void* bstart = (char*)j.tables.ptr + 128;
     int njobs = 1;
     void* args[] = {&tables, &bstart, &njobs};
-    if ((rc = c.launch(s.module->f_seed, j.blocks, SNELLY_BLOCK, args))) return bail(rc);
+    if ((rc = c.launch(j.module->f_seed, j.blocks, SNELLY_BLOCK, args))) return bail(rc);
+  }
+  if (desc->frames == 0) {  // the mean image of the seeded or restored state, for readback
+    void* tables = j.tables.ptr;
+    void* bstart = (char*)j.tables.ptr + 128;
+    int njobs = 1;
+    void* rargs[] = {&tables, &bstart, &njobs};
+    if ((rc = c.launch(j.module->f_resolve, j.blocks, SNELLY_BLOCK, rargs))) return bail(rc);
   }
   j.id = ++c.next_id;
   uint64_t id = j.id;
@@ -840,7 +867,8 @@ int snelly_advance_batch(snelly_ctx* ctx, const uint64_t* job_ids, const int* fr
   return c.advance_batch(js, fs);
 }
 
-static int wait_job(Context& c, Job& j, int flags) {
+extern "C++" {
+int snelly::wait_job(Context& c, Job& j, int flags) {
   if (flags & SNELLY_READ_POLL) {
     cudaError_t e = cudaEventQuery(j.done);
     if (e == cudaErrorNotReady) return fail(SNELLY_EBUSY, "job not finished");
@@ -852,6 +880,7 @@ static int wait_job(Context& c, Job& j, int flags) {
   if (e != cudaSuccess) return fail(SNELLY_EDEVICE, std::string("job failed: ") + cudaGetErrorString(e));
   return SNELLY_OK;
 }
+}  // extern "C++"
 
 int snelly_readback(snelly_ctx* ctx, uint64_t job_id, float* out, size_t bytes, int flags) {
   if (!ctx || !out) return fail(SNELLY_EINVAL, "null argument to snelly_readback");

@@ -46,6 +46,7 @@ struct Module {
   cudaKernel_t f_wf_generate = nullptr, f_wf_extend = nullptr, f_wf_shade = nullptr, f_wf_shadow = nullptr,
                f_wf_accumulate = nullptr;
   cudaKernel_t f_firsthit = nullptr;
+  int extend_blocks_per_sm = 8;  // resident blocks of the persistent extend stage (occupancy query)
   char* c_params = nullptr;  // device addresses of the constant banks
   char* c_uniforms = nullptr;
   size_t c_uniforms_bytes = 0, slot_uniform_bytes = 0;
@@ -59,15 +60,22 @@ struct Scene {
   std::vector<unsigned char> ublock;  // uniform block (host copy), snapshotted by jobs
   std::map<std::string, DevBuf> textures;
   std::shared_ptr<Module> module;
+  // IEEE-mode build of the same program for the first-hit passes (normals, AO, pick), compiled on
+  // first use when `module` is a fast-math build: those passes are deterministic and must agree
+  // with the reference per pixel, and they trace one ray per pixel, so exact arithmetic costs
+  // little there.
+  std::shared_ptr<Module> strict_module;
 };
 
 struct Job {
   uint64_t id = 0;
   Scene* scene = nullptr;
+  Module* module = nullptr;  // the build this job's kernels run from
   snelly_render_desc desc{};
   SnellyParams params{};
   std::vector<unsigned char> ublock;
   DevBuf rng, acc, comp, acc64, out, icdf, env, gparams, tables;
+  DevBuf display;  // tonemapped image (snelly_tonemap), allocated on first use
   DevBuf wf;  // wavefront path state and queues
   WfBuffers wfb{};
   int blocks = 0;
@@ -120,6 +128,9 @@ struct Context {
 
 int assemble_scene(const std::string& glsl, const snelly_scene_opts& o, SceneSource* out);
 std::string program_source(const SceneSource& ss);
+
+// Wait for (or, with SNELLY_READ_POLL, test) the completion of a job's enqueued frames.
+int wait_job(Context& c, Job& j, int flags);
 
 }  // namespace snelly
 

@@ -44,7 +44,7 @@ void Context::release_wavefront(Job& j) {
 }
 
 int Context::enqueue_wavefront_frame(Job& j) {
-  Module& m = *j.scene->module;
+  Module& m = *j.module;
   if (!j.wf.ptr || !m.f_wf_generate || !m.f_wf_extend || !m.f_wf_shade)
     return fail(SNELLY_EINVAL, "wavefront integrator not available for this job");
   void* jobs = j.tables.ptr;
@@ -55,7 +55,7 @@ int Context::enqueue_wavefront_frame(Job& j) {
   int rc = launch(m.f_wf_generate, gen_blocks, SNELLY_BLOCK, gargs);
   if (rc) return rc;
   const int iters = j.scene->opts.max_bounces + 2;
-  const int extend_blocks = sm_count * 16, shade_blocks = sm_count * 4;
+  const int extend_blocks = sm_count * m.extend_blocks_per_sm, shade_blocks = sm_count * 4;
   for (int it = 0; it < iters; ++it) {
     void* eargs[] = {&B, &it};
     if ((rc = launch(m.f_wf_extend, extend_blocks, SNELLY_BLOCK, eargs))) return rc;

@@ -175,12 +175,10 @@ class _Posed:
     def shader(self):
         return self.base.shader()
 
-    def syncShader(self, snelly, shader):
-        if hasattr(self.base, "syncShader"):
-            self.base.syncShader(snelly, shader)
-
-    def getMinLengthScale(self):
-        return self.base.getMinLengthScale()
+    def __getattr__(self, name):  # the other scene methods (syncShader, length scales, ...)
+        if name == "base":
+            raise AttributeError(name)
+        return getattr(self.base, name)
 
 
 def posed_scene(name, res, rs):

@@ -11,6 +11,8 @@ Run in a checkout that has the reference at /root/reference (or $SNELLY_REFERENC
   ao-fragment-shader.glsl, pick-fragment-shader.glsl, built the same way) on the same scenes:
   normals and AO running means and RNG lanes after a few frames, pick distance and material at
   every pixel centre. `python tests/golden/make_golden.py fh` regenerates only these.
+* tm_golden.npz: the reference's tonemapper program on path-traced and synthetic XYZ texels for
+  three display settings.
 * cie_csv.npy: the CIE XYZ table recomputed from scripts/color/lin2012xyz2e_fine_7sf.csv as
   scripts/color/cie.py does (linear interpolation to 1024 samples over 390..750 nm, both ends
   included), to pin the table in snelly_b200/data/materials.json.
@@ -80,6 +82,29 @@ def make_firsthit(name):
     print(f"fh_{name}: {h.width}x{h.height}, normals/ao {FH_FRAMES} frames, pick hits {(out['pick'][:, 1] >= 0).mean():.3f}")
 
 
+TM_PARAMS = [  # exposure, invGamma (= 1/gamma as the host uploads it), contrast, saturation, hueShift
+    (0.0, 1.0 / 2.2, 1.0, 1.0, 0.0),   # the Renderer defaults (js/renderer.js:118-122)
+    (1.5, 1.0 / 1.8, 1.3, 0.8, 0.25),
+    (-2.0, 1.0, 0.7, 1.6, 0.9),
+]
+
+
+def make_tonemap():
+    """tm_golden.npz: the reference's tonemapper program (shaders/tonemapper-fragment-shader.glsl)
+    on path-traced mean images and on wide-range synthetic XYZ values (out-of-gamut and HDR), for
+    three sets of display settings."""
+    rs = np.random.RandomState(11)
+    c1 = np.load(os.path.join(HERE, "pt_c1.npz"))["mean"]
+    atm = np.load(os.path.join(HERE, "pt_atmosphere.npz"))["mean"][:1024]
+    x = np.concatenate([c1, atm, np.abs(rs.standard_cauchy((1024, 4))), rs.uniform(-0.2, 3.0, (1024, 4))]).astype(np.float32)
+    x[:, 3] = 1.0
+    ref = build_ref.tonemapper_lib()
+    names = ["exposure", "invGamma", "contrast", "saturation", "hueShift"]
+    outs = np.stack([ref.tonemap(x, dict(zip(names, p))) for p in TM_PARAMS])
+    np.savez_compressed(os.path.join(HERE, "tm_golden.npz"), xyzn=x, params=np.asarray(TM_PARAMS, np.float32), rgba=outs)
+    print(f"tm_golden: {len(x)} texels x {len(TM_PARAMS)} settings")
+
+
 def make_cie():
     path = os.path.join(build_ref.REF_ROOT, "scripts", "color", "lin2012xyz2e_fine_7sf.csv")
     rows = [r for r in csv.reader(open(path))]
@@ -101,3 +126,5 @@ if __name__ == "__main__":
     for n in FH_CASES:
         if not only or "fh" in only:
             make_firsthit(n)
+    if not only or "tm" in only:
+        make_tonemap()

@@ -36,8 +36,15 @@ def test_strict_math_matches_reference_per_pixel(gpu_ctx, name, kernel):
     assert rel.max() <= 5e-3, rel
 
 
+# The C2 Mandelbox distance estimator amplifies last-bit differences (approximate division and
+# contracted multiply-adds in fast-math builds) into different hit points within a few steps, so
+# matched seeds give different paths at half the pixels: per-pixel agreement is not expected
+# there, and C2 is checked in distribution (test_statistical_agreement_independent_seeds).
+FAST_CASES = sorted(n for n in CASES if n != "c2")
+
+
 @pytest.mark.parametrize("kernel", sorted(KERNELS))
-@pytest.mark.parametrize("name", sorted(CASES))
+@pytest.mark.parametrize("name", FAST_CASES)
 def test_fast_math_matches_reference(gpu_ctx, name, kernel):
     """Production (fast-math) module vs the reference shader with matched seeds. Bar: >= 80% of
     pixels within 1e-3 relative (the rest diverged through ulp-level differences), image mean XYZ
@@ -67,55 +74,70 @@ def test_rng_seeding_matches_oracle(gpu_ctx):
     assert (acc == 0).all() and (comp == 0).all()
 
 
-@pytest.mark.parametrize("kernel", sorted(KERNELS))
-@pytest.mark.parametrize("scene_factory,frames_per_batch", [
-    (lambda: scenes.DispersiveFractal(160, 92), 4),
-    (lambda: scenes.PlainSphere(96, 96), 4),
-])
-def test_statistical_agreement_independent_seeds(gpu_ctx, scene_factory, frames_per_batch, kernel):
-    """GPU and oracle with independent seeds agree within Monte Carlo error: image mean luminance
-    within 0.5%; per-pixel luminance differences beyond 3 standard errors in at most 5% of pixels
-    (16 GPU batches give the per-pixel variance; caustic and firefly pixels of the dispersive glass
-    under a small sun have heavy-tailed estimators whose 16-batch variance underestimates the spread,
-    so more than the Gaussian 0.3-0.9% exceed 3 SE); and over 4x4-pixel tiles, whose means are
-    closer to Gaussian, in at most 2% of tiles."""
-    batches = 16
+STAT_SCENES = {
+    "c1": lambda: scenes.DispersiveFractal(160, 92),
+    "c0": lambda: scenes.PlainSphere(96, 96),
+    "c2": lambda: scenes.VolumetricSubsurface(64, 64),
+}
+
+
+def _gpu_batches(ctx, factory, kernel, batches, frames, seed0):
     ys = []
     for b in range(batches):
-        s, img = gpu_render(gpu_ctx, scene_factory(), frames_per_batch, seed=1000 + b, kernel_mode=KERNELS[kernel])
+        s, img = gpu_render(ctx, factory(), frames, seed=seed0 + b, kernel_mode=KERNELS[kernel])
         ys.append(img[..., 1].reshape(-1))
-        gpu_ctx.destroy_job(s.job_id())
-    ys = np.array(ys, np.float64)
-    g_mean = ys.mean(0)
-    var_b = ys.var(0, ddof=1)  # variance of a frames_per_batch-frame mean
-    h = host("c0")
+        ctx.destroy_job(s.job_id())
+    return np.array(ys, np.float64)
+
+
+def _oracle_batches(factory, batches, frames, seed0):
     from snelly_b200.testing import HostSnelly
-    h = HostSnelly(scene_factory(), seed=777)
-    pix = np.arange(h.width * h.height)
-    of = 4 * frames_per_batch
-    xyz, mean, _ = oracle_render(h, pix, of)
-    o_mean = xyz[:, 1] / of
-    se = np.sqrt(var_b / batches + var_b * frames_per_batch / of)
-    mask = se > 0
-    z = np.abs(g_mean - o_mean)[mask] / se[mask]
-    frac = (z > 3).mean()
-    lum_g, lum_o = g_mean.mean(), o_mean.mean()
-    # 4x4 tiles: batch means of the tile average, the same test
-    H, W = h.height, h.width
+    ys = []
+    for b in range(batches):
+        h = HostSnelly(factory(), seed=seed0 + b)
+        xyz, _, _ = oracle_render(h, np.arange(h.width * h.height), frames)
+        ys.append(xyz[:, 1] / frames)
+    return np.array(ys, np.float64), h.height, h.width
+
+
+def _welch(a, b):
+    """|mean difference| / standard error per column (Welch), and the zero-variance mask."""
+    se = np.sqrt(a.var(0, ddof=1) / len(a) + b.var(0, ddof=1) / len(b))
+    m = se > 0
+    return np.abs(a.mean(0) - b.mean(0))[m] / se[m], m
+
+
+@pytest.mark.parametrize("kernel", sorted(KERNELS))
+@pytest.mark.parametrize("scene", sorted(STAT_SCENES))
+def test_statistical_agreement_independent_seeds(gpu_ctx, scene, kernel):
+    """Production GPU module and the oracle with independent seeds agree within Monte Carlo error
+    at matched spp: 16 batches of 4 frames on each side (64 spp), per-pixel luminance compared with
+    Welch's two-sample statistic. Bars: the image mean luminance within 4 standard errors of the
+    difference (about 0.5-1% at these sizes); per pixel, at most 1.5% of pixels beyond 3 standard
+    errors (0.27% for a Gaussian; caustic and subsurface pixels have heavy-tailed estimators, and
+    two independent GPU runs show 0.4-0.6% here) and at most 0.1% beyond 5; over 4x4-pixel tiles at
+    most 2% beyond 3 standard errors and none beyond 6. Pixels with zero variance on both sides
+    must agree exactly."""
+    factory = STAT_SCENES[scene]
+    batches, frames = 16, 4
+    g = _gpu_batches(gpu_ctx, factory, kernel, batches, frames, 1000)
+    o, H, W = _oracle_batches(factory, batches, frames, 5000)
+    gm, om = g.mean(1), o.mean(1)  # image means of each batch
+    se_img = np.sqrt(gm.var(ddof=1) / batches + om.var(ddof=1) / batches)
+    z, m = _welch(g, o)
+
     def tiles(a):
-        a = a.reshape(*a.shape[:-1], H // 4, 4, W // 4, 4)
-        return a.mean(axis=(-1, -3)).reshape(*a.shape[:-4], -1)
-    yt = tiles(ys)
-    ot = tiles(o_mean)
-    tvar = yt.var(0, ddof=1)
-    tse = np.sqrt(tvar / batches + tvar * frames_per_batch / of)
-    tz = np.abs(yt.mean(0) - ot)[tse > 0] / tse[tse > 0]
-    tfrac = (tz > 3).mean()
-    msg = f"pixels beyond 3 SE {frac:.4f}, tiles {tfrac:.4f}, mean lum gpu {lum_g:.6f} oracle {lum_o:.6f}"
-    assert abs(lum_g - lum_o) / lum_o <= 5e-3, msg
-    assert frac <= 0.05, msg
-    assert tfrac <= 0.02, msg
-    assert (np.abs(g_mean - o_mean)[~mask] < 1e-5).all()
+        return a.reshape(a.shape[0], H // 4, 4, W // 4, 4).mean(axis=(2, 4)).reshape(a.shape[0], -1)
+
+    tz, _ = _welch(tiles(g), tiles(o))
+    msg = (f"image mean gpu {gm.mean():.6f} oracle {om.mean():.6f} (SE {se_img:.2e}); pixels beyond 3/5 SE "
+           f"{(z > 3).mean():.4f}/{(z > 5).mean():.5f}; tiles beyond 3/6 SE {(tz > 3).mean():.4f}/{(tz > 6).mean():.4f}")
+    assert abs(gm.mean() - om.mean()) <= 4 * se_img, msg
+    assert (z > 3).mean() <= 0.015, msg
+    assert (z > 5).mean() <= 0.001, msg
+    assert (tz > 3).mean() <= 0.02, msg
+    assert (tz > 6).sum() == 0, msg
+    assert (np.abs(g.mean(0) - o.mean(0))[~m] < 1e-5).all(), msg
 
 
 def test_kahan_vs_fp64_accumulation(gpu_ctx):

@@ -33,6 +33,16 @@ def test_firsthit_oracle_matches_reference_golden(name):
     np.testing.assert_array_equal(oracle_firsthit(h, 3, pix, 1), g["pick"])
 
 
+def test_tonemap_oracle_matches_reference_golden():
+    """The display-transform restatement reproduces the reference's tonemapper program bit for bit
+    on path-traced and out-of-gamut / HDR inputs, for three display settings."""
+    g = np.load(f"{GOLDEN}/tm_golden.npz")
+    lib = oracle_for(host("c0"))
+    for k, p in enumerate(g["params"]):
+        out = lib.tonemap(g["xyzn"], p)
+        np.testing.assert_array_equal(out, g["rgba"][k])
+
+
 def test_seeding_is_deterministic_and_in_range():
     h = host("c0")
     lib = oracle_for(h)
