@@ -202,6 +202,21 @@ int snelly_flush_l2(snelly_ctx* ctx, size_t bytes);
  * CDF of the emission spectrum over 390..750 nm (js/spectra.js:28-61). */
 int snelly_inverse_cdf(const snelly_spectrum* s, float* out);
 
+/* snelly_image_stats without any device allocation. No counterpart in the reference (whose host
+ * reads statistics back through gl.readPixels).
+ * Same results as snelly_image_stats up to the summation order of the double-precision sums; for
+ * callers that cannot allocate device memory at that point: a serving loop whose HBM budget is fully
+ * committed to resident jobs (the budgeted allocator would refuse the scratch), and code that must
+ * not call cudaFree, which synchronises the whole device. Its scratch is a fixed 160 KiB of
+ * file-scope device memory per device (4096 partial records), so it handles jobs of at most
+ * 4096 x 2048 = 8,388,608 pixels and returns SNELLY_EINVAL, naming the limit, for larger ones.
+ * The first call on a device looks up the scratch address (cudaGetSymbolAddress, with that device
+ * made current for the lookup); make that first call before any stream capture. The scratch is
+ * shared by every context and thread of the process on that device, so overlapping calls race;
+ * calls through one context are serialised by the context. It clears its completion counter
+ * before each launch and allocates nothing (no cudaMalloc, cudaFree or allocating library call). */
+int snelly_image_stats_static(snelly_ctx* ctx, uint64_t job_id, double* out5);
+
 /* Display transform of a job's mean image: shaders/tonemapper-fragment-shader.glsl as uploaded by
  * Renderer.render (js/renderer.js:619-638): XYZ -> linear sRGB, gamut shift, pow(., invGamma),
  * 2^exposure, L/(1+L), saturation, contrast, hue shift. Fields are the shader's uniforms (the

@@ -89,6 +89,68 @@ __global__ void selftest_rng_quotients(unsigned long long* bad) {
   if (n) atomicAdd(bad, n);
 }
 
+// ---- image statistics without allocation ------------------------------------------------------
+// Scratch of snelly_image_stats_static, in file-scope device memory so that entry point allocates
+// nothing: one partial record (5 doubles) per block for up to kStaticStatsMaxBlocks blocks of
+// kStaticStatsPixelsPerBlock pixels, the folded result, and the completion counter of the
+// last-block fold (which must start at zero). 160 KiB per device.
+constexpr int kStaticStatsMaxBlocks = 4096;
+constexpr int kStaticStatsPixelsPerThread = 8;
+constexpr int kStaticStatsPixelsPerBlock = kStatsThreads * kStaticStatsPixelsPerThread;
+constexpr long long kStaticStatsMaxPixels = (long long)kStaticStatsMaxBlocks * kStaticStatsPixelsPerBlock;
+struct StaticStatsScratch {
+  double partial[5 * kStaticStatsMaxBlocks];
+  double result[8];
+  unsigned int done_blocks;
+};
+static __device__ __align__(256) StaticStatsScratch g_static_stats_scratch;
+
+// One launch: block b reduces pixels [b * 2048, (b + 1) * 2048) into partial[b] (same per-pixel
+// terms as image_stats_partial), and the last block to finish folds the partials in block order
+// into result and resets the counter.
+__global__ void __launch_bounds__(kStatsThreads) image_stats_static(const float4* __restrict__ acc,
+                                                                     const float4* __restrict__ comp, long long npix,
+                                                                     StaticStatsScratch* __restrict__ scratch) {
+  __shared__ double sh[5][kStatsThreads];
+  __shared__ bool last;
+  double a[5] = {0, 0, 0, 0, 0};
+  const long long base = (long long)blockIdx.x * kStaticStatsPixelsPerBlock;
+  for (int k = 0; k < kStaticStatsPixelsPerThread; ++k) {
+    long long i = base + (long long)k * kStatsThreads + threadIdx.x;
+    if (i >= npix) break;
+    float4 s = acc[i], c = comp[i];
+    double n = s.w;
+    if (n > 0) {
+      double x = ((double)s.x - c.x) / n, y = ((double)s.y - c.y) / n, z = ((double)s.z - c.z) / n;
+      a[0] += x;
+      a[1] += y;
+      a[2] += z;
+      a[3] += y * y;
+    }
+    a[4] += n;
+  }
+  for (int k = 0; k < 5; ++k) sh[k][threadIdx.x] = a[k];
+  __syncthreads();
+  for (int w = kStatsThreads / 2; w > 0; w >>= 1) {
+    if ((int)threadIdx.x < w)
+      for (int k = 0; k < 5; ++k) sh[k][threadIdx.x] += sh[k][threadIdx.x + w];
+    __syncthreads();
+  }
+  if (threadIdx.x < 5) scratch->partial[5 * blockIdx.x + threadIdx.x] = sh[threadIdx.x][0];
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) last = atomicAdd(&scratch->done_blocks, 1u) == gridDim.x - 1;
+  __syncthreads();
+  if (!last) return;
+  __threadfence();
+  if (threadIdx.x < 5) {
+    double t = 0;
+    for (unsigned b = 0; b < gridDim.x; ++b) t += __ldcg(&scratch->partial[5 * b + threadIdx.x]);
+    scratch->result[threadIdx.x] = t;
+  }
+  if (threadIdx.x == 0) scratch->done_blocks = 0;
+}
+
 __global__ void l2_flush_kernel(float4* buf, size_t n, float v) {
   size_t stride = (size_t)gridDim.x * blockDim.x;
   for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) buf[i] = make_float4(v, v, v, v);
@@ -183,6 +245,54 @@ int snelly_selftest(snelly_ctx* ctx, int which, uint64_t* mismatches) {
   c.release(cnt);
   if (e != cudaSuccess) return snelly::fail(SNELLY_EDEVICE, std::string("self-test: ") + cudaGetErrorString(e));
   *mismatches = h;
+  return SNELLY_OK;
+}
+
+// Device address of g_static_stats_scratch per device, looked up once (with that device current).
+static std::mutex g_static_scratch_mu;
+static StaticStatsScratch* g_static_scratch_ptr[64];
+
+int snelly_image_stats_static(snelly_ctx* ctx, uint64_t job_id, double* out5) {
+  if (!ctx || !out5) return snelly::fail(SNELLY_EINVAL, "null argument to snelly_image_stats_static");
+  snelly::Context& c = *ctx->c;
+  std::lock_guard<std::mutex> lk(c.mu);
+  auto it = c.jobs.find(job_id);
+  if (it == c.jobs.end()) return snelly::fail(SNELLY_ENOTFOUND, "unknown job id");
+  snelly::Job& j = it->second;
+  const long long npix = (long long)j.desc.width * j.desc.height;
+  if (npix > kStaticStatsMaxPixels)
+    return snelly::fail(SNELLY_EINVAL, "snelly_image_stats_static handles at most " + std::to_string(kStaticStatsMaxPixels) +
+                                           " pixels (its fixed scratch has " + std::to_string(kStaticStatsMaxBlocks) +
+                                           " partial records); this job has " + std::to_string(npix));
+  if (c.device < 0 || c.device >= 64) return snelly::fail(SNELLY_EINVAL, "device index out of range");
+  StaticStatsScratch* scratch = nullptr;
+  {
+    std::lock_guard<std::mutex> g(g_static_scratch_mu);
+    if (!g_static_scratch_ptr[c.device]) {
+      int prev = -1;
+      cudaError_t e = cudaGetDevice(&prev);
+      if (e == cudaSuccess && prev != c.device) e = cudaSetDevice(c.device);
+      void* p = nullptr;
+      if (e == cudaSuccess) e = cudaGetSymbolAddress(&p, g_static_stats_scratch);
+      if (prev >= 0 && prev != c.device) cudaSetDevice(prev);
+      if (e != cudaSuccess || !p)
+        return snelly::fail(SNELLY_EDEVICE, std::string("cudaGetSymbolAddress of the statistics scratch: ") +
+                                                cudaGetErrorString(e));
+      g_static_scratch_ptr[c.device] = (StaticStatsScratch*)p;
+    }
+    scratch = g_static_scratch_ptr[c.device];
+  }
+  const int blocks = (int)std::max<long long>(1, (npix + kStaticStatsPixelsPerBlock - 1) / kStaticStatsPixelsPerBlock);
+  cudaError_t e = cudaMemsetAsync(&scratch->done_blocks, 0, sizeof(unsigned int), c.stream);
+  if (e == cudaSuccess) {
+    image_stats_static<<<blocks, kStatsThreads, 0, c.stream>>>((const float4*)j.acc.ptr, (const float4*)j.comp.ptr,
+                                                               npix, scratch);
+    c.launches += 1;
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess) e = cudaMemcpyAsync(out5, scratch->result, 5 * sizeof(double), cudaMemcpyDeviceToHost, c.stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(c.stream);
+  if (e != cudaSuccess) return snelly::fail(SNELLY_EDEVICE, std::string("image statistics failed: ") + cudaGetErrorString(e));
   return SNELLY_OK;
 }
 
