@@ -41,7 +41,8 @@ def parse():
     ap.add_argument("--steps", type=int, default=12)
     ap.add_argument("--warmup", type=int, default=4)
     ap.add_argument("--impl", choices=["snelly", "reference"], default="snelly")
-    ap.add_argument("--kernel", choices=["mega", "wavefront"], default=None)
+    ap.add_argument("--kernel", choices=["auto", "mega", "wavefront"], default="auto",
+                    help="integrator (auto: the library's autotuner picks per scene and image size)")
     ap.add_argument("--width", type=int, default=1920)
     ap.add_argument("--height", type=int, default=1080)
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="budget of the CPU baseline sample")
@@ -237,9 +238,9 @@ def gpu_arm(args, rank, world, local_rank):
     peak_tflops, _ = ctx.fp32_peak()
     s = api.Snelly(workload_scene(args), context=ctx)
     s.seed = 1 + rank
-    if args.kernel:
-        s.pathtracer.kernelMode = N.KERNEL_WAVEFRONT if args.kernel == "wavefront" else N.KERNEL_MEGA
-    s.render(0)  # compile, allocate, seed
+    s.pathtracer.kernelMode = {"auto": N.KERNEL_AUTO, "mega": N.KERNEL_MEGA, "wavefront": N.KERNEL_WAVEFRONT}[args.kernel]
+    s.render(0)  # compile, allocate, seed (and, for --kernel auto, the autotuner's trial frames)
+    kernel_used = "wavefront" if ctx.job_kernel(s.job_id()) == N.KERNEL_WAVEFRONT else "mega"
     W, H = s.width, s.height
     samples_per_step = W * H * int(round(s.pathtracer.maxSamplesPerFrame))
     stream = torch.cuda.ExternalStream(ctx.stream())
@@ -290,7 +291,7 @@ def gpu_arm(args, rank, world, local_rank):
         fpp, spp_special, counted = flops_per_path(host)
         per_launch_ms = statistics.mean(step_ms)
         achieved = fpp * samples_per_step / (per_launch_ms / 1000.0) / 1e12
-        kname = "pt_frame_mega" if (args.kernel or "mega") == "mega" else "pt_wavefront"
+        kname = "pt_frame_mega" if kernel_used == "mega" else "pt_wavefront"
         cpu = None if args.no_cpu_baseline else cpu_baseline(host, args.cpu_seconds)
         out = {
             "metric": METRIC, "value": value, "unit": "path samples/s", "n_gpus": world, "steps": args.steps,
@@ -299,7 +300,7 @@ def gpu_arm(args, rank, world, local_rank):
             "data": "synthetic (procedural SDF scene, seeded camera; no dataset)",
             "config": {"workload": WORKLOAD, "width": W, "height": H, "spp_per_step": 1, "image_spp": 64,
                        "max_bounces": 8, "max_march_steps": 512, "dispersive": True,
-                       "kernel": args.kernel or "mega", "math": "fast",
+                       "kernel": kernel_used, "kernel_choice": args.kernel, "math": "fast",
                        "l2": "flushed between timed steps (256 MiB write)", "parallelism": f"replicas x{world}"},
             "e2e": {"value": e2e_value, "unit": "path samples/s", "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": W * H * 16},

@@ -174,6 +174,10 @@ int snelly_pick(snelly_ctx* ctx, uint64_t scene_id, const snelly_render_desc* de
  * and compensations (4 floats each per pixel); acc64 (4 doubles per pixel) when enabled, else
  * may be NULL. Waits for the job. */
 int snelly_readback_state(snelly_ctx* ctx, uint64_t job_id, uint32_t* rng, float* acc, float* comp, double* acc64);
+/* The integrator a job's frames run: SNELLY_KERNEL_MEGA or SNELLY_KERNEL_WAVEFRONT (a scene
+ * created with SNELLY_KERNEL_AUTO gets the autotuner's choice for its module and image size:
+ * one warm-up and two timed frames of each integrator, once per size class). */
+int snelly_job_kernel(snelly_ctx* ctx, uint64_t job_id, int* kernel_mode);
 /* Start a job from saved state instead of seeding (resume). */
 int snelly_restore(snelly_ctx* ctx, uint64_t scene_id, const snelly_render_desc* desc, const uint32_t* rng,
                    const float* acc, const float* comp, uint64_t* job_id);

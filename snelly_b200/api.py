@@ -303,6 +303,7 @@ class Shader:
 
     def __init__(self):
         self.calls = {}
+        self.textures = {}
 
     def _put(self, name, typ, vals):
         self.calls[name] = (typ, vals)
@@ -336,6 +337,11 @@ class Shader:
 
     def uniformMatrix3Fv(self, name, v):
         self._put(name, N.U_MAT3, [float(x) for x in v])
+
+    def uniformTexture(self, name, texture, linear=True):
+        """Bind a texture array to a sampler2D / sampler3D uniform: (h, w, c) or (d, h, w, c) of
+        float32, float16 or uint8 (js/gl.js:262 binds a GLU.Texture the same way)."""
+        self.textures[name] = (texture, linear)
 
 
 # ---------------------------------------------------------------------------------------------
@@ -391,7 +397,7 @@ class Renderer:
         self.spp = 0.0
         # B200 build options (no reference counterpart)
         self.mathMode = N.MATH_FAST
-        self.kernelMode = N.KERNEL_MEGA
+        self.kernelMode = N.KERNEL_AUTO  # autotuned per scene module and image size
 
     def sun_dir(self):
         """updateSunDir, js/renderer.js:371-383."""
@@ -528,7 +534,7 @@ class Snelly:
         opts = self.scene_opts()
         key = (glsl, bytes(opts))
         if key != self._scene_key:
-            self._scene_id = self._ctx.create_scene(glsl, opts)
+            self._scene_id = self._ctx.scene_for(glsl, opts)
             self._scene_key = key
         return self._scene_id
 
@@ -576,11 +582,22 @@ class Snelly:
         self.materials.syncShader(p, self)
         return p
 
-    def scene_uniforms(self):
+    def scene_shader(self):
+        """The scene's syncShader calls, recorded (uniforms and textures)."""
         sh = Shader()
         if hasattr(self.sceneObj, "syncShader"):
             self.sceneObj.syncShader(self, sh)
-        return sh.calls
+        return sh
+
+    def scene_uniforms(self):
+        return self.scene_shader().calls
+
+    def sync_scene(self, sid):
+        """Upload the scene's uniforms and textures (Scene.syncShader, js/renderer.js:604-608)."""
+        sh = self.scene_shader()
+        self._ctx.set_uniforms(sid, sh.calls)
+        for name, (tex, linear) in sh.textures.items():
+            self._ctx.set_texture(sid, name, tex, linear)
 
     def render_desc(self, frames):
         d = N.RenderDesc()
@@ -611,7 +628,7 @@ class Snelly:
             self.sceneObj.preframeCallback(self, None)
         if self._job is None:
             sid = self.compileShaders()
-            self._ctx.set_uniforms(sid, self.scene_uniforms())
+            self.sync_scene(sid)
             self._job = self._ctx.render(sid, self.render_desc(frames))
         else:
             self._ctx.advance(self._job, frames)
@@ -623,7 +640,7 @@ class Snelly:
         """Renderer.pick: {"distance", "material"} of the first hit along the pinhole ray through
         pixel coordinate (xPick, yPick) (gl_FragCoord units; a miss gives maxLengthScale and -1)."""
         sid = self.compileShaders()
-        self._ctx.set_uniforms(sid, self.scene_uniforms())
+        self.sync_scene(sid)
         d, m = self._ctx.pick(sid, self.render_desc(1), xPick, yPick)
         return {"distance": d, "material": m}
 
@@ -665,6 +682,16 @@ class Context:
         h = ctypes.c_void_p()
         N.check(self._lib.snelly_init(ctypes.byref(h), int(device), int(hbm_budget)))
         self._h = h
+        self._scene_cache = {}  # (scene GLSL, options) -> scene id, shared by Snelly objects
+        self._bound = {}        # (scene id, sampler name) -> the array object uploaded last
+
+    def scene_for(self, glsl, opts):
+        """The scene id for a scene source and options, created on first use (one module and one
+        set of scene textures however many jobs render it)."""
+        key = (glsl, bytes(opts))
+        if key not in self._scene_cache:
+            self._scene_cache[key] = self.create_scene(glsl, opts)
+        return self._scene_cache[key]
 
     def close(self):
         if self._h:
@@ -690,6 +717,8 @@ class Context:
 
     def destroy_scene(self, sid):
         N.check(self._lib.snelly_destroy_scene(self._h, sid))
+        self._scene_cache = {k: v for k, v in self._scene_cache.items() if v != sid}
+        self._bound = {k: v for k, v in self._bound.items() if k[0] != sid}
 
     def set_uniforms(self, sid, calls):
         if not calls:
@@ -712,6 +741,9 @@ class Context:
         N.check(self._lib.snelly_set_uniforms(self._h, sid, arr, len(calls)))
 
     def set_texture(self, sid, name, array, linear=True):
+        if self._bound.get((sid, name)) is array:
+            return  # this very array is bound already
+        self._bound[(sid, name)] = array
         a = np.ascontiguousarray(array)
         fmt = {np.dtype(np.float32): 0, np.dtype(np.float16): 1, np.dtype(np.uint8): 2}[a.dtype]
         if a.ndim == 3:  # (h, w, c) 2-D texture
@@ -742,6 +774,12 @@ class Context:
         ids = (ctypes.c_uint64 * len(jobs_frames))(*jobs_frames.keys())
         fr = (ctypes.c_int * len(jobs_frames))(*jobs_frames.values())
         N.check(self._lib.snelly_advance_batch(self._h, ids, fr, len(jobs_frames)))
+
+    def job_kernel(self, jid):
+        """The integrator the job runs: N.KERNEL_MEGA or N.KERNEL_WAVEFRONT."""
+        k = ctypes.c_int()
+        N.check(self._lib.snelly_job_kernel(self._h, jid, ctypes.byref(k)))
+        return k.value
 
     def tonemap(self, jid, width, height, params, fmt=N.TONEMAP_RGBA8):
         """The job's mean image through the display transform: (H, W, 4) uint8 (RGBA8) or float32

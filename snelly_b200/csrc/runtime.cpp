@@ -373,7 +373,7 @@ int Context::enqueue_frames(Job& j, int frames) {
   void* args[] = {&tables, &bstart, &njobs, &gparams};
   for (int f = 0; f < frames; ++f) {
     if (j.desc.mode == SNELLY_MODE_PT) {
-      if (j.scene->kernel_mode == SNELLY_KERNEL_WAVEFRONT && m.f_wf_generate) {
+      if (j.kernel_mode == SNELLY_KERNEL_WAVEFRONT && m.f_wf_generate) {
         rc = enqueue_wavefront_frame(j);
       } else {
         rc = launch(m.f_frame_mega, j.blocks, SNELLY_BLOCK, args);
@@ -504,8 +504,10 @@ Context::~Context() {
     cudaStreamDestroy(L.stream);
   }
   for (auto& kv : jobs) free_job(kv.second);
-  for (auto& kv : scenes)
+  for (auto& kv : scenes) {
     for (auto& t : kv.second.textures) release(t.second);
+    for (auto& t : kv.second.retired_textures) release(t);
+  }
   release(xyz);
   release(stats_scratch);
   for (auto& kv : module_cache) cudaLibraryUnload(kv.second->lib);
@@ -604,8 +606,10 @@ int snelly_create_scene(snelly_ctx* ctx, const char* glsl, const snelly_scene_op
   s.opts = o;
   // The wavefront integrator serves one sample per pixel per frame (the reference default);
   // more samples per frame consume one pixel's RNG stream sequentially and use the per-pixel kernel.
-  s.kernel_mode = (o.kernel_mode == SNELLY_KERNEL_WAVEFRONT && o.max_samples_per_frame == 1) ? SNELLY_KERNEL_WAVEFRONT
-                                                                                              : SNELLY_KERNEL_MEGA;
+  // SNELLY_KERNEL_AUTO is decided per job by the autotuner (wavefront.cpp).
+  s.kernel_mode = o.max_samples_per_frame == 1 && (o.kernel_mode == SNELLY_KERNEL_WAVEFRONT || o.kernel_mode == SNELLY_KERNEL_AUTO)
+                      ? o.kernel_mode
+                      : SNELLY_KERNEL_MEGA;
   std::string nvlog;
   rc = c.compile_module(program_source(s.src), o.math_mode, &s.module, &nvlog);
   if (log && log_cap) snprintf(log, log_cap, "%s", rc ? t_last_error.c_str() : nvlog.c_str());
@@ -626,6 +630,7 @@ int snelly_destroy_scene(snelly_ctx* ctx, uint64_t scene_id) {
   for (auto& kv : c.jobs)
     if (kv.second.scene == &it->second) return fail(SNELLY_EBUSY, "scene has live jobs");
   for (auto& t : it->second.textures) c.release(t.second);
+  for (auto& t : it->second.retired_textures) c.release(t);
   c.scenes.erase(it);
   return SNELLY_OK;
 }
@@ -683,7 +688,17 @@ int snelly_set_texture(snelly_ctx* ctx, uint64_t scene_id, const char* name, con
   size_t esz = fmt == 0 ? 4 : (fmt == 1 ? 2 : 1);
   size_t bytes = (size_t)w * h * d * channels * esz;
   DevBuf& b = s.textures[name];
-  c.release(b);
+  // Jobs of this scene hold the old texture's address in their uniform snapshot: it stays
+  // allocated until the scene is destroyed (which needs the jobs gone).
+  bool referenced = false;
+  for (auto& kv : c.jobs)
+    if (kv.second.scene == &s) referenced = true;
+  if (referenced && b.ptr) {
+    s.retired_textures.push_back(b);
+    b = DevBuf{};
+  } else {
+    c.release(b);
+  }
   int rc = c.alloc(b, bytes);
   if (rc) return rc;
   RT_TRY(cudaMemcpy(b.ptr, data, bytes, cudaMemcpyHostToDevice));
@@ -785,8 +800,11 @@ static int start_job(Context& c, uint64_t scene_id, const snelly_render_desc* de
   if (cudaEventCreateWithFlags(&j.done, cudaEventDisableTiming) != cudaSuccess)
     return bail(fail(SNELLY_EDEVICE, "event creation failed"));
   if ((rc = c.single_job_tables(j))) return bail(rc);
-  if (s.kernel_mode == SNELLY_KERNEL_WAVEFRONT && desc->mode == SNELLY_MODE_PT && (rc = c.alloc_wavefront(j)))
-    return bail(rc);
+  j.kernel_mode = SNELLY_KERNEL_MEGA;
+  if (desc->mode == SNELLY_MODE_PT && s.kernel_mode != SNELLY_KERNEL_MEGA && j.module->f_wf_generate)
+    j.kernel_mode = s.kernel_mode;
+  if (j.kernel_mode != SNELLY_KERNEL_MEGA && (rc = c.alloc_wavefront(j))) return bail(rc);
+  if (j.kernel_mode == SNELLY_KERNEL_AUTO && (rc = c.autotune(j))) return bail(rc);
   if (rng) {
     if (cudaMemcpy(j.rng.ptr, rng, npix * 16, cudaMemcpyHostToDevice) != cudaSuccess ||
         cudaMemcpy(j.acc.ptr, acc, npix * 16, cudaMemcpyHostToDevice) != cudaSuccess ||
@@ -945,6 +963,16 @@ int snelly_readback_state(snelly_ctx* ctx, uint64_t job_id, uint32_t* rng, float
     if (!j.acc64.ptr) return fail(SNELLY_EINVAL, "job has no FP64 accumulation");
     RT_TRY(cudaMemcpy(acc64, j.acc64.ptr, npix * 32, cudaMemcpyDeviceToHost));
   }
+  return SNELLY_OK;
+}
+
+int snelly_job_kernel(snelly_ctx* ctx, uint64_t job_id, int* kernel_mode) {
+  if (!ctx || !kernel_mode) return fail(SNELLY_EINVAL, "null argument to snelly_job_kernel");
+  Context& c = *ctx->c;
+  std::lock_guard<std::mutex> lk(c.mu);
+  auto it = c.jobs.find(job_id);
+  if (it == c.jobs.end()) return fail(SNELLY_ENOTFOUND, "unknown job id");
+  *kernel_mode = it->second.kernel_mode;
   return SNELLY_OK;
 }
 

@@ -59,6 +59,7 @@ struct Scene {
   int kernel_mode = SNELLY_KERNEL_MEGA;
   std::vector<unsigned char> ublock;  // uniform block (host copy), snapshotted by jobs
   std::map<std::string, DevBuf> textures;
+  std::vector<DevBuf> retired_textures;  // replaced while jobs referenced them; freed with the scene
   std::shared_ptr<Module> module;
   // IEEE-mode build of the same program for the first-hit passes (normals, AO, pick), compiled on
   // first use when `module` is a fast-math build: those passes are deterministic and must agree
@@ -79,6 +80,7 @@ struct Job {
   DevBuf wf;  // wavefront path state and queues
   WfBuffers wfb{};
   int blocks = 0;
+  int kernel_mode = SNELLY_KERNEL_MEGA;  // the integrator this job's frames run (after tuning)
   int pick_at = 0;           // a one-pixel pick job (snelly_pick)
   float pick_x = 0.0f, pick_y = 0.0f;
   int frames_enqueued = 0;
@@ -108,6 +110,7 @@ struct Context {
   uint64_t launches = 0;
   std::string csrc_dir, kernel_dir, include_dir, cache_dir;
   std::vector<BatchLane> lanes;  // batch streams (created on first use)
+  std::map<std::string, int> tuned;  // autotuner decisions: (module, image-size class) -> integrator
   DevBuf stats_scratch;          // image-statistics partial sums
 
   ~Context();
@@ -124,6 +127,7 @@ struct Context {
   int alloc_wavefront(Job& j);
   void release_wavefront(Job& j);
   int enqueue_wavefront_frame(Job& j);
+  int autotune(Job& j);
 };
 
 int assemble_scene(const std::string& glsl, const snelly_scene_opts& o, SceneSource* out);

@@ -65,4 +65,54 @@ int Context::enqueue_wavefront_frame(Job& j) {
   return SNELLY_OK;
 }
 
+// The integrator choice of SNELLY_KERNEL_AUTO: per (scene module, image-size class) the first job
+// times one warm-up and two frames of each integrator on its own buffers, keeps the faster and
+// caches the decision; the job's state is seeded again afterwards by the caller. The size class is
+// the power of two nearest the pixel count (tail effects make the choice size-dependent).
+int Context::autotune(Job& j) {
+  const long long npix = (long long)j.desc.width * j.desc.height;
+  int cls = 0;
+  while ((1ll << (cls + 1)) <= npix) ++cls;
+  if (npix - (1ll << cls) > (1ll << (cls + 1)) - npix) ++cls;
+  const std::string key = j.module->key + "/" + std::to_string(cls);
+  auto it = tuned.find(key);
+  int best;
+  if (it != tuned.end()) {
+    best = it->second;
+  } else {
+    int rc = upload_slot(j, 0);
+    if (rc) return rc;
+    void* tables = j.tables.ptr;
+    void* bstart = (char*)j.tables.ptr + 128;
+    int njobs = 1;
+    void* gparams = j.gparams.ptr;
+    void* sargs[] = {&tables, &bstart, &njobs};
+    void* margs[] = {&tables, &bstart, &njobs, &gparams};
+    if ((rc = launch(j.module->f_seed, j.blocks, SNELLY_BLOCK, sargs))) return rc;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    if (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess) {
+      if (e0) cudaEventDestroy(e0);
+      return fail(SNELLY_EDEVICE, "autotune event creation failed");
+    }
+    float ms[2] = {0.0f, 0.0f};
+    for (int k = 0; k < 2 && !rc; ++k) {
+      for (int f = 0; f < 3 && !rc; ++f) {
+        if (f == 1) cudaEventRecord(e0, stream);
+        rc = k == 0 ? launch(j.module->f_frame_mega, j.blocks, SNELLY_BLOCK, margs) : enqueue_wavefront_frame(j);
+      }
+      cudaEventRecord(e1, stream);
+      if (!rc && cudaEventSynchronize(e1) != cudaSuccess) rc = fail(SNELLY_EDEVICE, "autotune timing failed");
+      if (!rc) cudaEventElapsedTime(&ms[k], e0, e1);
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (rc) return rc;
+    best = ms[1] < ms[0] ? SNELLY_KERNEL_WAVEFRONT : SNELLY_KERNEL_MEGA;
+    tuned[key] = best;
+  }
+  j.kernel_mode = best;
+  if (best == SNELLY_KERNEL_MEGA) release_wavefront(j);
+  return SNELLY_OK;
+}
+
 }  // namespace snelly

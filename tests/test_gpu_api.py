@@ -91,3 +91,30 @@ def test_native_kernels_ran(gpu_ctx):
     before = gpu_ctx.launch_count()
     gpu_render(gpu_ctx, scenes.PlainSphere(32, 32), 3)
     assert gpu_ctx.launch_count() >= before + 4  # seed + 3 frames + resolve
+
+
+def test_autotuned_kernel_choice_leaves_no_trace(gpu_ctx):
+    """A scene created with SNELLY_KERNEL_AUTO runs the autotuner's trial frames on the job's own
+    buffers, then seeds the job again: its image equals a render with the chosen integrator set
+    explicitly, bit for bit; the decision is cached per module and size class."""
+    from snelly_b200 import api
+    from snelly_b200 import _native as N
+
+    def run(kmode):
+        s = api.Snelly(scenes.DispersiveFractal(96, 54), context=gpu_ctx)
+        s.seed = 9
+        s.pathtracer.kernelMode = kmode
+        s.render(3)
+        img = s.readback().copy()
+        k = gpu_ctx.job_kernel(s.job_id())
+        gpu_ctx.destroy_job(s.job_id())
+        return img, k
+
+    img_auto, k = run(N.KERNEL_AUTO)
+    assert k in (N.KERNEL_MEGA, N.KERNEL_WAVEFRONT)
+    img_explicit, k2 = run(k)
+    assert k2 == k
+    np.testing.assert_array_equal(img_auto, img_explicit)
+    img_again, k3 = run(N.KERNEL_AUTO)
+    assert k3 == k
+    np.testing.assert_array_equal(img_again, img_auto)
