@@ -146,7 +146,8 @@ def cpu_sampler(host, prefer_reference=True):
             return time.perf_counter() - t
         return run, "reference", (keep,)
     p, keep = oracle.host_params(host)
-    ub = oracle.pack_uniforms(lib.cpp, host.scene_uniforms())
+    sh = host.scene_shader()
+    ub = oracle.pack_uniforms(lib.cpp, sh.calls, sh.textures)
 
     def run(n):
         pix = np.sort(rs.choice(W * H, n, replace=False))

@@ -231,7 +231,7 @@ class RefLib:
         size = int(re.search(r"sizeof\(RefShaderUniforms\) == (\d+)", cpp).group(1))
         return lay, size
 
-    def block(self, params, scene_calls, tables):
+    def block(self, params, scene_calls, tables, scene_textures=None):
         """Uniform block bytes: shader uniforms from SnellyParams fields of the same names, IOR
         coefficients, samplers bound to the host tables, scene uniforms from syncShader calls."""
         buf = bytearray(self.size)
@@ -259,13 +259,17 @@ class RefLib:
             if name in self.layout:
                 off = self.layout[name][1]
                 buf[off:off + 32] = struct.pack("<Q6i", ptr, w, h, ch, 0, linear, 0)
+        for name, (arr, linear) in (scene_textures or {}).items():
+            if name in self.layout:
+                off = self.layout[name][1]
+                buf[off:off + 32] = O.sampler_record(self.layout[name][0], arr, linear)
         return bytes(buf)
 
-    def pick(self, params, scene_calls, tables, width, pixels, threads=0):
+    def pick(self, params, scene_calls, tables, width, pixels, threads=0, scene_textures=None):
         """The pick program at the centre of each listed pixel: (n, 2) distance and material."""
         pixels = np.ascontiguousarray(pixels, np.int32)
         out = np.zeros((len(pixels), 4), np.float32)
-        blk = self.block(params, scene_calls, tables)
+        blk = self.block(params, scene_calls, tables, scene_textures)
         ub = ctypes.create_string_buffer(blk, len(blk))
         rc = self.lib.ref_pick(ub, len(blk), self.layout["mousePick"][1], int(width), pixels.ctypes.data, len(pixels),
                                out.ctypes.data, int(threads))
@@ -287,12 +291,12 @@ class RefLib:
         assert rc == 0
         return out
 
-    def render(self, params, scene_calls, tables, width, height, pixels, frames, rng, threads=0):
+    def render(self, params, scene_calls, tables, width, height, pixels, frames, rng, threads=0, scene_textures=None):
         pixels = np.ascontiguousarray(pixels, np.int32)
         n = len(pixels)
         rng = np.ascontiguousarray(rng, np.uint32).copy()
         mean = np.zeros((n, 4), np.float32)
-        blk = self.block(params, scene_calls, tables)
+        blk = self.block(params, scene_calls, tables, scene_textures)
         ub = ctypes.create_string_buffer(blk, len(blk))
         rc = self.lib.ref_render(ub, len(blk), self.layout["Radiance"][1], self.layout["RngData"][1], int(width),
                                  int(height), pixels.ctypes.data, n, int(frames), rng.ctypes.data, mean.ctypes.data,

@@ -130,11 +130,30 @@ def uniform_layout(cpp):
     return out, size
 
 
-def pack_uniforms(cpp, calls):
-    """Uniform block bytes for the recorded shader.uniform* calls ({name: (type, values)})."""
+def sampler_record(kind, array, linear=True):
+    """The 32-byte sampler2D / sampler3D record of glslcompat.h for a texture array ((h, w, c) or
+    (d, h, w, c) of float32 / float16 / uint8): {data pointer, w, h, [d,] channels, format,
+    filter, [srgb]}. The array must stay alive while the record is used."""
+    import struct
+    fmt = {np.dtype(np.float32): 0, np.dtype(np.float16): 1, np.dtype(np.uint8): 2}[array.dtype]
+    if kind == "sampler2D":
+        h, w, c = array.shape
+        return struct.pack("<Q6i", array.ctypes.data, w, h, c, fmt, 1 if linear else 0, 0)
+    d, h, w, c = array.shape
+    return struct.pack("<Q6i", array.ctypes.data, w, h, d, c, fmt, 1 if linear else 0)
+
+
+def pack_uniforms(cpp, calls, textures=None):
+    """Uniform block bytes for the recorded shader.uniform* calls ({name: (type, values)}) and
+    the bound textures ({name: (array, linear)}; the arrays must be contiguous and stay alive)."""
     layout, size = uniform_layout(cpp)
     buf = bytearray(size)
     for name, typ, off, alen in layout:
+        if typ in ("sampler2D", "sampler3D"):
+            if textures and name in textures:
+                arr, linear = textures[name]
+                buf[off:off + 32] = sampler_record(typ, arr, linear)
+            continue
         if name not in calls:
             continue
         _, vals = calls[name]
@@ -281,7 +300,8 @@ def flops_per_path(snelly, pixels=2000, frames=2, seed=5):
     n = snelly.width * snelly.height
     pix = np.sort(np.random.RandomState(seed).choice(n, min(pixels, n), replace=False))
     p, keep = host_params(snelly)
-    ub = pack_uniforms(lib.cpp, snelly.scene_uniforms())
+    sh = snelly.scene_shader()
+    ub = pack_uniforms(lib.cpp, sh.calls, sh.textures)
     lib.counts()
     lib.render(p, ub, snelly.width, snelly.height, pix, frames, lib.seed(snelly.seed, pix), threads=1)
     f, sp = lib.counts()

@@ -393,5 +393,101 @@ void CONSTRUCT_PRIMARY_RAY(in vec2 pixel, inout vec4 rnd, inout vec3 primaryStar
         shader.uniform3Fv("tint", [0.1, 0.6, 0.2])
 
 
+_GRIDS = {}
+
+
+def sphere_blend_grid(res=256, seed=4, count=32, k=0.1, extent=1.5):
+    """The mesh-like distance grid: res^3 float16 samples, at texel centres of the cube
+    [-extent, extent]^3, of the polynomial smooth minimum (blend width k) of `count` sphere
+    distances, radii U(0.1, 0.4) and centres U[-1, 1]^3 drawn from `seed`. Shape (d, h, w, 1),
+    x fastest. Cached per argument set, so every scene instance binds the same array."""
+    key = (res, seed, count, k, extent)
+    if key not in _GRIDS:
+        rs = np.random.RandomState(seed)
+        centres = rs.uniform(-1.0, 1.0, (count, 3)).astype(np.float32)
+        radii = rs.uniform(0.1, 0.4, count).astype(np.float32)
+        c = ((np.arange(res, dtype=np.float32) + 0.5) / res * 2.0 - 1.0) * extent
+        y, x = np.meshgrid(c, c, indexing="ij")
+        grid = np.empty((res, res, res, 1), np.float16)
+        for iz in range(res):
+            d = None
+            for n in range(count):
+                dn = np.sqrt((x - centres[n, 0]) ** 2 + (y - centres[n, 1]) ** 2 + (c[iz] - centres[n, 2]) ** 2) - radii[n]
+                if d is None:
+                    d = dn
+                else:
+                    h = np.maximum(k - np.abs(d - dn), 0.0) / k
+                    d = np.minimum(d, dn) - h * h * k * 0.25
+            grid[iz, :, :, 0] = d
+        _GRIDS[key] = grid
+    return _GRIDS[key]
+
+
+class MeshLike:
+    """C3's mesh-like SDF: a 256^3 float16 distance grid sampled trilinearly (a sampler3D, as the
+    reference's mesh scenes bind theirs), holding the smooth minimum of 32 spheres (radii
+    U(0.1, 0.4), centres U[-1, 1]^3, seed 4), over a ground plane y = -1.6; diffuse grey surface,
+    sky radiance 1 and a sun."""
+
+    width, height, spp = 512, 512, 16
+
+    def __init__(self, width=None, height=None, res=256, seed=4):
+        if width:
+            self.width = width
+        if height:
+            self.height = height
+        self.res, self.seed = res, seed
+
+    def init(self, snelly):
+        r = snelly.getRenderer()
+        r.width, r.height = self.width, self.height
+        r.dispersive = True
+        r.interactive = False
+        r.maxBounces = 6
+        r.maxMarchSteps = 256
+        r.skyPower = 0.0
+        r.sunPower = math.log10(5.0)
+        r.sunAngularSize = 4.0
+        r.sunLatitude = 55.0
+        r.sunLongitude = 20.0
+        cam = snelly.getCamera()
+        cam.fov = 40.0
+        cam.position.set(0.0, 1.5, 5.5)
+        cam.aperture = -math.inf
+        snelly.getControls().target.set(0.0, -0.2, 0.0)
+        s = snelly.getMaterials().loadSurface()
+        s.diffuseAlbedo = [0.7, 0.7, 0.7]
+        s.specAlbedo = [0.04, 0.04, 0.04]
+        s.roughness = 0.4
+
+    def shader(self):
+        return """
+uniform sampler3D sdfTex;
+uniform vec3 gridMin;
+uniform vec3 gridSize;
+
+float sdBox(vec3 X, vec3 bmin, vec3 bmax)
+{
+    vec3 d = abs(X - 0.5*(bmin + bmax)) - 0.5*(bmax - bmin);
+    return min(max(d.x, max(d.y, d.z)), 0.0) + length(max(d, 0.0));
+}
+
+float SDF_SURFACE(vec3 X)
+{
+    float ground = X.y + 1.6;
+    float box = sdBox(X, gridMin, gridMin + gridSize);
+    float mesh;
+    if (box > 0.0) mesh = box + 0.02;  // outside the grid: a lower bound of the distance to its contents
+    else mesh = texture(sdfTex, (X - gridMin) / gridSize).r;
+    return min(mesh, ground);
+}
+"""
+
+    def syncShader(self, snelly, shader):
+        shader.uniformTexture("sdfTex", sphere_blend_grid(self.res, self.seed))
+        shader.uniform3Fv("gridMin", [-1.5, -1.5, -1.5])
+        shader.uniform3Fv("gridSize", [3.0, 3.0, 3.0])
+
+
 SCENES = {"c0": PlainSphere, "c1": DispersiveFractal, "c2": VolumetricSubsurface, "atmosphere": AtmosphereLights,
-          "hooks": HooksAndMaps}
+          "hooks": HooksAndMaps, "mesh": MeshLike}

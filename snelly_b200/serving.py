@@ -23,6 +23,7 @@ from dataclasses import dataclass, field
 
 import numpy as np
 
+from . import _native as N
 from . import api, scenes
 
 JOB_BYTES_PER_PIXEL = 64 + 16  # rng, Kahan sums + compensations, resolved image (+ margin)
@@ -89,6 +90,7 @@ class Server:
                 req = waiting.pop(0)
                 s = api.Snelly(req.scene, context=self.ctx)
                 s.seed = req.seed
+                s.pathtracer.kernelMode = N.KERNEL_MEGA  # batched ticks run the path-per-thread kernel
                 s.render(0)  # allocate + seed
                 used += self.job_bytes(req)
                 active[s.job_id()] = {"req": req, "snelly": s, "spp": 0, "admitted": clock() - t0, "means": []}
@@ -136,9 +138,10 @@ class Server:
 
 
 def serving_requests(rate, duration, seed=5, noise_fraction=0.5, spp_range=(4, 64), res_range=(128, 1024),
-                     scene_names=("c0", "c1", "c2")):
+                     scene_names=("c0", "c1", "c2", "mesh")):
     """A Poisson request stream: arrivals at `rate` per second for `duration` seconds; each request
-    draws a scene, a square resolution (log-uniform), a camera pose on a sphere of radius U(4, 8), a
+    draws a scene (plain sphere, dispersive fractal, volumetric/subsurface Mandelbox, mesh-like
+    distance grid), a square resolution (log-uniform), a camera pose on a sphere of radius U(4, 8), a
     bounce limit U{4..12}, and either a fixed spp U{spp_range} or a 2% relative-noise target."""
     rs = np.random.RandomState(seed)
     t, reqs, rid = 0.0, [], 0

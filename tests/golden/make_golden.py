@@ -41,6 +41,7 @@ CASES = {
     "atmosphere": (lambda: scenes.AtmosphereLights(64, 48), 3),
     "atmosphere_disp": (lambda: scenes.AtmosphereLights(32, 24, dispersive=True), 2),
     "hooks": (lambda: scenes.HooksAndMaps(48, 48), 3),
+    "mesh": (lambda: scenes.MeshLike(48, 48, res=64), 3),
 }
 SEED = 1
 
@@ -52,13 +53,14 @@ def make_pt(name):
     lib = oracle.OracleLib(h.sceneObj.shader(), h.scene_opts())
     pix = np.arange(h.width * h.height)
     rng0 = lib.seed(SEED, pix)
-    mean, rng = ref.render(p, h.scene_uniforms(), tables, h.width, h.height, pix, frames, rng0)
+    sh = h.scene_shader()
+    mean, rng = ref.render(p, sh.calls, tables, h.width, h.height, pix, frames, rng0, scene_textures=sh.textures)
     np.savez_compressed(os.path.join(HERE, f"pt_{name}.npz"), case=name, width=h.width, height=h.height,
                         frames=frames, seed=SEED, rng0=rng0, mean=mean, rng=rng)
     print(f"pt_{name}: {h.width}x{h.height}, {frames} frames, mean XYZ {mean[:, :3].mean(0)}")
 
 
-FH_CASES = ("c0", "c1", "c2", "atmosphere", "hooks")
+FH_CASES = ("c0", "c1", "c2", "atmosphere", "hooks", "mesh")
 FH_FRAMES = 3
 
 
@@ -71,13 +73,14 @@ def make_firsthit(name):
     pix = np.arange(h.width * h.height)
     rng0 = lib.seed(SEED, pix)
     out = dict(case=name, width=h.width, height=h.height, frames=FH_FRAMES, seed=SEED, rng0=rng0)
+    sh = h.scene_shader()
     for prog in ("normals", "ao"):
         ref, p, tables, keep = build_ref.ref_for(h, program=prog)
-        mean, rng = ref.render(p, h.scene_uniforms(), tables, h.width, h.height, pix, FH_FRAMES, rng0)
+        mean, rng = ref.render(p, sh.calls, tables, h.width, h.height, pix, FH_FRAMES, rng0, scene_textures=sh.textures)
         out[prog + "_mean"] = mean
         out[prog + "_rng"] = rng
     ref, p, tables, keep = build_ref.ref_for(h, program="pick")
-    out["pick"] = ref.pick(p, h.scene_uniforms(), tables, h.width, pix)
+    out["pick"] = ref.pick(p, sh.calls, tables, h.width, pix, scene_textures=sh.textures)
     np.savez_compressed(os.path.join(HERE, f"fh_{name}.npz"), **out)
     print(f"fh_{name}: {h.width}x{h.height}, normals/ao {FH_FRAMES} frames, pick hits {(out['pick'][:, 1] >= 0).mean():.3f}")
 

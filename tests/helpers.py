@@ -16,10 +16,11 @@ CASES = {
     "atmosphere": lambda: scenes.AtmosphereLights(64, 48),
     "atmosphere_disp": lambda: scenes.AtmosphereLights(32, 24, dispersive=True),
     "hooks": lambda: scenes.HooksAndMaps(48, 48),
+    "mesh": lambda: scenes.MeshLike(48, 48, res=64),
 }
 
 
-FH_CASES = ("c0", "c1", "c2", "atmosphere", "hooks")
+FH_CASES = ("c0", "c1", "c2", "atmosphere", "hooks", "mesh")
 
 
 def golden(name):
@@ -37,7 +38,8 @@ def oracle_firsthit(host, mode, pixels, frames, rng0=None, threads=0):
     if rng0 is None and mode != 3:
         rng0 = lib.seed(host.seed, pixels)
     p, keep = oracle.host_params(host)
-    ub = oracle.pack_uniforms(lib.cpp, host.scene_uniforms())
+    sh = host.scene_shader()
+    ub = oracle.pack_uniforms(lib.cpp, sh.calls, sh.textures)
     return lib.firsthit(mode, p, ub, host.width, host.height, pixels, frames, rng0, threads)
 
 
@@ -52,7 +54,8 @@ def oracle_render(host, pixels, frames, rng0=None, threads=0):
     if rng0 is None:
         rng0 = lib.seed(host.seed, pixels)
     p, keep = oracle.host_params(host)
-    ub = oracle.pack_uniforms(lib.cpp, host.scene_uniforms())
+    sh = host.scene_shader()
+    ub = oracle.pack_uniforms(lib.cpp, sh.calls, sh.textures)
     return lib.render(p, ub, host.width, host.height, pixels, frames, rng0, threads)
 
 
