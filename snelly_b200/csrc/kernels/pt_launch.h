@@ -38,9 +38,12 @@ typedef struct JobRec {
 // pixel of the frame; device pointers). Layout shared with the host (wavefront.cpp).
 #define WF_A 0      // active-path queue counts [2] (ping-pong by iteration parity)
 #define WF_S 2      // shadow-ray queue counts [2]
-#define WF_Q 4      // shade-queue segment counts [2][4]
-#define WF_HEAD 12  // extend work heads, one per iteration
-#define WF_COUNTERS 96
+#define WF_C 4      // parked-ray queue counts [2]
+#define WF_LEFT 6   // paths of the frame not finished yet
+#define WF_Q 8      // shade-queue segment counts [2][4]
+#define WF_HEAD 16  // extend work heads, one per iteration
+#define WF_MAX_ITERS 300
+#define WF_COUNTERS (WF_HEAD + WF_MAX_ITERS)
 typedef struct WfBuffers {
   float4* pos;      // path vertex pW (xyz)
   float4* dir;      // ray direction (xyz)
@@ -58,9 +61,12 @@ typedef struct WfBuffers {
   float4* nee_dir[2];  // sky, sun shadow directions (xyz) and lengths (w)
   float4* nee_c[2];    // unoccluded contributions
   float4* nee_li[2];   // unshadowed radiance (gate)
+  float4* mt;       // march state of a parked ray (distance, sign, step count), by ray id
   unsigned char* shadow;  // occlusion result per shadow ray (2 per path)
-  int* qa[2];       // active-path queues
+  int* pend;        // rays each path waits for
+  int* qa[2];       // active-path queues (continuation rays)
   int* qs[2];       // shadow-ray queues (path * 2 + light)
+  int* qc[2];       // parked-ray queues (ray ids: 2 * path + light, or 2 * paths + path)
   int* qshade;      // shade queue, 4 segments of `paths` entries: finish/miss, surface, metal, dielectric
   int* cnt;         // counters (WF_*)
   int paths;

@@ -2,17 +2,19 @@
 // over queues of rays and paths in HBM (one job per launch, one sample per pixel per frame).
 //
 //   generate: camera rays (wavelength, jitter, primary ray) for every pixel -> active queue.
-//   extend  : persistent warps trace the continuation rays of the active paths and the pending
-//             shadow rays of the previous vertex. A lane that finishes a ray takes the next one
-//             from a global work head (warp-aggregated atomics), so warps stay full however
-//             uneven the sphere-tracing step counts are. Hits are appended to per-material
-//             segments of the shade queue (misses and finishing paths first).
+//   extend  : persistent warps trace the continuation rays of the active paths, the pending
+//             shadow rays of the previous vertex and the rays parked by the previous iteration.
+//             A lane that finishes a ray takes the next one from a global work head
+//             (warp-aggregated atomics), so warps stay full however uneven the sphere-tracing
+//             step counts are; when the work runs out, the longest rays are parked for the next
+//             iteration instead of holding the launch. A path whose last ray finished is appended
+//             to the per-material segment of the shade queue (misses and finishing paths first).
 //   shade   : per path: resolve the previous vertex's deferred next-event estimate with the
 //             shadow results, then run the vertex (vertex_step) with the sky/sun shadow rays
 //             deferred; continuing paths and new shadow rays go to the next iteration's queues,
 //             finished paths add their XYZ to the pixel's Kahan sums.
-// The host launches generate once and (extend, shade) MAX_BOUNCES + 2 times per frame; the queue
-// counters ping-pong by iteration parity, so the sequence needs no host synchronisation.
+// The host launches generate once and (extend, shade) until every path of the frame has finished
+// (a count the shade stage decrements); the queue counters ping-pong by iteration parity.
 #pragma once
 #include "pt_integrator.cuh"
 #include "pt_launch.h"
@@ -96,8 +98,9 @@ extern "C" __global__ void __launch_bounds__(SNELLY_BLOCK) snelly_wf_generate(co
   const JobRec& J = jobs[0];
   int path = blockIdx.x * blockDim.x + threadIdx.x;
   if (path == 0) {
+    for (int k = 0; k < WF_COUNTERS; ++k) B.cnt[k] = 0;
     B.cnt[WF_A + 0] = B.paths;
-    for (int k = 1; k < WF_COUNTERS; ++k) B.cnt[k] = 0;
+    B.cnt[WF_LEFT] = B.paths;
   }
   if (path >= B.paths) return;
   long long i = (long long)B.pixel_begin + path;
@@ -127,47 +130,59 @@ extern "C" __global__ void __launch_bounds__(SNELLY_BLOCK) snelly_wf_generate(co
   B.xyzw[path] = st3(xyzw);
   B.info[path] = make_int4(0, 0, s.inDiele ? WF_INDIELE : 0, 0);
   B.rng[path] = make_uint4(g.s[0], g.s[1], g.s[2], g.s[3]);
+  B.pend[path] = 1;  // the camera ray
   B.qa[0][path] = path;
 }
 
-// Trace the active continuation rays and the pending shadow rays of iteration `it`.
+// Trace the rays of iteration `it`: the continuation rays of the active paths, the pending shadow
+// rays of their previous vertex, and rays an earlier iteration set aside unfinished.
 //
 // Every pass of the loop runs up to WF_CHUNK sphere-tracing steps, each evaluating the scene SDFs
 // once for every lane that holds a ray; a ray's first evaluation (at its origin, which fixes the
 // marching sign, PT:888-900) is such a step too, so refilled lanes march in step with the rest of
 // the warp. Idle lanes are refilled when at least WF_REFILL of them are idle, or when none of the
 // warp is busy, from a range of WF_GRAB items the warp claims from the global work head with one
-// atomic.
-extern "C" __global__ void __launch_bounds__(SNELLY_BLOCK) snelly_wf_extend(WfBuffers B, int it) {
+// atomic. Once the work of the iteration is exhausted, a warp marches at most `drain` more steps
+// (0: no limit) and then parks its unfinished rays (distance, sign, step count) for the next
+// iteration, so no launch waits for the few longest rays. The march of a ray is the same sequence
+// of operations however it is split, so results do not depend on where it was interrupted.
+//
+// A path is shaded once all its rays (continuation and shadows) are done: each finished ray
+// decrements the path's pending count, and the last one queues the path for shading in the
+// shade-queue segment of its continuation hit's material (misses and finishing paths: segment 0).
+extern "C" __global__ void __launch_bounds__(SNELLY_BLOCK) snelly_wf_extend(WfBuffers B, int it, int drain) {
   using namespace sdev;
   const SnellyParams& P = c_params[0];
   Scene sc(uniforms_of(0));
   sc.INIT();
   int* cnt = B.cnt;
   const int cur = it & 1, nxt = cur ^ 1;
-  if (blockIdx.x == 0 && threadIdx.x == 0) {
+  if (blockIdx.x == 0 && threadIdx.x == 0) {  // queues the next shade stage and iteration fill
     cnt[WF_A + nxt] = 0;
     cnt[WF_S + nxt] = 0;
+    for (int k = 0; k < 4; ++k) cnt[WF_Q + 4 * nxt + k] = 0;
   }
-  const int nA = cnt[WF_A + cur], nS = cnt[WF_S + cur];
-  const int total = nA + nS;
+  const int nA = cnt[WF_A + cur], nS = cnt[WF_S + cur], nC = cnt[WF_C + cur];
+  const int total = nA + nS + nC;
   const int* qa = B.qa[cur];
   const int* qs = B.qs[cur];
+  const int* qc = B.qc[cur];
   int* qcnt = cnt + WF_Q + 4 * cur;
   const float minMarch = P.minLengthScale;
   const float maxLen = P.maxLengthScale;
+  const int P2 = 2 * B.paths;
 
   bool has = false, first = false;
   int path = 0, sidx = -1;  // sidx >= 0: a shadow ray
   vec3 o(0.0f), d(0.0f);
   float t = 0.0f, sgn = 1.0f, maxd = 0.0f;
   int n = 0;
-  // The warp's claimed range [wbase, wlim) of work items (warp-uniform); one atomic claims
-  // WF_GRAB items, handed to idle lanes over several refills.
+  // The warp's claimed range [wbase, wlim) of work items (warp-uniform).
   int wbase = 0, wlim = 0;
   bool wdone = false;
+  int drained = 0;  // steps marched since the iteration's work ran out (warp-uniform)
   for (;;) {
-    bool done = false, res_hit = false, finishing = false;
+    bool done = false, res_hit = false;
     int res_mat = MAT_INVAL;
     // ---- refill idle lanes ----------------------------------------------------------------
     const bool want = !has;
@@ -185,29 +200,37 @@ extern "C" __global__ void __launch_bounds__(SNELLY_BLOCK) snelly_wf_extend(WfBu
       const int w = wbase + __popc(need & lanemask_lt());
       wbase = min(wbase + __popc(need), wlim);
       if (want && w < wlim) {
+        int r;  // ray id: 2 * path + light for a shadow ray, 2 * paths + path for a continuation
+        bool resume = false;
         if (w < nA) {
-          const int e = qa[w];
-          path = e < 0 ? ~e : e;
-          sidx = -1;
-          if (e < 0) {  // the path only waits for its shadow results
-            finishing = true;
-            done = true;
-          } else {
-            o = ld3(B.pos[path]);
-            d = ld3(B.dir[path]);
-            maxd = maxLen;
-            has = true;
-            first = true;
-          }
+          r = P2 + qa[w];
+        } else if (w < nA + nS) {
+          r = qs[w - nA];
         } else {
-          sidx = qs[w - nA];
+          r = qc[w - nA - nS];
+          resume = true;
+        }
+        if (r >= P2) {
+          path = r - P2;
+          sidx = -1;
+          o = ld3(B.pos[path]);
+          d = ld3(B.dir[path]);
+          maxd = maxLen;
+        } else {
+          sidx = r;
           path = sidx >> 1;
           o = ld3(B.nee_org[path]);
           float4 dd = B.nee_dir[sidx & 1][path];
           d = ld3(dd);
           maxd = dd.w;
-          has = true;
-          first = true;
+        }
+        has = true;
+        first = !resume;
+        if (resume) {
+          float4 m = B.mt[r];
+          t = m.x;
+          sgn = m.y;
+          n = __float_as_int(m.z);
         }
       }
     }
@@ -265,26 +288,42 @@ extern "C" __global__ void __launch_bounds__(SNELLY_BLOCK) snelly_wf_extend(WfBu
         }
       }
     }
+    if (wdone) drained += WF_CHUNK;
+    const bool park = drain > 0 && drained >= drain && has && !done;  // set aside for the next iteration
     // ---- results ---------------------------------------------------------------------------
-    if (__any_sync(WF_FULL, done)) {
-      const bool cont_result = done && sidx < 0;
+    if (__any_sync(WF_FULL, done || park)) {
       int seg = -1;
-      if (cont_result) {
-        if (!finishing) B.hit[path] = st3(o + t * d, enc_hit(res_hit, res_mat));
-        seg = (finishing || !res_hit) ? 0 : (res_mat == MAT_SURFA ? 1 : (res_mat == MAT_METAL ? 2 : (res_mat == MAT_DIELE ? 3 : 0)));
+      if (done) {
+        if (sidx < 0) B.hit[path] = st3(o + t * d, enc_hit(res_hit, res_mat));
+        else B.shadow[sidx] = res_hit ? 1 : 0;
+        __threadfence();
+        if (atomicSub(B.pend + path, 1) == 1) {  // the path's last ray: queue it for shading
+          bool h;
+          int hm;
+          if (sidx < 0) {
+            h = res_hit;
+            hm = res_mat;
+          } else {
+            dec_hit(__ldcg(&B.hit[path].w), h, hm);
+          }
+          seg = !h ? 0 : (hm == MAT_SURFA ? 1 : (hm == MAT_METAL ? 2 : (hm == MAT_DIELE ? 3 : 0)));
+        }
       }
-      if (done && sidx >= 0) B.shadow[sidx] = res_hit ? 1 : 0;
       for (int sgi = 0; sgi < 4; ++sgi) {
         int slot = warp_append(qcnt + sgi, seg == sgi);
         if (slot >= 0) B.qshade[sgi * B.paths + slot] = path;
       }
-      if (done) has = false;
+      const int r = sidx >= 0 ? sidx : P2 + path;
+      if (park) B.mt[r] = make_float4(t, sgn, __int_as_float(n), 0.0f);
+      int slot = warp_append(cnt + WF_C + nxt, park);
+      if (slot >= 0) B.qc[nxt][slot] = r;
+      if (done || park) has = false;
     }
     if (wdone && !__any_sync(WF_FULL, has)) break;
   }
 }
 
-// Shade every path the extend stage of iteration `it` queued.
+// Shade every path the extend stage of iteration `it` queued, and count the frame's paths down.
 extern "C" __global__ void __launch_bounds__(SNELLY_BLOCK, SNELLY_SHADE_MIN_BLOCKS) snelly_wf_shade(const JobRec* __restrict__ jobs,
                                                                         const SnellyParams* __restrict__ gparams,
                                                                         WfBuffers B, int it) {
@@ -296,8 +335,7 @@ extern "C" __global__ void __launch_bounds__(SNELLY_BLOCK, SNELLY_SHADE_MIN_BLOC
   const int* qc = cnt + WF_Q + 4 * cur;
   const int n0 = qc[0], n1 = qc[1], n2 = qc[2], n3 = qc[3];
   const int total = n0 + n1 + n2 + n3;
-  if (blockIdx.x == 0 && threadIdx.x == 0)
-    for (int k = 0; k < 4; ++k) cnt[WF_Q + 4 * nxt + k] = 0;
+  if (blockIdx.x == 0 && threadIdx.x == 0) cnt[WF_C + cur] = 0;  // filled again by the next extend stage
   Scene sc(uniforms_of(0));
   sc.INIT();
   const int stride = gridDim.x * blockDim.x;
@@ -305,7 +343,7 @@ extern "C" __global__ void __launch_bounds__(SNELLY_BLOCK, SNELLY_SHADE_MIN_BLOC
     int w = base + threadIdx.x;
     bool valid = w < total;
     int path = 0;
-    bool push_active = false, finishing_entry = false;
+    bool push_active = false, push_direct = false, finished = false;
     int push_shadow = 0;  // bit 0: sky, bit 1: sun
     if (valid) {
       int seg = w < n0 ? 0 : (w < n0 + n1 ? 1 : (w < n0 + n1 + n2 ? 2 : 3));
@@ -349,7 +387,7 @@ extern "C" __global__ void __launch_bounds__(SNELLY_BLOCK, SNELLY_SHADE_MIN_BLOC
         s.L += resolve_deferred(c, nd, occ);
         flags &= ~(WF_NEE | WF_NEE_SKY | WF_NEE_SUN);
       }
-      bool finished;
+      bool continues = false;
       if (flags & WF_FINISHING) {
         finished = true;
       } else {
@@ -363,6 +401,7 @@ extern "C" __global__ void __launch_bounds__(SNELLY_BLOCK, SNELLY_SHADE_MIN_BLOC
         int r = vertex_step(c, s, h, vertex, g, &nd);
         ++vertex;
         finished = r == VERTEX_DONE || vertex > max_bounces(P) || maxc(s.thr) < kThroughputEps;
+        continues = !finished;
         if (nd.any) {
           flags |= WF_NEE;
           B.nee_org[path] = st3(nd.org);
@@ -392,16 +431,24 @@ extern "C" __global__ void __launch_bounds__(SNELLY_BLOCK, SNELLY_SHADE_MIN_BLOC
         B.mis[path] = make_float4(s.misSky, s.misSun, s.misSph, 0.0f);
         B.info[path] = make_int4(info.x, s.atmScatters, flags, 0);
         B.rng[path] = make_uint4(g.s[0], g.s[1], g.s[2], g.s[3]);
-        push_active = true;
-        finishing_entry = flags & WF_FINISHING;
+        // rays the path waits for: its continuation (unless it only resolves its shadows) and
+        // its shadow rays; a path with none goes straight to the next shade stage
+        const int nrays = (continues ? 1 : 0) + __popc(push_shadow);
+        if (!continues) B.hit[path] = make_float4(0.0f, 0.0f, 0.0f, enc_hit(false, MAT_INVAL));
+        B.pend[path] = nrays;
+        push_active = continues;
+        push_direct = nrays == 0;
       }
     }
-    // active-queue entries of paths that only wait for their shadow results are stored as ~path
     int slot = warp_append(cnt + WF_A + nxt, push_active);
-    if (slot >= 0) B.qa[nxt][slot] = finishing_entry ? ~path : path;
+    if (slot >= 0) B.qa[nxt][slot] = path;
     for (int l = 0; l < 2; ++l) {
       int ss = warp_append(cnt + WF_S + nxt, (push_shadow >> l) & 1);
       if (ss >= 0) B.qs[nxt][ss] = 2 * path + l;
     }
+    int ds = warp_append(cnt + WF_Q + 4 * nxt, push_direct);
+    if (ds >= 0) B.qshade[ds] = path;
+    unsigned fin = __ballot_sync(WF_FULL, finished);
+    if (fin && (int)(threadIdx.x & 31) == __ffs(fin) - 1) atomicSub(cnt + WF_LEFT, __popc(fin));
   }
 }

@@ -510,6 +510,9 @@ Context::~Context() {
   }
   release(xyz);
   release(stats_scratch);
+  if (poll_host) cudaFreeHost(poll_host);
+  for (auto& e : poll_done)
+    if (e) cudaEventDestroy(e);
   for (auto& kv : module_cache) cudaLibraryUnload(kv.second->lib);
   cudaStreamDestroy(stream);
 }
@@ -566,6 +569,7 @@ int snelly_init(snelly_ctx** out, int device, size_t budget) {
   c->include_dir = env ? std::string(env) + "/../../include" : dir + "/../include";
   if (!file_exists(c->kernel_dir + "/pt_kernels.cu"))
     return fail(SNELLY_EINVAL, "kernel sources not found under " + c->kernel_dir);
+  if (const char* dr = getenv("SNELLY_WF_DRAIN")) c->wf_drain_steps = atoi(dr);  // 0: never park rays
   const char* cdir = getenv("SNELLY_CACHE_DIR");
   c->cache_dir = cdir ? std::string(cdir) : dir + "/_build/kcache";
   mkdir((dir + "/_build").c_str(), 0755);

@@ -111,6 +111,9 @@ struct Context {
   std::string csrc_dir, kernel_dir, include_dir, cache_dir;
   std::vector<BatchLane> lanes;  // batch streams (created on first use)
   std::map<std::string, int> tuned;  // autotuner decisions: (module, image-size class) -> integrator
+  int wf_drain_steps = 64;           // steps an extend warp marches once its work runs out (SNELLY_WF_DRAIN)
+  int* poll_host = nullptr;          // pinned words the wavefront's paths-left reads land in
+  cudaEvent_t poll_done[2] = {nullptr, nullptr};
   DevBuf stats_scratch;          // image-statistics partial sums
 
   ~Context();

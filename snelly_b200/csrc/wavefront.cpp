@@ -8,8 +8,9 @@ int Context::alloc_wavefront(Job& j) {
   if (j.scene->opts.max_samples_per_frame != 1) return SNELLY_OK;  // served by the per-pixel kernel
   const size_t P = (size_t)j.desc.width * j.desc.height;
   const size_t f4 = 16 * P;
-  // 17 float4 arrays + info + rng, shadow flags, 2+2+1(x4) int queues, counters
-  size_t bytes = 19 * f4 + 2 * P + (2 + 2 * 2 + 4) * 4 * P + 4 * WF_COUNTERS + 27 * 256;
+  // 17 float4 arrays + info + rng + parked-ray state (3 per path), shadow flags, pending counts,
+  // int queues (2 active, 2 x 2 shadow, 2 x 3 parked, 4 shade), counters
+  size_t bytes = 19 * f4 + 3 * f4 + 2 * P + 4 * P + (2 + 2 * 2 + 2 * 3 + 4) * 4 * P + 4 * WF_COUNTERS + 32 * 256;
   int rc = alloc(j.wf, bytes);
   if (rc) return rc;
   char* p = (char*)j.wf.ptr;
@@ -25,6 +26,10 @@ int Context::alloc_wavefront(Job& j) {
   for (float4** q : f4s) *q = (float4*)take(f4);
   B.info = (int4*)take(f4);
   B.rng = (uint4*)take(f4);
+  B.mt = (float4*)take(3 * f4);
+  B.pend = (int*)take(4 * P);
+  B.qc[0] = (int*)take(12 * P);
+  B.qc[1] = (int*)take(12 * P);
   B.qa[0] = (int*)take(4 * P);
   B.qa[1] = (int*)take(4 * P);
   B.qs[0] = (int*)take(8 * P);
@@ -54,13 +59,53 @@ int Context::enqueue_wavefront_frame(Job& j) {
   void* gargs[] = {&jobs, &gparams, &B};
   int rc = launch(m.f_wf_generate, gen_blocks, SNELLY_BLOCK, gargs);
   if (rc) return rc;
-  const int iters = j.scene->opts.max_bounces + 2;
+  // Iterations: the first `budgeted` ones park the slowest rays when their work runs out; after
+  // them every iteration advances every path by one vertex, so `nominal` more always finish the
+  // frame. Beyond the nominal count, iterations go in pairs, each followed by a read of the
+  // paths-left count; the host waits for the read of the pair before last, so the GPU always
+  // has the next pair queued, and stops once a read shows zero (an extra pair then finds empty
+  // queues and returns at once).
+  const int nominal = j.scene->opts.max_bounces + 2;
+  const int budgeted = 3 * nominal;
+  const int max_iters = budgeted + nominal;
+  if (max_iters + 2 > WF_MAX_ITERS) return fail(SNELLY_EINVAL, "too many wavefront iterations for max_bounces");
   const int extend_blocks = sm_count * m.extend_blocks_per_sm, shade_blocks = sm_count * 4;
-  for (int it = 0; it < iters; ++it) {
-    void* eargs[] = {&B, &it};
-    if ((rc = launch(m.f_wf_extend, extend_blocks, SNELLY_BLOCK, eargs))) return rc;
+  int it = 0;
+  auto pair = [&]() {
+    int drain = it < budgeted ? wf_drain_steps : 0;
+    void* eargs[] = {&B, &it, &drain};
+    int r = launch(m.f_wf_extend, extend_blocks, SNELLY_BLOCK, eargs);
+    if (r) return r;
     void* sargs[] = {&jobs, &gparams, &B, &it};
-    if ((rc = launch(m.f_wf_shade, shade_blocks, SNELLY_BLOCK, sargs))) return rc;
+    r = launch(m.f_wf_shade, shade_blocks, SNELLY_BLOCK, sargs);
+    ++it;
+    return r;
+  };
+  while (it < nominal)
+    if ((rc = pair())) return rc;
+  if (!poll_host) {
+    if (cudaMallocHost((void**)&poll_host, 2 * sizeof(int)) != cudaSuccess) {
+      poll_host = nullptr;
+      return fail(SNELLY_EDEVICE, "pinned host allocation failed");
+    }
+    for (auto& e : poll_done)
+      if (cudaEventCreateWithFlags(&e, cudaEventDisableTiming) != cudaSuccess)
+        return fail(SNELLY_EDEVICE, "event creation failed");
+  }
+  int checks = 0;
+  while (it < max_iters) {
+    if ((rc = pair())) return rc;
+    if ((rc = pair())) return rc;
+    const int slot = checks & 1;
+    if (cudaMemcpyAsync(poll_host + slot, B.cnt + WF_LEFT, sizeof(int), cudaMemcpyDeviceToHost, stream) != cudaSuccess ||
+        cudaEventRecord(poll_done[slot], stream) != cudaSuccess)
+      return fail(SNELLY_EDEVICE, "wavefront progress read failed");
+    ++checks;
+    if (checks >= 2) {
+      const int prev = (checks - 2) & 1;
+      if (cudaEventSynchronize(poll_done[prev]) != cudaSuccess) return fail(SNELLY_EDEVICE, "wavefront progress wait failed");
+      if (poll_host[prev] == 0) break;
+    }
   }
   return SNELLY_OK;
 }
