@@ -109,6 +109,8 @@ typedef struct snelly_spectrum {
 #define SNELLY_MODE_NORMALS 1 /* first-hit normals (normals-fragment-shader.glsl) */
 #define SNELLY_MODE_AO 2      /* first-hit ambient occlusion (ao-fragment-shader.glsl) */
 #define SNELLY_MODE_PICK 3    /* first-hit distance and material (pick-fragment-shader.glsl) */
+#define SNELLY_MODE_PTSIMPLE 4 /* RGB surface-only path tracer (renderMode 'ptsimple',
+                                  simplepathtracer-fragment-shader.glsl) */
 
 typedef struct snelly_render_desc {
   int width, height;
@@ -143,9 +145,12 @@ int snelly_set_texture(snelly_ctx* ctx, uint64_t scene_id, const char* name, con
                        int d, int channels, int fmt, int linear);
 
 /* Start a job: allocates its per-pixel state, seeds it and enqueues desc->frames frames. Returns
- * without waiting. */
+ * without waiting for the frames, except that a wavefront job's frame is enqueued in pairs of
+ * iterations until a progress read shows the frame complete, so the call returns roughly one
+ * pair of iterations before its last frame ends. A SNELLY_KERNEL_AUTO scene's first job of a
+ * module and image-size class also runs the autotuner's trial frames. */
 int snelly_render(snelly_ctx* ctx, uint64_t scene_id, const snelly_render_desc* desc, uint64_t* job_id);
-/* Enqueue more frames on an existing job (progressive accumulation). */
+/* Enqueue more frames on an existing job (progressive accumulation); same timing as snelly_render. */
 int snelly_advance(snelly_ctx* ctx, uint64_t job_id, int frames);
 
 /* Enqueue frames[i] more frames on each job_ids[i], batched: for every frame, the jobs that share
@@ -240,6 +245,12 @@ int snelly_tonemap(snelly_ctx* ctx, uint64_t job_id, const snelly_tonemap_params
  * conversion and its quotients against float() and __fdiv_rn for every state of each of the four
  * lanes. *mismatches = number of differing results. */
 int snelly_selftest(snelly_ctx* ctx, int which, uint64_t* mismatches);
+
+/* Reconstruct 8-bit PNG image bytes from decompressed scanlines (each a filter-type byte and
+ * width*channels filtered bytes; PNG specification section 9) into out (height*width*channels).
+ * Used by the host to load environment maps (Scene.envMap, js/renderer.js:143-157) and the
+ * SDF-PNG assets of scripts/pngPacker.html. No device work. */
+int snelly_png_unfilter(const uint8_t* raw, size_t raw_bytes, int width, int height, int channels, uint8_t* out);
 
 /* sizeof of the ABI structs, for bindings to check their layouts: 0 SnellyParams,
  * 1 snelly_render_desc, 2 snelly_scene_opts, 3 snelly_uniform, 4 snelly_spectrum. */

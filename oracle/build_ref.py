@@ -114,7 +114,7 @@ float K_METAL(float wavelength_nm)
 MODEL_NAMES = {0: "abbe", 1: "sellmeier", 2: "sellmeier2", 3: "polyanskiy", 4: "cauchy"}
 
 
-PROGRAMS = ("pathtracer", "normals", "ao", "pick", "tonemapper")
+PROGRAMS = ("pathtracer", "normals", "ao", "pick", "tonemapper", "simplepathtracer")
 
 
 def shader_source(scene_glsl, opts, diele_model, ncoeffs, program="pathtracer"):
@@ -255,10 +255,12 @@ class RefLib:
             dt = np.int32 if typ == "int" else np.float32
             b = np.asarray(vals, dt).tobytes()
             buf[off:off + len(b)] = b
-        for name, (ptr, w, h, ch, linear) in tables.items():
+        for name, rec in tables.items():
+            ptr, w, h, ch, linear = rec[:5]
+            fmt, srgb = rec[5:7] if len(rec) > 5 else (0, 0)
             if name in self.layout:
                 off = self.layout[name][1]
-                buf[off:off + 32] = struct.pack("<Q6i", ptr, w, h, ch, 0, linear, 0)
+                buf[off:off + 32] = struct.pack("<Q6i", ptr, w, h, ch, fmt, linear, srgb)
         for name, (arr, linear) in (scene_textures or {}).items():
             if name in self.layout:
                 off = self.layout[name][1]
@@ -317,7 +319,7 @@ def ref_for(snelly, name=None, prebuilt_only=False, program="pathtracer"):
     named build in oracle/_ref/<name>; prebuilt_only: never build (returns None if absent);
     program: which fragment shader (pathtracer, normals, ao, pick)."""
     p, keep = O.host_params(snelly)
-    xyz, icdf = keep
+    xyz, icdf, env = keep
     metal_n = np.asarray(list(p.metalN), np.float32)
     metal_k = np.asarray(list(p.metalK), np.float32)
     tables = {
@@ -326,13 +328,15 @@ def ref_for(snelly, name=None, prebuilt_only=False, program="pathtracer"):
         "iorTex": (metal_n.ctypes.data, 64, 1, 1, 1),
         "kTex": (metal_k.ctypes.data, 64, 1, 1, 1),
     }
+    if env is not None:  # SRGB8 RGB, LINEAR (GLU.loadImageAndCreateTextureInfo, js/gl.js:532-559)
+        tables["envMap"] = (env.ctypes.data, env.shape[1], env.shape[0], 3, 1, 2, 1)
     args = (snelly.sceneObj.shader(), snelly.scene_opts(), p.dieleModel, p.dieleNumCoeffs)
     lib = RefLib.load(name, *args, program=program) if name else None
     if lib is None:
         if prebuilt_only or not os.path.isdir(os.path.join(REF_ROOT, "shaders")):
             return None
         lib = RefLib(*args, name=name, program=program)
-    return lib, p, tables, (xyz, icdf, metal_n, metal_k)
+    return lib, p, tables, (xyz, icdf, metal_n, metal_k, env)
 
 
 if __name__ == "__main__":

@@ -217,8 +217,8 @@ class OracleLib:
             h.update("".join(flags).encode())
         except OSError:
             pass
-        for f in ("pt_oracle.h", "pt_oracle_bsdf.inc", "pt_oracle_integrator.inc", "fh_oracle.inc", "tm_oracle.h",
-                  "oracle_main.cpp", "counted.h"):
+        for f in ("pt_oracle.h", "pt_oracle_bsdf.inc", "pt_oracle_integrator.inc", "fh_oracle.inc", "ps_oracle.inc",
+                  "tm_oracle.h", "oracle_main.cpp", "counted.h"):
             p = os.path.join(HERE, f)
             if os.path.exists(p):
                 h.update(open(p, "rb").read())
@@ -247,9 +247,9 @@ class OracleLib:
         return xyz, mean, rng
 
     def firsthit(self, mode, params, uniforms, width, height, pixels, frames, rng=None, threads=0):
-        """First-hit programs: mode 1 normals, 2 ambient occlusion (returns xyz_sum, running mean,
-        final rng as render() does), 3 pick (returns (n, 2) distance and material at the pixel
-        centres)."""
+        """The other programs: mode 1 normals, 2 ambient occlusion, 4 the simplified path tracer
+        (returns xyz_sum, running mean, final rng as render() does), 3 pick (returns (n, 2)
+        distance and material at the pixel centres)."""
         pixels = np.ascontiguousarray(pixels, np.int32)
         n = len(pixels)
         rng = np.ascontiguousarray(rng if rng is not None else np.ones((n, 4)), np.uint32).copy()
@@ -286,9 +286,14 @@ def host_params(snelly):
         icdf = inverse_cdf("mono", wavelength=sp.wavelength)
     else:
         icdf = inverse_cdf("blackbody", temperature=sp.skyTemperature)
-    keep = (xyz, icdf)
+    env = snelly.env_map()
+    keep = (xyz, icdf, env)
     p.xyzTable = xyz.ctypes.data
     p.icdfTable = icdf.ctypes.data
+    if env is not None:  # as snelly_render binds desc.env_map
+        p.envMap = env.ctypes.data
+        p.envMapH, p.envMapW = int(env.shape[0]), int(env.shape[1])
+        p.haveEnvMap = 1
     return p, keep
 
 

@@ -112,14 +112,14 @@ int oracle_render(const SnellyParams* P, const void* uniforms, int width, int he
   return 0;
 }
 
-// One frame per call of the first-hit programs for the listed pixels: mode 1 normals
-// (NM:293-345), 2 ambient occlusion (AO:395-488), both updating rng, xyz_sum and the running mean
-// as oracle_render does; mode 3 pick (PK:133-152) at each pixel centre, writing
-// (distance, material, 0, 0) to mean (rng and xyz_sum untouched).
+// `frames` frames of the other programs for the listed pixels: mode 1 normals (NM:293-345),
+// 2 ambient occlusion (AO:395-488), 4 the simplified path tracer (SP:1083-1130), all updating rng,
+// xyz_sum and the running mean as oracle_render does; mode 3 pick (PK:133-152) at each pixel
+// centre, writing (distance, material, 0, 0) to mean (rng and xyz_sum untouched).
 int oracle_firsthit(const SnellyParams* P, const void* uniforms, int mode, int width, int height, const int* pixels,
                     int n, int frames, uint32_t* rng, double* xyz_sum, float* mean, int threads) {
   (void)height;
-  if (mode < 1 || mode > 3) return -1;
+  if (mode < 1 || mode > 4) return -1;
   const glsl::SceneUniforms& U = *reinterpret_cast<const glsl::SceneUniforms*>(uniforms);
 #ifdef _OPENMP
   if (threads > 0) omp_set_num_threads(threads);
@@ -149,6 +149,9 @@ int oracle_firsthit(const SnellyParams* P, const void* uniforms, int mode, int w
       if (mode == 1) {
         sc.INIT();
         c = inv.normals(pixel, rnd);
+      } else if (mode == 4) {
+        sc.INIT();
+        c = inv.ptsimple(pixel, rnd);
       } else {
         // AO:397-414: the interactive-mode skip comes before INIT()
         c = inv.ao_frame(pixel, rnd, skipped);

@@ -245,6 +245,7 @@ struct Invocation {
 #include "pt_oracle_bsdf.inc"
 #include "pt_oracle_integrator.inc"
 #include "fh_oracle.inc"
+#include "ps_oracle.inc"
 };
 
 }  // namespace oracle

@@ -19,7 +19,7 @@ ERRORS = {
 }
 KERNEL_AUTO, KERNEL_MEGA, KERNEL_WAVEFRONT = 0, 1, 2
 MATH_FAST, MATH_STRICT = 0, 1
-MODE_PT, MODE_NORMALS, MODE_AO, MODE_PICK = 0, 1, 2, 3
+MODE_PT, MODE_NORMALS, MODE_AO, MODE_PICK, MODE_PTSIMPLE = 0, 1, 2, 3, 4
 SPECTRUM_BLACKBODY, SPECTRUM_FLAT, SPECTRUM_MONO = 0, 1, 2
 READ_WAIT, READ_POLL = 1, 2
 U_FLOAT, U_INT, U_BOOL, U_VEC2, U_VEC3, U_VEC4 = 0, 1, 2, 3, 4, 5
@@ -131,6 +131,7 @@ def lib():
         "snelly_readback": (i32, [vp, u64, vp, sz, i32]),
         "snelly_readback_state": (i32, [vp, u64, vp, vp, vp, vp]),
         "snelly_selftest": (i32, [vp, i32, P(u64)]),
+        "snelly_png_unfilter": (i32, [vp, sz, i32, i32, i32, vp]),
         "snelly_job_kernel": (i32, [vp, u64, P(i32)]),
         "snelly_image_stats_static": (i32, [vp, u64, P(ctypes.c_double)]),
         "snelly_tonemap": (i32, [vp, u64, P(TonemapParams), vp, sz, i32]),

@@ -467,7 +467,35 @@ class Snelly:
         self.camera.aspect = self.width / self.height  # Snelly._resize
         self.addSpectrum(BlackbodySpectrum("blackbody", "Blackbody spectrum", r.skyTemperature))
         self.loadSpectrum("blackbody")
+        self._env = self._load_env_map()
+        # What a user does after the scene is set up (the reference's GUI or console: another
+        # spectrum, other settings); the reference has no such hook, initScene ends here.
+        if hasattr(sc, "after_init"):
+            sc.after_init(self)
         self.reset()
+
+    def _load_env_map(self):
+        """The scene's environment map (Scene.envMap, js/renderer.js:143-157): a PNG file path (the
+        reference loads a URL) or an (h, w, 3|4) uint8 sRGB array, row 0 the top row of the image;
+        None without one."""
+        sc = self.sceneObj
+        if not hasattr(sc, "envMap"):
+            return None
+        src = sc.envMap()
+        if src is None:
+            return None
+        if isinstance(src, (str, bytes, os.PathLike)):
+            from .image import read_png
+            src = read_png(src)
+        a = np.asarray(src, np.uint8)
+        if a.ndim == 2:
+            a = a[..., None]
+        if a.shape[2] == 1:
+            a = np.repeat(a, 3, axis=2)
+        return np.ascontiguousarray(a[..., :3])
+
+    def env_map(self):
+        return getattr(self, "_env", None)
 
     # accessors of the reference's facade
     def getRenderer(self):
@@ -603,12 +631,16 @@ class Snelly:
         d = N.RenderDesc()
         d.width, d.height = int(self.width), int(self.height)
         d.frames = int(frames)
-        d.mode = {"pt": N.MODE_PT, "normals": N.MODE_NORMALS, "ao": N.MODE_AO,
-                  "pick": N.MODE_PICK}.get(self.pathtracer.renderMode, N.MODE_PT)
+        d.mode = {"pt": N.MODE_PT, "normals": N.MODE_NORMALS, "ao": N.MODE_AO, "pick": N.MODE_PICK,
+                  "ptsimple": N.MODE_PTSIMPLE}.get(self.pathtracer.renderMode, N.MODE_PT)
         d.seed = int(self.seed)
         d.params = self.uniform_params()
         d.spectrum = self.spectrumObj.native()
         d.accum_fp64 = 1 if getattr(self, "fp64", False) else 0
+        env = self.env_map()
+        if env is not None:
+            d.env_map = env.ctypes.data
+            d.env_h, d.env_w = int(env.shape[0]), int(env.shape[1])
         return d
 
     # -- progressive rendering ---------------------------------------------------------------------

@@ -11,7 +11,7 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 CUDA = os.environ.get("CUDA_HOME", "/usr/local/cuda")
-SOURCES = ["runtime.cpp", "glsl_transform.cpp", "wavefront.cpp", "aot_kernels.cu", "tonemap.cu"]
+SOURCES = ["runtime.cpp", "glsl_transform.cpp", "wavefront.cpp", "aot_kernels.cu", "tonemap.cu", "png_unfilter.cpp"]
 OUT = os.path.join(HERE, "libsnelly.so")
 
 

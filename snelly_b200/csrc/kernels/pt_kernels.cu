@@ -112,6 +112,7 @@ extern "C" __global__ void __launch_bounds__(SNELLY_BLOCK, SNELLY_MEGA_MIN_BLOCK
 
 #include "pt_wavefront.cuh"
 #include "pt_firsthit.cuh"
+#include "pt_simple.cuh"
 
 // Mean XYZ and sample count per pixel into `out` (float4), for readback.
 extern "C" __global__ void __launch_bounds__(SNELLY_BLOCK) snelly_resolve(const JobRec* __restrict__ jobs, const int* __restrict__ block_start,

@@ -16,6 +16,7 @@
 #define JOB_MODE_NORMALS 1
 #define JOB_MODE_AO 2
 #define JOB_MODE_PICK 3
+#define JOB_MODE_PTSIMPLE 4
 
 // One job's slice of a batched launch. Pointers are device addresses of the job's SoA buffers.
 typedef struct JobRec {

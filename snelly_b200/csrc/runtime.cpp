@@ -290,7 +290,8 @@ int Context::compile_module(const std::string& src, int math_mode, std::shared_p
              {"snelly_wf_shade", &m->f_wf_shade, false},
              {"snelly_wf_shadow", &m->f_wf_shadow, false},
              {"snelly_wf_accumulate", &m->f_wf_accumulate, false},
-             {"snelly_firsthit", &m->f_firsthit, false}};
+             {"snelly_firsthit", &m->f_firsthit, false},
+             {"snelly_ptsimple", &m->f_ptsimple, false}};
   for (auto& f : fns) {
     cudaError_t r = cudaLibraryGetKernel(f.f, m->lib, f.name);
     if (r != cudaSuccess) {
@@ -378,6 +379,9 @@ int Context::enqueue_frames(Job& j, int frames) {
       } else {
         rc = launch(m.f_frame_mega, j.blocks, SNELLY_BLOCK, args);
       }
+    } else if (j.desc.mode == SNELLY_MODE_PTSIMPLE) {
+      if (!m.f_ptsimple) return fail(SNELLY_EINVAL, "the simplified path tracer is not available in this module");
+      rc = launch(m.f_ptsimple, j.blocks, SNELLY_BLOCK, args);
     } else {
       if (!m.f_firsthit) return fail(SNELLY_EINVAL, "first-hit render modes are not available in this module");
       rc = launch(m.f_firsthit, j.blocks, SNELLY_BLOCK, args);
@@ -736,7 +740,7 @@ static int start_job(Context& c, uint64_t scene_id, const snelly_render_desc* de
   if (desc->width < 1 || desc->height < 1 || (long long)desc->width * desc->height > (1ll << 30))
     return fail(SNELLY_EINVAL, "bad image size");
   if (desc->frames < 0) return fail(SNELLY_EINVAL, "frames must be >= 0");
-  if (desc->mode < SNELLY_MODE_PT || desc->mode > SNELLY_MODE_PICK) return fail(SNELLY_EINVAL, "bad render mode");
+  if (desc->mode < SNELLY_MODE_PT || desc->mode > SNELLY_MODE_PTSIMPLE) return fail(SNELLY_EINVAL, "bad render mode");
   const SnellyParams& p = desc->params;
   if (p.dieleModel < SNELLY_IOR_ABBE || p.dieleModel > SNELLY_IOR_CAUCHY || p.dieleNumCoeffs < 0 ||
       p.dieleNumCoeffs > SNELLY_MAX_IOR_COEFFS)
@@ -746,7 +750,7 @@ static int start_job(Context& c, uint64_t scene_id, const snelly_render_desc* de
   Job j;
   j.scene = &s;
   j.module = s.module.get();
-  if (desc->mode != SNELLY_MODE_PT) {
+  if (desc->mode != SNELLY_MODE_PT && desc->mode != SNELLY_MODE_PTSIMPLE) {  // first-hit passes
     if (s.opts.math_mode == SNELLY_MATH_STRICT) {
       s.strict_module = s.module;
     } else if (!s.strict_module) {

@@ -13,7 +13,8 @@
 #include "snelly.h"
 
 static_assert(JOB_MODE_PT == SNELLY_MODE_PT && JOB_MODE_NORMALS == SNELLY_MODE_NORMALS &&
-                  JOB_MODE_AO == SNELLY_MODE_AO && JOB_MODE_PICK == SNELLY_MODE_PICK,
+                  JOB_MODE_AO == SNELLY_MODE_AO && JOB_MODE_PICK == SNELLY_MODE_PICK &&
+                  JOB_MODE_PTSIMPLE == SNELLY_MODE_PTSIMPLE,
               "kernel render-mode values follow the ABI's");
 static_assert(sizeof(JobRec) <= 128, "a single-job table holds one JobRec before the block starts at byte 128");
 
@@ -45,7 +46,7 @@ struct Module {
   cudaKernel_t f_seed = nullptr, f_frame_mega = nullptr, f_resolve = nullptr;
   cudaKernel_t f_wf_generate = nullptr, f_wf_extend = nullptr, f_wf_shade = nullptr, f_wf_shadow = nullptr,
                f_wf_accumulate = nullptr;
-  cudaKernel_t f_firsthit = nullptr;
+  cudaKernel_t f_firsthit = nullptr, f_ptsimple = nullptr;
   int extend_blocks_per_sm = 8;  // resident blocks of the persistent extend stage (occupancy query)
   char* c_params = nullptr;  // device addresses of the constant banks
   char* c_uniforms = nullptr;

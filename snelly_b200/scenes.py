@@ -45,6 +45,10 @@ class PlainSphere:
         s.diffuseAlbedo = [0.8, 0.8, 0.8]
         s.specAlbedo = [0.0, 0.0, 0.0]
         s.roughness = 0.3
+
+    def after_init(self, snelly):
+        # Snelly.initScene loads the blackbody spectrum after init() (js/snelly.js:285-286), so the
+        # flat spectrum is selected afterwards, as a user does from the GUI or console
         snelly.addSpectrum(FlatSpectrum("flat", "Flat spectrum", 390.0, 750.0))
         snelly.loadSpectrum("flat")
 
@@ -327,7 +331,6 @@ class HooksAndMaps:
             self.height = height
 
     def init(self, snelly):
-        from .api import MonochromaticSpectrum
         r = snelly.getRenderer()
         r.width, r.height = self.width, self.height
         r.dispersive = True
@@ -351,7 +354,10 @@ class HooksAndMaps:
         s.subsurface = 0.5
         s.subsurfaceMFP = 0.1
         s.subsurfaceAlbedoRGB = [0.8, 0.8, 0.7]
-        snelly.addSpectrum(MonochromaticSpectrum("mono", "550 nm", 550.0))
+
+    def after_init(self, snelly):
+        from .api import MonochromaticSpectrum
+        snelly.addSpectrum(MonochromaticSpectrum("mono", "550 nm", 550.0))  # selected after initScene
         snelly.loadSpectrum("mono")
 
     def shader(self):
@@ -391,6 +397,67 @@ void CONSTRUCT_PRIMARY_RAY(in vec2 pixel, inout vec4 rnd, inout vec3 primaryStar
     def syncShader(self, snelly, shader):
         shader.uniformF("ripple", 1.5)
         shader.uniform3Fv("tint", [0.1, 0.6, 0.2])
+
+
+def sky_env_map(width=64, height=32):
+    """A procedural lat-long environment map (sRGB8, row 0 = the top row, as an image loads): a
+    blue-to-white sky gradient over a brown ground with a bright sun patch, for the env-map
+    coverage scene."""
+    v = (np.arange(height) + 0.5) / height  # 0 at the top (theta = 0)
+    u = (np.arange(width) + 0.5) / width
+    uu, vv = np.meshgrid(u, v)
+    sky = np.stack([0.35 + 0.6 * vv, 0.55 + 0.4 * vv, 0.95 + 0.0 * vv], -1)
+    ground = np.stack([0.35 + 0.0 * vv, 0.25 + 0.0 * vv, 0.15 + 0.0 * vv], -1)
+    img = np.where((vv < 0.5)[..., None], sky, ground)
+    sun = np.exp(-(((uu - 0.3) / 0.04) ** 2 + ((vv - 0.25) / 0.06) ** 2))[..., None]
+    img = np.clip(img + 3.0 * sun, 0.0, 1.0)
+    return np.ascontiguousarray((img * 255.0 + 0.5).astype(np.uint8))
+
+
+class EnvMapLit:
+    """Coverage scene lit by a lat-long environment map (Scene.envMap): a diffuse sphere and a
+    polished aluminium sphere on a ground plane, the map rotated by envMapPhiRotation /
+    envMapThetaRotation and visible to camera rays; no sun."""
+
+    width, height, spp = 48, 48, 4
+
+    def __init__(self, width=None, height=None):
+        if width:
+            self.width = width
+        if height:
+            self.height = height
+
+    def init(self, snelly):
+        r = snelly.getRenderer()
+        r.width, r.height = self.width, self.height
+        r.dispersive = True
+        r.interactive = False
+        r.maxBounces = 4
+        r.maxMarchSteps = 200
+        r.skyPower = math.log10(1.5)
+        r.sunPower = -7.0
+        r.envMapVisible = True
+        r.envMapPhiRotation = 40.0
+        r.envMapThetaRotation = 15.0
+        cam = snelly.getCamera()
+        cam.fov = 50.0
+        cam.position.set(0.0, 0.8, 4.0)
+        cam.aperture = -math.inf
+        snelly.getControls().target.set(0.0, 0.0, 0.0)
+        s = snelly.getMaterials().loadSurface()
+        s.diffuseAlbedo = [0.7, 0.6, 0.5]
+        s.specAlbedo = [0.1, 0.1, 0.1]
+        s.roughness = 0.3
+        snelly.getMaterials().loadMetal("Aluminium").roughness = 0.05
+
+    def shader(self):
+        return """
+float SDF_SURFACE(vec3 X) { return min(length(X - vec3(-0.9, 0.0, 0.0)) - 0.8, X.y + 0.8); }
+float SDF_METAL(vec3 X) { return length(X - vec3(0.9, -0.2, 0.0)) - 0.6; }
+"""
+
+    def envMap(self):
+        return sky_env_map()
 
 
 _GRIDS = {}
@@ -489,5 +556,21 @@ float SDF_SURFACE(vec3 X)
         shader.uniform3Fv("gridSize", [3.0, 3.0, 3.0])
 
 
+class SdfAsset(MeshLike):
+    """A mesh distance grid loaded from an SDF-PNG asset (scripts/pngPacker.html format, see
+    sdfpng.py) over a ground plane, bound like the reference's mesh scenes bind theirs: the grid
+    spans ORIG .. ORIG + EDGE of the asset's metadata."""
+
+    def __init__(self, path, width=None, height=None):
+        super().__init__(width, height)
+        from .sdfpng import load_texture
+        self.meta, self.grid = load_texture(path)
+
+    def syncShader(self, snelly, shader):
+        shader.uniformTexture("sdfTex", self.grid)
+        shader.uniform3Fv("gridMin", [float(v) for v in self.meta["ORIG"]])
+        shader.uniform3Fv("gridSize", [float(v) for v in self.meta["EDGE"]])
+
+
 SCENES = {"c0": PlainSphere, "c1": DispersiveFractal, "c2": VolumetricSubsurface, "atmosphere": AtmosphereLights,
-          "hooks": HooksAndMaps, "mesh": MeshLike}
+          "hooks": HooksAndMaps, "mesh": MeshLike, "envmap": EnvMapLit}

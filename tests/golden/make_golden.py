@@ -11,6 +11,8 @@ Run in a checkout that has the reference at /root/reference (or $SNELLY_REFERENC
   ao-fragment-shader.glsl, pick-fragment-shader.glsl, built the same way) on the same scenes:
   normals and AO running means and RNG lanes after a few frames, pick distance and material at
   every pixel centre. `python tests/golden/make_golden.py fh` regenerates only these.
+* ps_<case>.npz: the reference's simplified path tracer (renderMode 'ptsimple',
+  simplepathtracer-fragment-shader.glsl) on the same scenes: running means and RNG lanes.
 * tm_golden.npz: the reference's tonemapper program on path-traced and synthetic XYZ texels for
   three display settings.
 * cie_csv.npy: the CIE XYZ table recomputed from scripts/color/lin2012xyz2e_fine_7sf.csv as
@@ -42,6 +44,7 @@ CASES = {
     "atmosphere_disp": (lambda: scenes.AtmosphereLights(32, 24, dispersive=True), 2),
     "hooks": (lambda: scenes.HooksAndMaps(48, 48), 3),
     "mesh": (lambda: scenes.MeshLike(48, 48, res=64), 3),
+    "envmap": (lambda: scenes.EnvMapLit(48, 48), 3),
 }
 SEED = 1
 
@@ -60,7 +63,7 @@ def make_pt(name):
     print(f"pt_{name}: {h.width}x{h.height}, {frames} frames, mean XYZ {mean[:, :3].mean(0)}")
 
 
-FH_CASES = ("c0", "c1", "c2", "atmosphere", "hooks", "mesh")
+FH_CASES = ("c0", "c1", "c2", "atmosphere", "hooks", "mesh", "envmap")
 FH_FRAMES = 3
 
 
@@ -83,6 +86,25 @@ def make_firsthit(name):
     out["pick"] = ref.pick(p, sh.calls, tables, h.width, pix, scene_textures=sh.textures)
     np.savez_compressed(os.path.join(HERE, f"fh_{name}.npz"), **out)
     print(f"fh_{name}: {h.width}x{h.height}, normals/ao {FH_FRAMES} frames, pick hits {(out['pick'][:, 1] >= 0).mean():.3f}")
+
+
+PS_FRAMES = 3
+
+
+def make_ptsimple(name):
+    """ps_<case>.npz: the reference's simplified path tracer (simplepathtracer-fragment-shader.glsl,
+    renderMode 'ptsimple'), PS_FRAMES frames: running mean and final RNG lanes."""
+    factory, _ = CASES[name]
+    h = HostSnelly(factory())
+    lib = oracle.OracleLib(h.sceneObj.shader(), h.scene_opts())
+    pix = np.arange(h.width * h.height)
+    rng0 = lib.seed(SEED, pix)
+    ref, p, tables, keep = build_ref.ref_for(h, program="simplepathtracer")
+    sh = h.scene_shader()
+    mean, rng = ref.render(p, sh.calls, tables, h.width, h.height, pix, PS_FRAMES, rng0, scene_textures=sh.textures)
+    np.savez_compressed(os.path.join(HERE, f"ps_{name}.npz"), case=name, width=h.width, height=h.height,
+                        frames=PS_FRAMES, seed=SEED, rng0=rng0, mean=mean, rng=rng)
+    print(f"ps_{name}: {h.width}x{h.height}, {PS_FRAMES} frames, mean XYZ {mean[:, :3].mean(0)}")
 
 
 TM_PARAMS = [  # exposure, invGamma (= 1/gamma as the host uploads it), contrast, saturation, hueShift
@@ -129,5 +151,8 @@ if __name__ == "__main__":
     for n in FH_CASES:
         if not only or "fh" in only:
             make_firsthit(n)
+    for n in FH_CASES:
+        if not only or "ps" in only:
+            make_ptsimple(n)
     if not only or "tm" in only:
         make_tonemap()

@@ -17,14 +17,19 @@ CASES = {
     "atmosphere_disp": lambda: scenes.AtmosphereLights(32, 24, dispersive=True),
     "hooks": lambda: scenes.HooksAndMaps(48, 48),
     "mesh": lambda: scenes.MeshLike(48, 48, res=64),
+    "envmap": lambda: scenes.EnvMapLit(48, 48),
 }
 
 
-FH_CASES = ("c0", "c1", "c2", "atmosphere", "hooks", "mesh")
+FH_CASES = ("c0", "c1", "c2", "atmosphere", "hooks", "mesh", "envmap")
 
 
 def golden(name):
     return dict(np.load(os.path.join(GOLDEN, f"pt_{name}.npz")))
+
+
+def golden_ps(name):
+    return dict(np.load(os.path.join(GOLDEN, f"ps_{name}.npz")))
 
 
 def golden_fh(name):

@@ -1,0 +1,71 @@
+"""The simplified path tracer (renderMode 'ptsimple') on the GPU against the reference's own
+program (golden fixtures), same seeds. Tolerances are written in each test."""
+import numpy as np
+import pytest
+
+from helpers import CASES, FH_CASES, golden_ps
+from snelly_b200 import _native as N
+from snelly_b200 import api
+
+pytestmark = pytest.mark.gpu
+
+
+def _close(a, b, rtol):
+    return np.abs(a - b).max(-1) <= rtol * np.maximum(1.0, np.abs(b).max(-1))
+
+
+def _render(ctx, name, math, frames, seed):
+    s = api.Snelly(CASES[name](), context=ctx)
+    s.seed = seed
+    s.pathtracer.renderMode = "ptsimple"
+    s.pathtracer.mathMode = math
+    s.render(frames)
+    img = s.readback().reshape(-1, 4).copy()
+    rng = s.readback_state()[0]
+    ctx.destroy_job(s.job_id())
+    return img, rng
+
+
+@pytest.mark.parametrize("name", FH_CASES)
+def test_ptsimple_strict_matches_reference_per_pixel(gpu_ctx, name):
+    """IEEE-mode build vs the reference program: >= 93% of pixels within 1e-4 relative (the rest:
+    paths whose branch flipped on a last-bit difference of a transcendental, CUDA's vs glibc's),
+    image mean XYZ within 1%."""
+    g = golden_ps(name)
+    img, _ = _render(gpu_ctx, name, N.MATH_STRICT, int(g["frames"]), int(g["seed"]))
+    ref = g["mean"]
+    assert (img[:, 3] == ref[:, 3]).all()
+    ok = _close(img[:, :3], ref[:, :3], 1e-4)
+    assert ok.mean() >= 0.93, f"{name}: only {ok.mean():.4f} of pixels within 1e-4"
+    rel = np.abs(img[:, :3].mean(0) - ref[:, :3].mean(0)) / np.abs(ref[:, :3].mean(0))
+    assert rel.max() <= 1e-2, rel
+
+
+@pytest.mark.parametrize("name", [n for n in FH_CASES if n != "c2"])
+def test_ptsimple_fast_matches_reference(gpu_ctx, name):
+    """Production (fast-math) build: >= 80% of pixels within 1e-3 relative, image mean within 3%
+    (C2's Mandelbox diverges per pixel under approximate division, as in the spectral tracer)."""
+    g = golden_ps(name)
+    img, _ = _render(gpu_ctx, name, N.MATH_FAST, int(g["frames"]), int(g["seed"]))
+    ref = g["mean"]
+    assert np.isfinite(img).all()
+    ok = _close(img[:, :3], ref[:, :3], 1e-3)
+    assert ok.mean() >= 0.80, f"{name}: only {ok.mean():.4f} of pixels within 1e-3"
+    rel = np.abs(img[:, :3].mean(0) - ref[:, :3].mean(0)) / np.abs(ref[:, :3].mean(0))
+    assert rel.max() <= 3e-2, rel
+
+
+def test_ptsimple_is_progressive(gpu_ctx):
+    """Frames accumulate: 2 + 2 frames equal 4 frames in one call, bit for bit."""
+    s = api.Snelly(CASES["c0"](), context=gpu_ctx)
+    s.pathtracer.renderMode = "ptsimple"
+    s.render(2)
+    s.render(2)
+    a = s.readback().copy()
+    gpu_ctx.destroy_job(s.job_id())
+    t = api.Snelly(CASES["c0"](), context=gpu_ctx)
+    t.pathtracer.renderMode = "ptsimple"
+    t.render(4)
+    b = t.readback().copy()
+    gpu_ctx.destroy_job(t.job_id())
+    np.testing.assert_array_equal(a, b)

@@ -59,3 +59,90 @@ def test_scene_uniform_recording():
     h = HostSnelly(scenes.HooksAndMaps())
     calls = h.scene_uniforms()
     assert calls["ripple"][1] == [1.5] and calls["tint"][1] == [0.1, 0.6, 0.2]
+
+
+def test_png_decode_all_scanline_filters():
+    """decode_png undoes the five PNG filter types (hand-filtered rows) and reads back what
+    png_bytes wrote."""
+    import struct
+    import zlib
+
+    from snelly_b200 import image
+    rs = np.random.RandomState(2)
+    h, w, c = 6, 5, 4
+    img = rs.randint(0, 256, (h, w, c)).astype(np.uint8)
+
+    def paeth(a, b, cc):
+        p = a + b - cc
+        pa, pb, pc = abs(p - a), abs(p - b), abs(p - cc)
+        return a if pa <= pb and pa <= pc else (b if pb <= pc else cc)
+
+    flat = img.reshape(h, w * c).astype(int)
+    rows = []
+    for y in range(h):
+        f = y % 5
+        prev = flat[y - 1] if y else np.zeros(w * c, int)
+        line = []
+        for i in range(w * c):
+            a_ = flat[y, i - c] if i >= c else 0
+            b_ = prev[i]
+            c_ = prev[i - c] if i >= c else 0
+            pred = [0, a_, b_, (a_ + b_) >> 1, paeth(a_, b_, c_)][f]
+            line.append((flat[y, i] - pred) & 255)
+        rows.append(bytes([f]) + bytes(line))
+
+    def chunk(tag, data):
+        return struct.pack(">I", len(data)) + tag + data + struct.pack(">I", zlib.crc32(tag + data) & 0xFFFFFFFF)
+
+    png = (b"\x89PNG\r\n\x1a\n" + chunk(b"IHDR", struct.pack(">IIBBBBB", w, h, 8, 6, 0, 0, 0)) +
+           chunk(b"IDAT", zlib.compress(b"".join(rows))) + chunk(b"IEND", b""))
+    np.testing.assert_array_equal(image.decode_png(png), img)
+    rgb = rs.randint(0, 256, (7, 9, 3)).astype(np.uint8)
+    np.testing.assert_array_equal(image.decode_png(image.png_bytes(rgb)), rgb)
+
+
+def test_sdf_png_round_trip(tmp_path):
+    """The packer's SDF-PNG layout (magic, version, sizes, JSON metadata, float32 samples in the
+    RGB bytes of a square image) round-trips, and load_texture gives the sampler3D shape."""
+    from snelly_b200 import scenes, sdfpng
+    g = scenes.sphere_blend_grid(16)[..., 0].astype(np.float32)
+    md = {"GRES": [16, 16, 16], "ORIG": [-1.5, -1.5, -1.5], "EDGE": [3.0, 3.0, 3.0]}
+    png = sdfpng.pack(g, md)
+    raw = __import__("snelly_b200.image", fromlist=["x"]).decode_png(png)[..., :3].reshape(-1)
+    assert raw[0] == 0xBE and raw[1] == 0xEF and raw[2] == 1 and raw[3] == 0
+    path = tmp_path / "grid.png"
+    path.write_bytes(png)
+    meta, tex = sdfpng.load_texture(str(path))
+    assert meta == md and tex.shape == (16, 16, 16, 1)
+    np.testing.assert_array_equal(tex[..., 0], g)
+
+
+def test_env_map_from_png_file_equals_array(tmp_path):
+    """Scene.envMap may return a PNG path (the reference returns a URL) or an array: both bind
+    the same sRGB8 texels, row 0 the top row of the image."""
+    from snelly_b200 import image, scenes
+    from snelly_b200.testing import HostSnelly
+    arr = scenes.sky_env_map()
+    path = tmp_path / "env.png"
+    image.write_png(str(path), arr)
+
+    class FromFile(scenes.EnvMapLit):
+        def envMap(self):
+            return str(path)
+
+    a = HostSnelly(scenes.EnvMapLit(16, 16)).env_map()
+    b = HostSnelly(FromFile(16, 16)).env_map()
+    np.testing.assert_array_equal(a, b)
+    assert a.shape == (32, 64, 3)
+
+
+def test_sdf_asset_scene_binds_the_packed_grid(tmp_path):
+    from snelly_b200 import scenes, sdfpng
+    from snelly_b200.testing import HostSnelly
+    g = scenes.sphere_blend_grid(16)[..., 0].astype(np.float32)
+    path = tmp_path / "asset.png"
+    path.write_bytes(sdfpng.pack(g, {"GRES": [16, 16, 16], "ORIG": [-1.0, -1.0, -1.0], "EDGE": [2.0, 2.0, 2.0]}))
+    sh = HostSnelly(scenes.SdfAsset(str(path), 16, 16)).scene_shader()
+    tex, linear = sh.textures["sdfTex"]
+    assert tex.shape == (16, 16, 16, 1) and tex.dtype == np.float32 and linear
+    assert sh.calls["gridMin"][1] == [-1.0, -1.0, -1.0] and sh.calls["gridSize"][1] == [2.0, 2.0, 2.0]

@@ -3,7 +3,8 @@ and its building blocks: RNG, seeding, inverse CDF, tables."""
 import numpy as np
 import pytest
 
-from helpers import CASES, FH_CASES, GOLDEN, golden, golden_fh, host, oracle_firsthit, oracle_for, oracle_render
+from helpers import (CASES, FH_CASES, GOLDEN, golden, golden_fh, golden_ps, host, oracle_firsthit, oracle_for,
+                     oracle_render)
 
 
 @pytest.mark.parametrize("name", sorted(CASES))
@@ -41,6 +42,18 @@ def test_tonemap_oracle_matches_reference_golden():
     for k, p in enumerate(g["params"]):
         out = lib.tonemap(g["xyzn"], p)
         np.testing.assert_array_equal(out, g["rgba"][k])
+
+
+@pytest.mark.parametrize("name", FH_CASES)
+def test_ptsimple_oracle_matches_reference_golden(name):
+    """The restatement of the simplified path tracer reproduces the reference's own program bit for
+    bit (running means and RNG lanes)."""
+    g = golden_ps(name)
+    h = host(name)
+    pix = np.arange(h.width * h.height)
+    xyz, mean, rng = oracle_firsthit(h, 4, pix, int(g["frames"]), rng0=g["rng0"])
+    np.testing.assert_array_equal(rng, g["rng"])
+    np.testing.assert_array_equal(mean, g["mean"])
 
 
 def test_seeding_is_deterministic_and_in_range():
