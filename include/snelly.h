@@ -153,6 +153,19 @@ int snelly_render(snelly_ctx* ctx, uint64_t scene_id, const snelly_render_desc* 
 /* Enqueue more frames on an existing job (progressive accumulation); same timing as snelly_render. */
 int snelly_advance(snelly_ctx* ctx, uint64_t job_id, int frames);
 
+/* Replace an existing job's camera, renderer and material parameters, its emission spectrum and
+ * its snapshot of the scene's uniforms (taken now from the scene, after snelly_set_uniforms /
+ * snelly_set_texture) for the frames enqueued after this call; the accumulated samples and the
+ * RNG state are kept. Replaces the per-frame uniform upload of Renderer.render
+ * (js/renderer.js:520-611: camera, renderer, Materials.syncShader and Scene.syncShader run every
+ * frame, so a preframeCallback's changes reach the next frame without a reset,
+ * js/sceneAPI.js:287-358). desc->width, height and mode must equal the job's (SNELLY_EINVAL
+ * otherwise: the reference resizes through a reset); desc->frames, seed, accum_fp64 and the
+ * environment-map fields are ignored (the job keeps its own). The module's compile-time bounds
+ * (maxBounces above the compiled value, maxMarchSteps, ...) do not change, as in the reference
+ * without a recompile. Returns after the new parameters are on the device. */
+int snelly_update_job(snelly_ctx* ctx, uint64_t job_id, const snelly_render_desc* desc);
+
 /* Enqueue frames[i] more frames on each job_ids[i], batched: for every frame, the jobs that share
  * a scene module run in one launch (up to 32 jobs per launch, each with its own parameter slot),
  * and the launches of different modules go to separate streams so that they overlap on the GPU.

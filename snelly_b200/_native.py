@@ -127,6 +127,7 @@ def lib():
         "snelly_set_texture": (i32, [vp, u64, ctypes.c_char_p, vp, i32, i32, i32, i32, i32, i32]),
         "snelly_render": (i32, [vp, u64, P(RenderDesc), P(u64)]),
         "snelly_advance": (i32, [vp, u64, i32]),
+        "snelly_update_job": (i32, [vp, u64, P(RenderDesc)]),
         "snelly_advance_batch": (i32, [vp, P(u64), P(i32), sz]),
         "snelly_readback": (i32, [vp, u64, vp, sz, i32]),
         "snelly_readback_state": (i32, [vp, u64, vp, vp, vp, vp]),

@@ -13,6 +13,7 @@ import ctypes
 import json
 import math
 import os
+import textwrap
 
 import numpy as np
 
@@ -119,6 +120,9 @@ class Surface:
         self.subsurfaceAnisotropy = 0.0
         self.subsurfaceDiffuseWeight = 1.0
 
+    def repr(self, lang="js"):
+        return material_repr("surface", self, lang)
+
     def syncShader(self, p, snelly):
         p.surfaceDiffuseAlbedoRGB[:] = self.diffuseAlbedo
         p.surfaceSpecAlbedoRGB[:] = self.specAlbedo
@@ -149,6 +153,9 @@ class Volume:
         self.fogMaxOpticalDepth = 5.0
         self.fogEmission = [1.0, 1.0, 1.0]
         self.fogTint = [0.5, 0.5, 0.5]
+
+    def repr(self, lang="js"):
+        return material_repr("volume", self, lang)
 
     def syncShader(self, p, snelly):
         sca = list(self.scatteringColor)
@@ -181,6 +188,9 @@ class Metal:
     def getName(self):
         return self._name
 
+    def repr(self, lang="js"):
+        return material_repr("metal", self, lang)
+
     def syncShader(self, p, snelly):
         p.metalRoughness = self.roughness
         p.metalSpecAlbedoRGB[:] = self.specAlbedo
@@ -204,6 +214,9 @@ class Dielectric:
 
     def getName(self):
         return self._name
+
+    def repr(self, lang="js"):
+        return material_repr("dielectric", self, lang)
 
     def syncShader(self, p, snelly):
         if self.absorptionScale < 0.0:
@@ -395,6 +408,7 @@ class Renderer:
         self.hueShift = 0.0
         self.skipProbability = 0.0
         self.spp = 0.0
+        self.numSamples = 0.0
         # B200 build options (no reference counterpart)
         self.mathMode = N.MATH_FAST
         self.kernelMode = N.KERNEL_AUTO  # autotuned per scene module and image size
@@ -408,10 +422,18 @@ class Renderer:
     def getSPP(self):
         return self.spp
 
+    def reset(self, no_recompile=False):
+        """Restart accumulating samples (Renderer.prototype.reset, js/renderer.js:191-201); with
+        no_recompile the compiled program, and its compile-time settings, stay."""
+        self._snelly.reset(no_recompile)
+
     def pick(self, xPick, yPick):
         """First-hit distance and material along the camera ray through pixel coordinate
         (xPick, yPick) of the frame (Renderer.prototype.pick, js/renderer.js:398-461)."""
         return self._snelly.pick(xPick, yPick)
+
+    def resize(self, width, height):
+        self._snelly.resize(width, height)
 
     def focusAt(self, x, y):
         """Set the camera's focal distance to the first hit under the frame fraction (x, y)
@@ -424,12 +446,185 @@ class Renderer:
         return hit
 
 
+class HeadlessGUI:
+    """Stands in for the dat.GUI wrapper (js/gui.js) a scene may call: there are no widgets."""
+
+    closed = True
+
+    def sync(self):
+        pass
+
+    def addParameter(self, *a, **k):
+        return self
+
+    def addFolder(self, *a, **k):
+        return self
+
+    def onChange(self, *a, **k):
+        return self
+
+
+def js_number(v):
+    """A number as JavaScript's String(v) writes it (ECMA-262 Number::toString): the shortest
+    digits that round-trip, integers without a fraction, exponent form below 1e-6 and from 1e21."""
+    v = float(v)
+    if v != v:
+        return "NaN"
+    if v in (math.inf, -math.inf):
+        return "Infinity" if v > 0 else "-Infinity"
+    if v == 0.0:
+        return "0"
+    sign = "-" if v < 0 else ""
+    m, _, e = repr(abs(v)).partition("e")
+    ip, _, fp = m.partition(".")
+    digits = (ip + fp).lstrip("0")
+    n = len(ip.lstrip("0")) if ip.strip("0") else -(len(fp) - len(fp.lstrip("0")))
+    n += int(e) if e else 0
+    digits = digits.rstrip("0") or "0"
+    k = len(digits)
+    if k <= n <= 21:
+        out = digits + "0" * (n - k)
+    elif 0 < n <= 21:
+        out = digits[:n] + "." + digits[n:]
+    elif -6 < n <= 0:
+        out = "0." + "0" * (-n) + digits
+    else:
+        out = digits[0] + ("." + digits[1:] if k > 1 else "") + "e" + ("+" if n - 1 >= 0 else "-") + str(abs(n - 1))
+    return sign + out
+
+
+def _fmt(v, lang):
+    if v is None:
+        return "undefined" if lang == "js" else "None"
+    if isinstance(v, bool):
+        return ("true" if v else "false") if lang == "js" else repr(v)
+    if isinstance(v, str):
+        return "'" + v + "'"
+    if isinstance(v, (list, tuple)):
+        return "[" + ", ".join(_fmt(x, lang) for x in v) + "]"
+    if lang == "js":
+        return js_number(v)
+    if isinstance(v, float) and not math.isfinite(v):
+        return f"float('{v!r}')"
+    return repr(float(v)) if isinstance(v, float) else repr(v)
+
+
+_DUMP_RENDERER = [
+    ("General rendering settings", ["renderMode", "dispersive", "maxSamplesPerFrame", "maxSpp", "maxBounces",
+                                    "maxAtmosphereScatters", "maxMarchSteps", "maxStepsIsMiss", "interactive",
+                                    "goalFPS", "minsSPPToRedraw", "filterRadius", "radianceClamp",
+                                    "wavelengthSamples", "shadowStrength"]),
+    ("Tone-mapping", ["exposure", "gamma", "contrast", "saturation", "hueShift"]),
+]
+_DUMP_LIGHTS = [
+    ("sky light", ["skyPower", "skyTintUp", "skyTintDown", "envMapVisible", "envMapPhiRotation",
+                   "envMapThetaRotation", "envMapTransitionAngle"]),
+    ("sun light", ["sunPower", "sunColor", "sunAngularSize", "sunLatitude", "sunLongitude", "sunVisibleDirectly"]),
+    ("sphere light", ["sphereLightPosition", "sphereLightRadius", "sphereLightPower", "sphereLightColor"]),
+]
+_REPR = {
+    "surface": ["roughness", "ior", "diffuseAlbedo", "specAlbedo", "subsurface", "subsurfaceAlbedoRGB",
+                "subsurfaceMFP", "subsurfaceAnisotropy", "subsurfaceDiffuseWeight"],
+    "metal": ["roughness", "specAlbedo"],
+    "dielectric": ["absorptionColor", "absorptionScale", "roughness", "iorVal", "abbe"],
+    "volume": ["atmosphereMinX", "atmosphereMinY", "atmosphereMinZ", "atmosphereMaxX", "atmosphereMaxY",
+               "atmosphereMaxZ", "lof10_mfp", "scatteringColor", "absorptionColor", "emission", "emissionColor",
+               "fogEmission", "fogTint", "fogMFP", "fogMaxOpticalDepth", "fogEnable"],
+}
+
+
+def material_repr(var, obj, lang="js"):
+    """Material.repr (js/materials.js:56-70 Surface, 222-243 Volume, 488-495 Metal, 740-750
+    Dielectric): one assignment per property. A property the material lacks (iorVal and abbe of a
+    non-Abbe dielectric) reads `undefined` in JavaScript and is left out in Python."""
+    end = ";" if lang == "js" else ""
+    lines = []
+    for f in _REPR[var]:
+        v = getattr(obj, f, None)
+        if v is None and lang != "js":
+            continue
+        note = " // mfp in multiples of scene scale" if (lang == "js" and f == "absorptionScale") else ""
+        lines.append(f"    {var}.{f} = {_fmt(v, lang)}{end}{note}")
+    return "\n" + "\n".join(lines) + "\n    "
+
+
+def dump_scene(snelly, lang="js"):
+    """Snelly.dumpScene (js/snelly.js:296-407) for lang "js" or "python"."""
+    if lang not in ("js", "python"):
+        raise ValueError("lang must be 'js' or 'python'")
+    js = lang == "js"
+    end = ";" if js else ""
+    com = "//" if js else "#"
+    let = "let " if js else ""
+    cam, ctl, r, mats = snelly.camera, snelly.camControls, snelly.pathtracer, snelly.materials
+    sc = snelly.sceneObj
+    out = []
+    out.append("{\n    /******* copy-pasted console output on 'O', begin *******/\n" if js
+               else "# ------- copy-pasted output of dumpScene, begin -------\n")
+    out.append(f"""
+    {let}renderer  = snelly.getRenderer(){end}
+    {let}camera    = snelly.getCamera(){end}
+    {let}controls  = snelly.getControls(){end}
+    {let}materials = snelly.getMaterials(){end}
+    """)
+    if hasattr(sc, "initGenerator"):
+        out.append(_Verbatim(sc.initGenerator()))
+    out.append(f"\nsnelly.showGUI({_fmt(bool(snelly.guiVisible), lang)}){end}\n")
+    out.append(f"\n    {'/**' if js else '#'} Camera settings {'**/' if js else ''}\n")
+    for f in ("fov", "aperture", "focalDistance", "auto_focus"):
+        v = getattr(cam, f)
+        out.append(f"    camera.{f} = {_fmt(v if isinstance(v, bool) else float(v), lang)}{end}\n")
+    for name, vec in (("camera.up", cam.up), ("camera.position", cam.position), ("controls.target", ctl.target)):
+        out.append(f"    {name}.set({_fmt(vec.x, lang)}, {_fmt(vec.y, lang)}, {_fmt(vec.z, lang)}){end}\n")
+    out.append(f"\n    {'/**' if js else '#'} Renderer settings {'**/' if js else ''}\n")
+    for title, fields in _DUMP_RENDERER:
+        out.append(f"    {com} {title}\n")
+        for f in fields:
+            out.append(f"    renderer.{f} = {_fmt(getattr(r, f), lang)}{end}\n")
+    out.append(f"    {com} Lights\n")
+    for title, fields in _DUMP_LIGHTS:
+        out.append(f"        {com} {title}\n")
+        for f in fields:
+            out.append(f"        renderer.{f} = {_fmt(getattr(r, f), lang)}{end}\n")
+    out.append(f"\n    {'/**' if js else '#'} Material settings {'**/' if js else ''}")
+    shader = sc.shader()
+    if "SDF_SURFACE(" in shader:
+        out.append(f"\n    {let}surface = materials.loadSurface(){end}")
+        out.append(material_repr("surface", mats.loadSurface(), lang))
+    if "SDF_METAL(" in shader:
+        name = mats.getLoadedMetal().getName()
+        out.append(f"\n    {let}metal = materials.loadMetal('{name}'){end}")
+        out.append(material_repr("metal", mats.loadMetal(name), lang))
+    if "SDF_DIELECTRIC(" in shader:
+        name = mats.getLoadedDielectric().getName()
+        out.append(f"\n    {let}dielectric = materials.loadDielectric('{name}'){end}")
+        out.append(material_repr("dielectric", mats.loadDielectric(name), lang))
+    out.append(f"\n    {let}volume = materials.loadVolume(){end}")
+    out.append(material_repr("volume", mats.loadVolume(), lang))
+    out.append("\n    /******* copy-pasted console output on 'O', end *******/\n}" if js
+               else "\n# ------- copy-pasted output of dumpScene, end -------\n")
+    if js:
+        return "".join(out)
+    # Python statements start at column 0; the scene's own text keeps its relative indentation
+    return "".join(textwrap.dedent(c) if isinstance(c, _Verbatim) else "\n".join(x.strip() for x in c.split("\n"))
+                   for c in out)
+
+
+class _Verbatim(str):
+    """Text a scene supplies (initGenerator), inserted into a dump as it is."""
+
+
 class Snelly:
     """The application facade of js/snelly.js, headless: one GPU context and one scene."""
 
     LAMBDA_MIN, LAMBDA_MAX, SPECTRUM_SAMPLES = 390.0, 750.0, 1024
 
     def __init__(self, scene, width=256, height=256, device=0, hbm_budget=0, context=None):
+        self._setup(scene, width, height, context if context is not None else Context(device, hbm_budget))
+        self.initScene()
+
+    def _setup(self, scene, width, height, ctx):
+        """The facade's objects with their defaults (js/snelly.js:33-105), before initScene."""
         self.sceneObj = scene
         self.width, self.height = width, height
         self.camera = Camera(45.0, width / height)
@@ -438,13 +633,20 @@ class Snelly:
         self.pathtracer = Renderer(self)
         self.spectra = {}
         self.spectrumObj = None
-        self._ctx = context if context is not None else Context(device, hbm_budget)
+        self._ctx = ctx
         self._scene_id = None
         self._scene_key = None
+        self._need_compile = True
+        self._compiled_bounces = None
         self._job = None
+        self._job_key = None
+        self._ready = False  # initScene has finished (Snelly.initialized, js/snelly.js:497-499)
+        self.guiVisible = True
+        self.guiEnabled = True
+        self.statusText = ""
+        self.gui = HeadlessGUI()
         self.seed = 1
         self.fp64 = False  # also accumulate in FP64 (precision study)
-        self.initScene()
 
     # js/snelly.js:209-291
     def initScene(self):
@@ -472,6 +674,7 @@ class Snelly:
         # spectrum, other settings); the reference has no such hook, initScene ends here.
         if hasattr(sc, "after_init"):
             sc.after_init(self)
+        self._ready = True
         self.reset()
 
     def _load_env_map(self):
@@ -537,14 +740,73 @@ class Snelly:
         self.spectra[s.getName()] = s
 
     def loadSpectrum(self, name):
+        """js/snelly.js:420-427: the emission spectrum the wavelengths are drawn from; resets
+        without a recompile."""
         self.spectrumObj = self.spectra[name]
-        self.reset()
+        self.reset(True)
+
+    def getLoadedSpectrum(self):
+        return self.spectrumObj
+
+    def getDielectrics(self):
+        return self.materials.getDielectrics()
+
+    def getMetals(self):
+        return self.materials.getMetals()
 
     def getScene(self):
         return self.sceneObj
 
-    def showGUI(self, *a):
-        pass
+    def getVersion(self):
+        """The reference version whose scene API this mirrors (js/snelly.js:107-110)."""
+        return [1, 19, 0]
+
+    def getGUI(self):
+        return self.gui
+
+    def getGLContext(self):
+        return None  # headless: there is no WebGL context
+
+    def getUserTextureUnitStart(self):
+        """js/snelly.js:660-663. Scene textures are bound by sampler name here, so the unit is
+        informational only."""
+        return 7
+
+    def showGUI(self, show):
+        self.guiVisible = bool(show)
+
+    def enableGUI(self, enable):
+        self.guiEnabled = bool(enable)
+        if not enable:
+            self.showGUI(False)
+
+    def setStatus(self, statusText):
+        self.statusText = statusText
+
+    def resize(self, width, height):
+        """Snelly._resize (js/snelly.js:588-608) with an explicit size: a headless renderer has no
+        window to follow. The camera aspect follows and the accumulation restarts."""
+        self.width, self.height = int(width), int(height)
+        self.pathtracer.width, self.pathtracer.height = self.width, self.height
+        self.camera.aspect = self.width / self.height
+        self.reset(True)
+
+    def auto_focus(self):
+        """Snelly.auto_focus (js/snelly.js:707-722): focal distance from the first hit under the
+        image centre."""
+        hit = self.pick(0.5 * self.width, 0.5 * self.height)
+        fd = max(1.0e-6, abs(hit["distance"]))
+        self.camera.focalDistance = math.log10(fd / self.lengthScale)
+        self.gui.sync()
+
+    def dumpScene(self, lang="js"):
+        """The code that re-creates the current scene, camera, renderer and material settings
+        (Snelly.dumpScene, js/snelly.js:296-407; the reference prints it on key 'O' for pasting
+        into a scene's init). lang="js" gives the reference's JavaScript text, statement for
+        statement; lang="python" the same statements for a scene written against this module
+        (exec it with `snelly` and the scene as `self` in scope). The scene's own initGenerator()
+        text is inserted as it is."""
+        return dump_scene(self, lang)
 
     # -- compile + uniforms ---------------------------------------------------------------------
     def scene_opts(self):
@@ -564,6 +826,8 @@ class Snelly:
         if key != self._scene_key:
             self._scene_id = self._ctx.scene_for(glsl, opts)
             self._scene_key = key
+        self._compiled_bounces = opts.max_bounces
+        self._need_compile = False
         return self._scene_id
 
     def uniform_params(self):
@@ -586,7 +850,9 @@ class Snelly:
         p.shadowStrength = r.shadowStrength
         p.maxSSSSteps = int(r.maxSSSSteps)
         jb = getattr(r, "jobMaxBounces", None)  # per-job limit below the module's bound
-        p.maxBounces = int(round(jb if jb else r.maxBounces))
+        if not jb:  # MAX_BOUNCES is a compile-time constant of the program that runs
+            jb = self._compiled_bounces if self._compiled_bounces is not None else r.maxBounces
+        p.maxBounces = int(round(jb))
         p.maxStepsIsMiss = 1 if r.maxStepsIsMiss else 0
         p.wavelengthSamples = int(r.wavelengthSamples)
         p.skyPower = 10.0 ** r.skyPower
@@ -645,33 +911,116 @@ class Snelly:
 
     # -- progressive rendering ---------------------------------------------------------------------
     def reset(self, no_recompile=False):
-        """Snelly.reset / Renderer.reset: drop accumulated samples (js/renderer.js:191-201)."""
+        """Snelly.reset / Renderer.reset (js/snelly.js:497-504, js/renderer.js:191-201): drop the
+        accumulated samples; without no_recompile the next frame compiles the program again from
+        the current settings (a cached module when they are unchanged). With camera.auto_focus the
+        focal distance is first set from the first hit under the image centre."""
         if self._job is not None:
             self._ctx.destroy_job(self._job)
             self._job = None
-        self.pathtracer.spp = 0.0
+        if not no_recompile:
+            self._need_compile = True
+        if self.camera.auto_focus and self._ready:
+            self.auto_focus()
+        r = self.pathtracer
+        r.numSamples = 0.0
+        r.spp = 0.0
+
+    def _scene(self):
+        """The compiled scene the next frame runs: compiled again only after a reset without
+        no_recompile (Renderer.reset, js/renderer.js:199)."""
+        if self._scene_id is None or self._need_compile:
+            self.compileShaders()
+            self._need_compile = False
+        return self._scene_id
+
+    def _frame_state(self):
+        """Everything Renderer.render uploads before a frame (js/renderer.js:520-611): the uniform
+        block, the spectrum, and the scene's recorded uniforms and textures. Compiles first when
+        a reset asked for it, since the program's compile-time bounds enter the uniform block."""
+        self._scene()
+        desc = self.render_desc(0)
+        sh = self.scene_shader()
+        key = (bytes(desc.params), bytes(desc.spectrum), repr(sorted(sh.calls.items())),
+               tuple((n, id(t), lin) for n, (t, lin) in sorted(sh.textures.items())))
+        return desc, sh, key
+
+    def _enqueue(self, frames, state):
+        """Run `frames` frames with the given frame state: a new job, or the live job after its
+        parameters are brought up to date when they changed since its last frame."""
+        desc, sh, key = state
+        sid = self._scene()
+        if self._job is None:
+            self._upload_scene(sid, sh)
+            desc.frames = int(frames)
+            self._job = self._ctx.render(sid, desc)
+            self._job_key = key
+            return
+        if key != self._job_key:
+            self._upload_scene(sid, sh)
+            self._ctx.update_job(self._job, desc)
+            self._job_key = key
+        if frames:
+            self._ctx.advance(self._job, frames)
+
+    def _upload_scene(self, sid, sh):
+        self._ctx.set_uniforms(sid, sh.calls)
+        for name, (tex, linear) in sh.textures.items():
+            self._ctx.set_texture(sid, name, tex, linear)
 
     def render(self, frames=1):
-        """Renderer.render: enqueue `frames` progressive frames (js/renderer.js:462-673)."""
-        r = self.pathtracer
-        if r.spp >= r.maxSpp:
+        """Renderer.render (js/renderer.js:462-673), called `frames` times: each frame runs the
+        scene's preframeCallback, stops once the sample count would pass maxSpp, picks up every
+        change of camera, renderer, material or scene uniforms made since the previous frame (the
+        accumulated samples stay, as in the reference, until a reset), and runs postframeCallback.
+        Frames without callbacks in between go to the GPU as one call. render(0) only compiles,
+        allocates and seeds the job."""
+        sc, r = self.sceneObj, self.pathtracer
+        if hasattr(sc, "isReady") and not sc.isReady(self):  # Snelly.render, js/snelly.js:514-521
             return
-        if hasattr(self.sceneObj, "preframeCallback"):
-            self.sceneObj.preframeCallback(self, None)
-        if self._job is None:
-            sid = self.compileShaders()
-            self.sync_scene(sid)
-            self._job = self._ctx.render(sid, self.render_desc(frames))
-        else:
-            self._ctx.advance(self._job, frames)
-        r.spp += frames * int(round(r.maxSamplesPerFrame))
-        if hasattr(self.sceneObj, "postframeCallback"):
-            self.sceneObj.postframeCallback(self, None)
+        if frames <= 0:
+            self._enqueue(0, self._frame_state())
+            return
+        pre, post = hasattr(sc, "preframeCallback"), hasattr(sc, "postframeCallback")
+        if not (pre or post):
+            n = 0
+            for _ in range(frames):
+                if not self._count_frame():
+                    break
+                n += 1
+            if n:
+                self._enqueue(n, self._frame_state())
+            return
+        for _ in range(frames):
+            if r.spp > r.maxSpp or (hasattr(sc, "isReady") and not sc.isReady(self)):
+                return
+            if pre:
+                sc.preframeCallback(self, None)
+            if not self._count_frame():
+                continue
+            self._enqueue(1, self._frame_state())
+            if post:
+                sc.postframeCallback(self, None)
+
+    def _count_frame(self):
+        """The sample bookkeeping of Renderer.render (js/renderer.js:467, 480-493): False when
+        this frame would take the mean sample count past maxSpp (which then reads maxSpp)."""
+        r = self.pathtracer
+        if r.spp > r.maxSpp:
+            return False
+        npix = self.width * self.height
+        spf = round(r.maxSamplesPerFrame)
+        r.numSamples += ((1.0 - r.skipProbability) if r.interactive else 1.0) * spf * npix
+        r.spp = r.numSamples / npix
+        if r.spp > r.maxSpp:
+            r.spp = r.maxSpp
+            return False
+        return True
 
     def pick(self, xPick, yPick):
         """Renderer.pick: {"distance", "material"} of the first hit along the pinhole ray through
         pixel coordinate (xPick, yPick) (gl_FragCoord units; a miss gives maxLengthScale and -1)."""
-        sid = self.compileShaders()
+        sid = self._scene()
         self.sync_scene(sid)
         d, m = self._ctx.pick(sid, self.render_desc(1), xPick, yPick)
         return {"distance": d, "material": m}
@@ -800,6 +1149,10 @@ class Context:
 
     def advance(self, jid, frames):
         N.check(self._lib.snelly_advance(self._h, jid, int(frames)))
+
+    def update_job(self, jid, desc):
+        """New parameters and scene uniforms for the job's next frames; samples are kept."""
+        N.check(self._lib.snelly_update_job(self._h, jid, ctypes.byref(desc)))
 
     def advance_batch(self, jobs_frames):
         """Enqueue frames on many jobs in batched launches: {job id: frames}."""

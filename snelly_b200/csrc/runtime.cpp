@@ -873,6 +873,45 @@ int snelly_advance(snelly_ctx* ctx, uint64_t job_id, int frames) {
   return c.enqueue_frames(it->second, frames);
 }
 
+int snelly_update_job(snelly_ctx* ctx, uint64_t job_id, const snelly_render_desc* desc) {
+  if (!ctx || !desc) return fail(SNELLY_EINVAL, "null argument to snelly_update_job");
+  Context& c = *ctx->c;
+  std::lock_guard<std::mutex> lk(c.mu);
+  auto it = c.jobs.find(job_id);
+  if (it == c.jobs.end()) return fail(SNELLY_ENOTFOUND, "unknown job id");
+  Job& j = it->second;
+  if (j.cancelled) return fail(SNELLY_ECANCELLED, "job was cancelled");
+  if (j.pick_at) return fail(SNELLY_EINVAL, "pick jobs cannot be updated");
+  if (desc->width != j.desc.width || desc->height != j.desc.height || desc->mode != j.desc.mode)
+    return fail(SNELLY_EINVAL, "image size and render mode are fixed for a job: reset and render a new one");
+  const SnellyParams& p = desc->params;
+  if (p.dieleModel < SNELLY_IOR_ABBE || p.dieleModel > SNELLY_IOR_CAUCHY || p.dieleNumCoeffs < 0 ||
+      p.dieleNumCoeffs > SNELLY_MAX_IOR_COEFFS)
+    return fail(SNELLY_EINVAL, "bad dielectric model");
+  // The job's own resources stay: resolution, environment map and the table pointers.
+  SnellyParams np = p;
+  np.resolution[0] = j.params.resolution[0];
+  np.resolution[1] = j.params.resolution[1];
+  np.envMap = j.params.envMap;
+  np.envMapW = j.params.envMapW;
+  np.envMapH = j.params.envMapH;
+  np.haveEnvMap = j.params.haveEnvMap;
+  np.xyzTable = j.params.xyzTable;
+  np.icdfTable = j.params.icdfTable;
+  // Every upload below is ordered on the context stream after the frames already enqueued.
+  if (memcmp(&desc->spectrum, &j.desc.spectrum, sizeof(snelly_spectrum)) != 0) {
+    std::vector<float> icdf = inverse_cdf(desc->spectrum);
+    RT_TRY(cudaMemcpyAsync(j.icdf.ptr, icdf.data(), icdf.size() * 4, cudaMemcpyHostToDevice, c.stream));
+    RT_TRY(cudaStreamSynchronize(c.stream));  // the staging vector goes out of scope
+    j.desc.spectrum = desc->spectrum;
+  }
+  j.params = np;
+  j.ublock = j.scene->ublock;
+  RT_TRY(cudaMemcpyAsync(j.gparams.ptr, &j.params, sizeof(SnellyParams), cudaMemcpyHostToDevice, c.stream));
+  RT_TRY(cudaStreamSynchronize(c.stream));  // j.params may change again before the copy runs
+  return SNELLY_OK;
+}
+
 int snelly_advance_batch(snelly_ctx* ctx, const uint64_t* job_ids, const int* frames, size_t n) {
   if (!ctx || (n && (!job_ids || !frames))) return fail(SNELLY_EINVAL, "null argument to snelly_advance_batch");
   Context& c = *ctx->c;

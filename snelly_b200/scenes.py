@@ -572,5 +572,103 @@ class SdfAsset(MeshLike):
         shader.uniform3Fv("gridSize", [float(v) for v in self.meta["EDGE"]])
 
 
+class Turntable:
+    """An animated scene written to the reference's scene template (js/sceneAPI.js:16-397): a
+    sphere smoothly blended with a box above a ground plane, the scene parameters `radius` and
+    `blend` uploaded as uniforms, init/initGenerator for those parameters, and a turntable orbit
+    of the camera about the look-at point driven from preframeCallback. Every animation frame
+    accumulates `target_spp` samples; postframeCallback then hands the finished frame to
+    `on_frame(index, snelly)` (the reference posts the canvas to a local server there) and the
+    next preframeCallback moves to the next animation frame and resets the accumulation
+    without a recompile."""
+
+    width, height = 96, 96
+
+    def __init__(self, width=None, height=None, frames=24, target_spp=16, period=24.0, on_frame=None):
+        if width:
+            self.width = width
+        if height:
+            self.height = height
+        self.frames, self.target_spp, self.period, self.on_frame = frames, target_spp, period, on_frame
+
+    def init(self, snelly):
+        self.parameters = {"radius": 0.6, "blend": 0.25}
+        self.animFrame = 0
+        self.advanceFrame = False
+        self.exported = -1
+        r = snelly.getRenderer()
+        r.width, r.height = self.width, self.height
+        r.dispersive = True
+        r.interactive = False
+        r.maxBounces = 4
+        r.maxMarchSteps = 192
+        r.skyPower = 0.0
+        r.sunPower = math.log10(4.0)
+        r.sunLatitude = 55.0
+        cam = snelly.getCamera()
+        cam.fov = 40.0
+        cam.aperture = -math.inf
+        cam.position.set(0.0, 1.2, 4.0)
+        snelly.getControls().target.set(0.2, -0.2, 0.0)
+        srf = snelly.getMaterials().loadSurface()
+        srf.diffuseAlbedo = [0.7, 0.45, 0.3]
+        srf.specAlbedo = [0.1, 0.1, 0.1]
+        srf.roughness = 0.25
+
+    def initGenerator(self):
+        """The init statements that restore the current parameters (Scene.initGenerator,
+        js/sceneAPI.js:83-91), for Snelly.dumpScene(lang="python")."""
+        return (f"\nself.parameters = {{}}\nself.parameters['radius'] = {self.parameters['radius']!r}\n"
+                f"self.parameters['blend'] = {self.parameters['blend']!r}\nself.animFrame = {self.animFrame!r}\n"
+                f"self.advanceFrame = False\nself.exported = -1\n")
+
+    def shader(self):
+        return """
+uniform float radius;
+uniform float blend;
+float sdBox(vec3 p, vec3 b) { vec3 q = abs(p) - b; return length(max(q, 0.0)) + min(max(q.x, max(q.y, q.z)), 0.0); }
+float smin(float a, float b, float k) { float h = clamp(0.5 + 0.5*(b - a)/k, 0.0, 1.0); return mix(b, a, h) - k*h*(1.0 - h); }
+float SDF_SURFACE(vec3 X)
+{
+    float s = length(X) - radius;
+    float b = sdBox(X - vec3(0.8, -0.45, 0.0), vec3(0.35));
+    return min(smin(s, b, blend), X.y + 0.8);
+}
+"""
+
+    def syncShader(self, snelly, shader):
+        shader.uniformF("radius", self.parameters["radius"])
+        shader.uniformF("blend", self.parameters["blend"])
+
+    def pose(self, snelly, frame):
+        """Camera and scene parameters of animation frame `frame`: the camera turned about the
+        vertical axis through the look-at point by 360 degrees per `period` frames, the sphere
+        radius and the blend width breathing with the same phase."""
+        if not hasattr(self, "_orbit"):
+            cam, tgt = snelly.getCamera().position, snelly.getControls().target
+            self._orbit = (tgt.tolist(), [cam.x - tgt.x, cam.y - tgt.y, cam.z - tgt.z])
+        (tx, ty, tz), (ox, oy, oz) = self._orbit
+        phase = 2.0 * math.pi * frame / self.period
+        c, s = math.cos(phase), math.sin(phase)
+        snelly.getCamera().position.set(tx + c * ox + s * oz, ty + oy, tz - s * ox + c * oz)
+        self.parameters["radius"] = 0.6 + 0.15 * math.sin(phase)
+        self.parameters["blend"] = 0.25 + 0.15 * math.cos(phase)
+
+    def preframeCallback(self, snelly, gl):
+        if self.advanceFrame:  # the previous frame was handed over: start the next one
+            self.animFrame += 1
+            self.advanceFrame = False
+            snelly.getRenderer().reset(True)
+        self.pose(snelly, self.animFrame)
+
+    def postframeCallback(self, snelly, gl):
+        r = snelly.getRenderer()
+        if self.animFrame < self.frames and r.getSPP() >= self.target_spp and self.exported != self.animFrame:
+            if self.on_frame is not None:
+                self.on_frame(self.animFrame, snelly)
+            self.exported = self.animFrame
+            self.advanceFrame = self.animFrame + 1 < self.frames
+
+
 SCENES = {"c0": PlainSphere, "c1": DispersiveFractal, "c2": VolumetricSubsurface, "atmosphere": AtmosphereLights,
-          "hooks": HooksAndMaps, "mesh": MeshLike, "envmap": EnvMapLit}
+          "hooks": HooksAndMaps, "mesh": MeshLike, "envmap": EnvMapLit, "turntable": Turntable}
