@@ -9,8 +9,9 @@ random-pose camera drawn from seed 2. A full image is 64 frames.
 Prints one JSON line (rank 0). `value`: path samples/s with all state resident on the device,
 timed with CUDA events on the renderer's stream around each step, L2 flushed between steps,
 max over ranks. `e2e`: the same through the public scene API with host buffers (per step:
-parameter upload, the frame, and a device-to-host read of the whole mean image into pinned host
-memory), wall clock. `--impl reference` times the reference's own shader built for the host CPU
+parameter upload, the frame, and a device-to-host read of the whole mean image into page-locked
+host memory, which overlaps the next step's frame), wall clock until every image is on the host.
+`--impl reference` times the reference's own shader built for the host CPU
 (oracle/_ref, else the oracle port) on a bounded pixel sample per step, all host threads.
 
 Multi-GPU: replicas (one job per GPU, no collective): `value` sums all ranks' samples over the
@@ -43,6 +44,8 @@ def parse():
     ap.add_argument("--impl", choices=["snelly", "reference"], default="snelly")
     ap.add_argument("--kernel", choices=["auto", "mega", "wavefront"], default="auto",
                     help="integrator (auto: the library's autotuner picks per scene and image size)")
+    ap.add_argument("--spp-per-step", type=int, default=1,
+                    help="frames (samples per pixel) rendered per step, as one advance of the job")
     ap.add_argument("--width", type=int, default=1920)
     ap.add_argument("--height", type=int, default=1080)
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="budget of the CPU baseline sample")
@@ -239,15 +242,17 @@ def gpu_arm(args, rank, world, local_rank):
     peak_tflops, _ = ctx.fp32_peak()
     s = api.Snelly(workload_scene(args), context=ctx)
     s.seed = 1 + rank
+    s.pathtracer.maxSpp = 1 << 30  # progressive rendering never stops inside the benchmark
     s.pathtracer.kernelMode = {"auto": N.KERNEL_AUTO, "mega": N.KERNEL_MEGA, "wavefront": N.KERNEL_WAVEFRONT}[args.kernel]
     s.render(0)  # compile, allocate, seed (and, for --kernel auto, the autotuner's trial frames)
     kernel_used = "wavefront" if ctx.job_kernel(s.job_id()) == N.KERNEL_WAVEFRONT else "mega"
     W, H = s.width, s.height
-    samples_per_step = W * H * int(round(s.pathtracer.maxSamplesPerFrame))
+    fps = max(1, args.spp_per_step)
+    samples_per_step = W * H * int(round(s.pathtracer.maxSamplesPerFrame)) * fps
     stream = torch.cuda.ExternalStream(ctx.stream())
     jid = s.job_id()
     for _ in range(args.warmup):
-        ctx.advance(jid, 1)
+        ctx.advance(jid, fps)
     ctx.sync()
     torch.cuda.synchronize()
 
@@ -263,7 +268,7 @@ def gpu_arm(args, rank, world, local_rank):
     for k in range(args.steps):
         ctx.flush_l2(256 << 20)  # evict L2 between timed steps (outside the events)
         starts[k].record(stream)
-        ctx.advance(jid, 1)
+        ctx.advance(jid, fps)
         ends[k].record(stream)
     ctx.sync()
     torch.cuda.synchronize()
@@ -275,16 +280,18 @@ def gpu_arm(args, rank, world, local_rank):
     value = world * samples_per_step * args.steps / (total_ms / 1000.0)
 
     # ---- end to end through the public API ----------------------------------------------------
-    pinned = torch.empty((H, W, 4), dtype=torch.float32, pin_memory=True).numpy()
+    # each step's image is read into one of two page-locked host buffers while the next step renders
+    pinned = [torch.empty((H, W, 4), dtype=torch.float32, pin_memory=True).numpy() for _ in range(2)]
     h2d = ctypes.sizeof(N.SnellyParams) + max(4, len(s.scene_uniforms()) * 4)
     barrier()
     t0 = time.perf_counter()
     for k in range(args.steps):
-        s.render(1)
-        s.readback(out=pinned)
+        s.render(fps)
+        s.readback(out=pinned[k % 2], wait=False)
+    ctx.sync()  # every step's image is on the host
     e2e_s = allmax(time.perf_counter() - t0)
     e2e_value = world * samples_per_step * args.steps / e2e_s
-    assert np.isfinite(pinned).all()
+    assert all(np.isfinite(p).all() for p in pinned)
 
     if rank == 0:
         from snelly_b200.testing import HostSnelly
@@ -299,7 +306,7 @@ def gpu_arm(args, rank, world, local_rank):
             "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic (procedural SDF scene, seeded camera; no dataset)",
-            "config": {"workload": WORKLOAD, "width": W, "height": H, "spp_per_step": 1, "image_spp": 64,
+            "config": {"workload": WORKLOAD, "width": W, "height": H, "spp_per_step": fps, "image_spp": 64,
                        "max_bounces": 8, "max_march_steps": 512, "dispersive": True,
                        "kernel": kernel_used, "kernel_choice": args.kernel, "math": "fast",
                        "l2": "flushed between timed steps (256 MiB write)", "parallelism": f"replicas x{world}"},

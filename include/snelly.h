@@ -175,6 +175,12 @@ int snelly_advance_batch(snelly_ctx* ctx, const uint64_t* job_ids, const int* fr
 
 #define SNELLY_READ_WAIT 1 /* block until the job's enqueued frames are done */
 #define SNELLY_READ_POLL 2 /* return SNELLY_EBUSY if not done */
+/* Enqueue the copy after the job's enqueued frames on a separate copy stream and return at once,
+ * so that the copy overlaps the frames enqueued next (no reference counterpart: gl.readPixels
+ * blocks). out_xyzn must stay valid until the copy is done: snelly_sync, or a later
+ * SNELLY_READ_WAIT readback of the same job, returns after it; page-locked memory makes the copy
+ * asynchronous. Frames enqueued afterwards write the job's mean image only once the copy is done. */
+#define SNELLY_READ_ASYNC 4
 /* Mean XYZ and sample count per pixel: width*height*4 floats (X, Y, Z, N). */
 int snelly_readback(snelly_ctx* ctx, uint64_t job_id, float* out_xyzn, size_t bytes, int flags);
 /* Mean values per pixel of a first-hit job: NORMALS and AO give mean XYZ and the frame count;

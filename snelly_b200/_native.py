@@ -21,7 +21,7 @@ KERNEL_AUTO, KERNEL_MEGA, KERNEL_WAVEFRONT = 0, 1, 2
 MATH_FAST, MATH_STRICT = 0, 1
 MODE_PT, MODE_NORMALS, MODE_AO, MODE_PICK, MODE_PTSIMPLE = 0, 1, 2, 3, 4
 SPECTRUM_BLACKBODY, SPECTRUM_FLAT, SPECTRUM_MONO = 0, 1, 2
-READ_WAIT, READ_POLL = 1, 2
+READ_WAIT, READ_POLL, READ_ASYNC = 1, 2, 4
 U_FLOAT, U_INT, U_BOOL, U_VEC2, U_VEC3, U_VEC4 = 0, 1, 2, 3, 4, 5
 U_IVEC2, U_IVEC3, U_IVEC4, U_MAT2, U_MAT3, U_MAT4, U_SAMPLER2D, U_SAMPLER3D = 6, 7, 8, 9, 10, 11, 12, 13
 IOR_MODELS = {"abbe": 0, "sellmeier": 1, "sellmeier2": 2, "polyanskiy": 3, "cauchy": 4}

@@ -1025,9 +1025,11 @@ class Snelly:
         d, m = self._ctx.pick(sid, self.render_desc(1), xPick, yPick)
         return {"distance": d, "material": m}
 
-    def readback(self, out=None):
-        """(H, W, 4) float32 array: mean X, Y, Z and sample count; row 0 is the bottom row."""
-        return self._ctx.readback(self._job, self.width, self.height, out=out)
+    def readback(self, out=None, wait=True):
+        """(H, W, 4) float32 array: mean X, Y, Z and sample count; row 0 is the bottom row.
+        wait=False only enqueues the copy into `out` behind the frames rendered so far, so that it
+        overlaps the next frames; `out` holds the image once the context's sync() returns."""
+        return self._ctx.readback(self._job, self.width, self.height, out=out, wait=wait)
 
     def tonemap_params(self):
         """The tonemapper's uniforms as Renderer.render uploads them (js/renderer.js:623-630)."""
@@ -1187,10 +1189,16 @@ class Context:
                                       ctypes.byref(m)))
         return d.value, m.value
 
-    def readback(self, jid, width, height, out=None, poll=False):
+    def readback(self, jid, width, height, out=None, poll=False, wait=True):
+        """Mean XYZ and count per pixel. wait=False enqueues the copy behind the job's frames and
+        returns at once (SNELLY_READ_ASYNC): `out` (page-locked for an overlapped copy) is filled
+        once sync() returns, or a later waiting readback of the job."""
         if out is None:
+            if not wait:
+                raise ValueError("an asynchronous readback needs its output array")
             out = np.empty((height, width, 4), np.float32)
-        N.check(self._lib.snelly_readback(self._h, jid, out.ctypes.data, out.nbytes, N.READ_POLL if poll else N.READ_WAIT))
+        flags = N.READ_ASYNC if not wait else (N.READ_POLL if poll else N.READ_WAIT)
+        N.check(self._lib.snelly_readback(self._h, jid, out.ctypes.data, out.nbytes, flags))
         return out
 
     def readback_state(self, jid, width, height, fp64=False):

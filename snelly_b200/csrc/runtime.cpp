@@ -40,12 +40,6 @@ static const float kXyzTable[4 * SNELLY_XYZ_SAMPLES] = {
 #include "cie_xyz_table.inc"
 };
 
-#define RT_TRY(expr)                                                                        \
-  do {                                                                                      \
-    cudaError_t e_ = (expr);                                                                \
-    if (e_ != cudaSuccess) return fail(SNELLY_EDEVICE, std::string(#expr) + ": " + cudaGetErrorString(e_)); \
-  } while (0)
-
 // ---- device buffers under the context's HBM budget --------------------------------------------
 int Context::alloc(DevBuf& b, size_t bytes) {
   b.bytes = 0;
@@ -389,6 +383,7 @@ int Context::enqueue_frames(Job& j, int frames) {
     if (rc) return rc;
   }
   void* rargs[] = {&tables, &bstart, &njobs};
+  if (j.read_pending) RT_TRY(cudaStreamWaitEvent(stream, j.read_done, 0));  // `out` is being copied out
   rc = launch(m.f_resolve, j.blocks, SNELLY_BLOCK, rargs);
   if (rc) return rc;
   j.frames_enqueued += frames;
@@ -481,6 +476,7 @@ int Context::advance_batch(const std::vector<Job*>& js, const std::vector<int>& 
         void* bstart = (char*)j.tables.ptr + 128;
         int one = 1;
         void* rargs[] = {&tables, &bstart, &one};
+        if (j.read_pending) RT_TRY(cudaStreamWaitEvent(L.stream, j.read_done, 0));  // `out` is being copied out
         RT_TRY(cudaLaunchKernel((const void*)m.f_resolve, dim3((unsigned)j.blocks), dim3(SNELLY_BLOCK), rargs, 0,
                                 L.stream));
         launches++;
@@ -512,16 +508,33 @@ Context::~Context() {
     for (auto& t : kv.second.textures) release(t.second);
     for (auto& t : kv.second.retired_textures) release(t);
   }
+  if (copy_stream) cudaStreamSynchronize(copy_stream);
   release(xyz);
   release(stats_scratch);
   if (poll_host) cudaFreeHost(poll_host);
-  for (auto& e : poll_done)
+  for (auto& row : poll_done)
+    for (auto& e : row)
+      if (e) cudaEventDestroy(e);
+  for (int k = 1; k < SNELLY_WF_MAX_PARTS; ++k)
+    if (wf_streams[k]) {
+      cudaStreamSynchronize(wf_streams[k]);
+      cudaStreamDestroy(wf_streams[k]);
+    }
+  if (wf_fork) cudaEventDestroy(wf_fork);
+  for (auto& e : wf_join)
     if (e) cudaEventDestroy(e);
   for (auto& kv : module_cache) cudaLibraryUnload(kv.second->lib);
+  if (copy_stream) cudaStreamDestroy(copy_stream);
   cudaStreamDestroy(stream);
 }
 
 void Context::free_job(Job& j) {
+  if (j.read_done) {  // an asynchronous readback may still be copying `out`
+    cudaEventSynchronize(j.read_done);
+    cudaEventDestroy(j.read_done);
+    j.read_done = nullptr;
+    j.read_pending = false;
+  }
   release(j.rng);
   release(j.acc);
   release(j.comp);
@@ -574,6 +587,8 @@ int snelly_init(snelly_ctx** out, int device, size_t budget) {
   if (!file_exists(c->kernel_dir + "/pt_kernels.cu"))
     return fail(SNELLY_EINVAL, "kernel sources not found under " + c->kernel_dir);
   if (const char* dr = getenv("SNELLY_WF_DRAIN")) c->wf_drain_steps = atoi(dr);  // 0: never park rays
+  if (const char* pi = getenv("SNELLY_WF_PARK_ITERS")) c->wf_park_iters = atoi(pi);
+  if (const char* sp = getenv("SNELLY_WF_SPLIT")) c->wf_split = std::max(1, std::min(atoi(sp), SNELLY_WF_MAX_PARTS));
   const char* cdir = getenv("SNELLY_CACHE_DIR");
   c->cache_dir = cdir ? std::string(cdir) : dir + "/_build/kcache";
   mkdir((dir + "/_build").c_str(), 0755);
@@ -957,8 +972,21 @@ int snelly_readback(snelly_ctx* ctx, uint64_t job_id, float* out, size_t bytes, 
   if (j.cancelled) return fail(SNELLY_ECANCELLED, "job was cancelled");
   size_t need = (size_t)j.desc.width * j.desc.height * 16;
   if (bytes < need) return fail(SNELLY_EINVAL, "output buffer too small: need " + std::to_string(need) + " bytes");
+  if (flags & SNELLY_READ_ASYNC) {  // copy after the enqueued frames, on the copy stream; return now
+    if (!c.copy_stream) RT_TRY(cudaStreamCreateWithFlags(&c.copy_stream, cudaStreamNonBlocking));
+    if (!j.read_done) RT_TRY(cudaEventCreateWithFlags(&j.read_done, cudaEventDisableTiming));
+    RT_TRY(cudaStreamWaitEvent(c.copy_stream, j.done, 0));
+    RT_TRY(cudaMemcpyAsync(out, j.out.ptr, need, cudaMemcpyDeviceToHost, c.copy_stream));
+    RT_TRY(cudaEventRecord(j.read_done, c.copy_stream));
+    j.read_pending = true;
+    return SNELLY_OK;
+  }
   int rc = wait_job(c, j, flags);
   if (rc) return rc;
+  if (j.read_pending) {  // earlier asynchronous copies of this job are complete when this returns
+    RT_TRY(cudaEventSynchronize(j.read_done));
+    j.read_pending = false;
+  }
   RT_TRY(cudaMemcpyAsync(out, j.out.ptr, need, cudaMemcpyDeviceToHost, c.stream));
   RT_TRY(cudaStreamSynchronize(c.stream));
   return SNELLY_OK;
@@ -1060,6 +1088,7 @@ int snelly_destroy_job(snelly_ctx* ctx, uint64_t job_id) {
 int snelly_sync(snelly_ctx* ctx) {
   if (!ctx) return fail(SNELLY_EINVAL, "ctx is null");
   RT_TRY(cudaStreamSynchronize(ctx->c->stream));
+  if (ctx->c->copy_stream) RT_TRY(cudaStreamSynchronize(ctx->c->copy_stream));  // SNELLY_READ_ASYNC copies
   return SNELLY_OK;
 }
 

@@ -10,6 +10,15 @@
 
 #include "glsl_transform.h"
 #include "kernels/pt_launch.h"
+
+// Return SNELLY_EDEVICE with the failing call and CUDA's message (needs `fail` in scope).
+#define RT_TRY(expr)                                                                        \
+  do {                                                                                      \
+    cudaError_t e_ = (expr);                                                                \
+    if (e_ != cudaSuccess) return fail(SNELLY_EDEVICE, std::string(#expr) + ": " + cudaGetErrorString(e_)); \
+  } while (0)
+
+#define SNELLY_WF_MAX_PARTS 8  // concurrent wavefront pixel ranges of one job, at most
 #include "snelly.h"
 
 static_assert(JOB_MODE_PT == SNELLY_MODE_PT && JOB_MODE_NORMALS == SNELLY_MODE_NORMALS &&
@@ -79,7 +88,8 @@ struct Job {
   DevBuf rng, acc, comp, acc64, out, icdf, env, gparams, tables;
   DevBuf display;  // tonemapped image (snelly_tonemap), allocated on first use
   DevBuf wf;  // wavefront path state and queues
-  WfBuffers wfb{};
+  WfBuffers wfb[SNELLY_WF_MAX_PARTS]{};  // one set per pixel range, each run on its own stream
+  int wf_parts = 0;
   int blocks = 0;
   int kernel_mode = SNELLY_KERNEL_MEGA;  // the integrator this job's frames run (after tuning)
   int pick_at = 0;           // a one-pixel pick job (snelly_pick)
@@ -87,6 +97,8 @@ struct Job {
   int frames_enqueued = 0;
   bool cancelled = false;
   cudaEvent_t done = nullptr;
+  cudaEvent_t read_done = nullptr;  // the last SNELLY_READ_ASYNC copy of `out` (on the copy stream)
+  bool read_pending = false;
 };
 
 // Device-side tables of a batched launch, one set per batch stream.
@@ -101,6 +113,7 @@ struct Context {
   int device = 0;
   int sm_count = 0;
   cudaStream_t stream = nullptr;
+  cudaStream_t copy_stream = nullptr;  // SNELLY_READ_ASYNC device-to-host copies (created on first use)
   std::mutex mu;
   std::map<uint64_t, Scene> scenes;
   std::map<uint64_t, Job> jobs;
@@ -113,8 +126,12 @@ struct Context {
   std::vector<BatchLane> lanes;  // batch streams (created on first use)
   std::map<std::string, int> tuned;  // autotuner decisions: (module, image-size class) -> integrator
   int wf_drain_steps = 64;           // steps an extend warp marches once its work runs out (SNELLY_WF_DRAIN)
+  int wf_park_iters = -1;            // iterations that may park rays; -1: 3 x (max_bounces + 2) (SNELLY_WF_PARK_ITERS)
+  int wf_split = 3;                  // wavefront pixel ranges run concurrently (SNELLY_WF_SPLIT)
   int* poll_host = nullptr;          // pinned words the wavefront's paths-left reads land in
-  cudaEvent_t poll_done[2] = {nullptr, nullptr};
+  cudaEvent_t poll_done[2][SNELLY_WF_MAX_PARTS] = {};
+  cudaStream_t wf_streams[SNELLY_WF_MAX_PARTS] = {};  // [0] is the context stream
+  cudaEvent_t wf_fork = nullptr, wf_join[SNELLY_WF_MAX_PARTS] = {};
   DevBuf stats_scratch;          // image-statistics partial sums
 
   ~Context();

@@ -1,16 +1,26 @@
 // wavefront.cpp - host side of the wavefront integrator (kernels in kernels/pt_wavefront.cuh):
-// the per-path state and queues in HBM, and the stage launches of one frame.
+// the per-path state and queues in HBM, and the stage launches of one frame on one or more
+// concurrent streams.
+#include <algorithm>
+
 #include "runtime_internal.h"
 
 namespace snelly {
 
+// The job's pixels are split into up to wf_split contiguous ranges ("parts"), each with its own
+// path state, queues and counters, whose stages run on their own streams: while one part's
+// extend launch drains (its last, longest rays on few lanes) or its shade stage runs, the other
+// parts' launches fill the SMs it leaves idle. A path's computation does not depend on its part.
 int Context::alloc_wavefront(Job& j) {
   if (j.scene->opts.max_samples_per_frame != 1) return SNELLY_OK;  // served by the per-pixel kernel
   const size_t P = (size_t)j.desc.width * j.desc.height;
-  const size_t f4 = 16 * P;
-  // 17 float4 arrays + info + rng + parked-ray state (3 per path), shadow flags, pending counts,
-  // int queues (2 active, 2 x 2 shadow, 2 x 3 parked, 4 shade), counters
-  size_t bytes = 19 * f4 + 3 * f4 + 2 * P + 4 * P + (2 + 2 * 2 + 2 * 3 + 4) * 4 * P + 4 * WF_COUNTERS + 32 * 256;
+  int parts = std::max(1, std::min(wf_split, SNELLY_WF_MAX_PARTS));
+  if (P < (size_t)parts * 65536) parts = 1;  // small images: one part keeps each launch full
+  // per path: 17 float4 arrays + info + rng + parked-ray state (3 per path), shadow flags, pending
+  // count, int queues (2 active, 2 x 2 shadow, 2 x 3 parked, 4 shade); per part: counters and
+  // the 256-byte alignment of its 30 sub-buffers
+  size_t bytes = (19 * 16 + 3 * 16 + 2 + 4 + (2 + 2 * 2 + 2 * 3 + 4) * 4) * P +
+                 (size_t)parts * (4 * WF_COUNTERS + 32 * 256);
   int rc = alloc(j.wf, bytes);
   if (rc) return rc;
   char* p = (char*)j.wf.ptr;
@@ -19,93 +29,134 @@ int Context::alloc_wavefront(Job& j) {
     p += (n + 255) / 256 * 256;
     return q;
   };
-  WfBuffers& B = j.wfb;
-  float4** f4s[] = {&B.pos, &B.dir, &B.thr, &B.rad, &B.cmf, &B.mis, &B.xyzw, &B.hit, &B.nee_org, &B.nee_thr,
-                    &B.nee_extra, &B.nee_dir[0], &B.nee_dir[1], &B.nee_c[0], &B.nee_c[1], &B.nee_li[0],
-                    &B.nee_li[1]};
-  for (float4** q : f4s) *q = (float4*)take(f4);
-  B.info = (int4*)take(f4);
-  B.rng = (uint4*)take(f4);
-  B.mt = (float4*)take(3 * f4);
-  B.pend = (int*)take(4 * P);
-  B.qc[0] = (int*)take(12 * P);
-  B.qc[1] = (int*)take(12 * P);
-  B.qa[0] = (int*)take(4 * P);
-  B.qa[1] = (int*)take(4 * P);
-  B.qs[0] = (int*)take(8 * P);
-  B.qs[1] = (int*)take(8 * P);
-  B.qshade = (int*)take(16 * P);
-  B.cnt = (int*)take(4 * WF_COUNTERS);
-  B.shadow = (unsigned char*)take(2 * P);
-  B.paths = (int)P;
-  B.pixel_begin = 0;
+  size_t begin = 0;
+  for (int k = 0; k < parts; ++k) {
+    const size_t Pk = P / parts + ((size_t)k < P % parts ? 1 : 0);
+    const size_t f4 = 16 * Pk;
+    WfBuffers& B = j.wfb[k];
+    float4** f4s[] = {&B.pos, &B.dir, &B.thr, &B.rad, &B.cmf, &B.mis, &B.xyzw, &B.hit, &B.nee_org, &B.nee_thr,
+                      &B.nee_extra, &B.nee_dir[0], &B.nee_dir[1], &B.nee_c[0], &B.nee_c[1], &B.nee_li[0],
+                      &B.nee_li[1]};
+    for (float4** q : f4s) *q = (float4*)take(f4);
+    B.info = (int4*)take(f4);
+    B.rng = (uint4*)take(f4);
+    B.mt = (float4*)take(3 * f4);
+    B.pend = (int*)take(4 * Pk);
+    B.qc[0] = (int*)take(12 * Pk);
+    B.qc[1] = (int*)take(12 * Pk);
+    B.qa[0] = (int*)take(4 * Pk);
+    B.qa[1] = (int*)take(4 * Pk);
+    B.qs[0] = (int*)take(8 * Pk);
+    B.qs[1] = (int*)take(8 * Pk);
+    B.qshade = (int*)take(16 * Pk);
+    B.cnt = (int*)take(4 * WF_COUNTERS);
+    B.shadow = (unsigned char*)take(2 * Pk);
+    B.paths = (int)Pk;
+    B.pixel_begin = (int)begin;
+    begin += Pk;
+  }
+  j.wf_parts = parts;
   if ((size_t)(p - (char*)j.wf.ptr) > bytes) return fail(SNELLY_EDEVICE, "wavefront buffer layout overflow");
   return SNELLY_OK;
 }
 
 void Context::release_wavefront(Job& j) {
   release(j.wf);
-  j.wfb = WfBuffers{};
+  for (auto& B : j.wfb) B = WfBuffers{};
+  j.wf_parts = 0;
 }
 
 int Context::enqueue_wavefront_frame(Job& j) {
   Module& m = *j.module;
-  if (!j.wf.ptr || !m.f_wf_generate || !m.f_wf_extend || !m.f_wf_shade)
+  if (!j.wf.ptr || j.wf_parts < 1 || !m.f_wf_generate || !m.f_wf_extend || !m.f_wf_shade)
     return fail(SNELLY_EINVAL, "wavefront integrator not available for this job");
+  const int parts = j.wf_parts;
+  // streams and events, created on first use; part 0 runs on the context stream
+  wf_streams[0] = stream;
+  for (int k = 1; k < parts; ++k)
+    if (!wf_streams[k]) RT_TRY(cudaStreamCreateWithFlags(&wf_streams[k], cudaStreamNonBlocking));
+  if (!wf_fork) RT_TRY(cudaEventCreateWithFlags(&wf_fork, cudaEventDisableTiming));
+  for (int k = 0; k < parts; ++k)
+    if (!wf_join[k]) RT_TRY(cudaEventCreateWithFlags(&wf_join[k], cudaEventDisableTiming));
+  if (!poll_host) {
+    if (cudaMallocHost((void**)&poll_host, 2 * SNELLY_WF_MAX_PARTS * sizeof(int)) != cudaSuccess) {
+      poll_host = nullptr;
+      return fail(SNELLY_EDEVICE, "pinned host allocation failed");
+    }
+  }
+  for (auto& row : poll_done)
+    for (int k = 0; k < parts; ++k)
+      if (!row[k]) RT_TRY(cudaEventCreateWithFlags(&row[k], cudaEventDisableTiming));
+  // the other parts start after the work already on the context stream (parameter upload)
+  RT_TRY(cudaEventRecord(wf_fork, stream));
+  for (int k = 1; k < parts; ++k) RT_TRY(cudaStreamWaitEvent(wf_streams[k], wf_fork, 0));
   void* jobs = j.tables.ptr;
   void* gparams = j.gparams.ptr;
-  WfBuffers B = j.wfb;
-  int gen_blocks = (B.paths + SNELLY_BLOCK - 1) / SNELLY_BLOCK;
-  void* gargs[] = {&jobs, &gparams, &B};
-  int rc = launch(m.f_wf_generate, gen_blocks, SNELLY_BLOCK, gargs);
-  if (rc) return rc;
+  auto launch_on = [&](int k, cudaKernel_t f, int blocks, void** args) -> int {
+    RT_TRY(cudaLaunchKernel((const void*)f, dim3((unsigned)blocks), dim3(SNELLY_BLOCK), args, 0, wf_streams[k]));
+    launches++;
+    return SNELLY_OK;
+  };
+  int rc;
+  for (int k = 0; k < parts; ++k) {
+    WfBuffers B = j.wfb[k];
+    void* gargs[] = {&jobs, &gparams, &B};
+    if ((rc = launch_on(k, m.f_wf_generate, (B.paths + SNELLY_BLOCK - 1) / SNELLY_BLOCK, gargs))) return rc;
+  }
   // Iterations: the first `budgeted` ones park the slowest rays when their work runs out; after
   // them every iteration advances every path by one vertex, so `nominal` more always finish the
-  // frame. Beyond the nominal count, iterations go in pairs, each followed by a read of the
-  // paths-left count; the host waits for the read of the pair before last, so the GPU always
-  // has the next pair queued, and stops once a read shows zero (an extra pair then finds empty
-  // queues and returns at once).
+  // frame. Beyond the nominal count, iterations go in pairs, each followed by a read of every
+  // part's paths-left count; the host waits for the reads of the pair before last, so the GPU
+  // always has the next pair queued, and stops once they all show zero (an extra pair then finds
+  // empty queues and returns at once). Each part's launches go to its own stream in order.
   const int nominal = j.scene->opts.max_bounces + 2;
-  const int budgeted = 3 * nominal;
+  const int budgeted = wf_park_iters >= 0 ? std::min(wf_park_iters, 8 * nominal) : 3 * nominal;
   const int max_iters = budgeted + nominal;
   if (max_iters + 2 > WF_MAX_ITERS) return fail(SNELLY_EINVAL, "too many wavefront iterations for max_bounces");
   const int extend_blocks = sm_count * m.extend_blocks_per_sm, shade_blocks = sm_count * 4;
   int it = 0;
-  auto pair = [&]() {
+  auto pair = [&]() -> int {
     int drain = it < budgeted ? wf_drain_steps : 0;
-    void* eargs[] = {&B, &it, &drain};
-    int r = launch(m.f_wf_extend, extend_blocks, SNELLY_BLOCK, eargs);
-    if (r) return r;
-    void* sargs[] = {&jobs, &gparams, &B, &it};
-    r = launch(m.f_wf_shade, shade_blocks, SNELLY_BLOCK, sargs);
+    for (int k = 0; k < parts; ++k) {
+      WfBuffers B = j.wfb[k];
+      void* eargs[] = {&B, &it, &drain};
+      int r = launch_on(k, m.f_wf_extend, extend_blocks, eargs);
+      if (r) return r;
+      void* sargs[] = {&jobs, &gparams, &B, &it};
+      r = launch_on(k, m.f_wf_shade, shade_blocks, sargs);
+      if (r) return r;
+    }
     ++it;
-    return r;
+    return SNELLY_OK;
   };
   while (it < nominal)
     if ((rc = pair())) return rc;
-  if (!poll_host) {
-    if (cudaMallocHost((void**)&poll_host, 2 * sizeof(int)) != cudaSuccess) {
-      poll_host = nullptr;
-      return fail(SNELLY_EDEVICE, "pinned host allocation failed");
-    }
-    for (auto& e : poll_done)
-      if (cudaEventCreateWithFlags(&e, cudaEventDisableTiming) != cudaSuccess)
-        return fail(SNELLY_EDEVICE, "event creation failed");
-  }
   int checks = 0;
   while (it < max_iters) {
     if ((rc = pair())) return rc;
     if ((rc = pair())) return rc;
     const int slot = checks & 1;
-    if (cudaMemcpyAsync(poll_host + slot, B.cnt + WF_LEFT, sizeof(int), cudaMemcpyDeviceToHost, stream) != cudaSuccess ||
-        cudaEventRecord(poll_done[slot], stream) != cudaSuccess)
-      return fail(SNELLY_EDEVICE, "wavefront progress read failed");
+    for (int k = 0; k < parts; ++k)
+      if (cudaMemcpyAsync(poll_host + slot * SNELLY_WF_MAX_PARTS + k, j.wfb[k].cnt + WF_LEFT, sizeof(int),
+                          cudaMemcpyDeviceToHost, wf_streams[k]) != cudaSuccess ||
+          cudaEventRecord(poll_done[slot][k], wf_streams[k]) != cudaSuccess)
+        return fail(SNELLY_EDEVICE, "wavefront progress read failed");
     ++checks;
     if (checks >= 2) {
       const int prev = (checks - 2) & 1;
-      if (cudaEventSynchronize(poll_done[prev]) != cudaSuccess) return fail(SNELLY_EDEVICE, "wavefront progress wait failed");
-      if (poll_host[prev] == 0) break;
+      int left = 0;
+      for (int k = 0; k < parts; ++k) {
+        if (cudaEventSynchronize(poll_done[prev][k]) != cudaSuccess)
+          return fail(SNELLY_EDEVICE, "wavefront progress wait failed");
+        left += poll_host[prev * SNELLY_WF_MAX_PARTS + k];
+      }
+      if (left == 0) break;
     }
+  }
+  // later work on the context stream (resolve, readback) waits for every part
+  for (int k = 1; k < parts; ++k) {
+    RT_TRY(cudaEventRecord(wf_join[k], wf_streams[k]));
+    RT_TRY(cudaStreamWaitEvent(stream, wf_join[k], 0));
   }
   return SNELLY_OK;
 }

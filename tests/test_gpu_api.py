@@ -118,3 +118,30 @@ def test_autotuned_kernel_choice_leaves_no_trace(gpu_ctx):
     img_again, k3 = run(N.KERNEL_AUTO)
     assert k3 == k
     np.testing.assert_array_equal(img_again, img_auto)
+
+
+def test_async_readback_overlaps_and_matches(gpu_ctx):
+    """SNELLY_READ_ASYNC: the copy is ordered after the frames enqueued before it and before the
+    frames enqueued after it touch the mean image; page-locked and pageable outputs both hold the
+    image of their moment once the context is synchronised."""
+    import torch
+    s = api.Snelly(scenes.PlainSphere(64, 48), context=gpu_ctx)
+    pinned = [torch.empty((48, 64, 4), dtype=torch.float32, pin_memory=True).numpy() for _ in range(2)]
+    pageable = np.full((48, 64, 4), -1.0, np.float32)
+    s.render(2)
+    s.readback(out=pinned[0], wait=False)
+    s.render(3)
+    s.readback(out=pinned[1], wait=False)
+    s.readback(out=pageable, wait=False)
+    gpu_ctx.sync()
+    ref2 = api.Snelly(scenes.PlainSphere(64, 48), context=gpu_ctx)
+    ref2.render(2)
+    np.testing.assert_array_equal(pinned[0], ref2.readback())
+    np.testing.assert_array_equal(pinned[1], s.readback())
+    np.testing.assert_array_equal(pageable, pinned[1])
+    assert (pinned[1][..., 3] == 5).all()
+    # a job destroyed right after an asynchronous readback waits for the copy
+    s.render(1)
+    s.readback(out=pinned[0], wait=False)
+    gpu_ctx.destroy_job(s.job_id())
+    assert (pinned[0][..., 3] == 6).all()

@@ -188,3 +188,29 @@ def test_wavefront_parking_does_not_change_results(name):
         ctx.close()
     np.testing.assert_array_equal(imgs[0], imgs[1])
     np.testing.assert_array_equal(imgs[0], imgs[2])
+
+
+@pytest.mark.parametrize("name", ["c1", "atmosphere"])
+def test_wavefront_split_does_not_change_results(name):
+    """The wavefront splits a large image into pixel ranges whose stages run on concurrent
+    streams; one, two and four ranges give the same image bit for bit (a path's computation does
+    not depend on its range)."""
+    import os
+    from snelly_b200 import api
+    imgs = []
+    for split in ("1", "2", "4"):
+        old = os.environ.pop("SNELLY_WF_SPLIT", None)
+        os.environ["SNELLY_WF_SPLIT"] = split
+        try:
+            ctx = api.Context(0)
+        finally:
+            os.environ.pop("SNELLY_WF_SPLIT", None)
+            if old is not None:
+                os.environ["SNELLY_WF_SPLIT"] = old
+        scene = {"c1": scenes.DispersiveFractal, "atmosphere": scenes.AtmosphereLights}[name](512, 512)
+        s, img = gpu_render(ctx, scene, 2, seed=5, kernel_mode=N.KERNEL_WAVEFRONT)
+        imgs.append(img.copy())
+        ctx.destroy_job(s.job_id())
+        ctx.close()
+    np.testing.assert_array_equal(imgs[0], imgs[1])
+    np.testing.assert_array_equal(imgs[0], imgs[2])
