@@ -1,10 +1,11 @@
 #!/usr/bin/env python
 """Benchmark: spectral path samples per second on the 1080p dispersive + metallic fractal workload.
 
-Workload (one step = one progressive frame = one spectral path sample per pixel): a 5-iteration
-Menger sponge (Cauchy dielectric, roughness 0.02), a tabulated-gold sphere and a diffuse ground
-plane under a 3-degree sun and a sky, 1920x1080, maxBounces 8, maxMarchSteps 512, dispersive,
-random-pose camera drawn from seed 2. A full image is 64 frames.
+Workload (one step = one full image: 64 progressive frames, i.e. 64 spectral path samples per
+pixel, in one advance of the job; --spp-per-step changes it): a 5-iteration Menger sponge
+(Cauchy dielectric, roughness 0.02), a tabulated-gold sphere and a diffuse ground plane under a
+3-degree sun and a sky, 1920x1080, maxBounces 8, maxMarchSteps 512, dispersive, random-pose
+camera drawn from seed 2.
 
 Prints one JSON line (rank 0). `value`: path samples/s with all state resident on the device,
 timed with CUDA events on the renderer's stream around each step, L2 flushed between steps,
@@ -44,8 +45,9 @@ def parse():
     ap.add_argument("--impl", choices=["snelly", "reference"], default="snelly")
     ap.add_argument("--kernel", choices=["auto", "mega", "wavefront"], default="auto",
                     help="integrator (auto: the library's autotuner picks per scene and image size)")
-    ap.add_argument("--spp-per-step", type=int, default=1,
-                    help="frames (samples per pixel) rendered per step, as one advance of the job")
+    ap.add_argument("--spp-per-step", type=int, default=64,
+                    help="frames (samples per pixel) rendered per step, as one advance of the job "
+                         "(64: one full image of the workload)")
     ap.add_argument("--width", type=int, default=1920)
     ap.add_argument("--height", type=int, default=1080)
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="budget of the CPU baseline sample")
@@ -200,13 +202,14 @@ def reference_arm(args, rank):
         run(min(per_step, 2000))
     times = [run(per_step) for _ in range(args.steps)]
     value = per_step * args.steps / sum(times)
-    sample = f"{per_step} random pixels x 1 frame per step of the {host.width}x{host.height} workload"
+    sample = (f"{per_step} random pixels x 1 frame per step of the {host.width}x{host.height} workload "
+              f"(a bounded sample of its {args.spp_per_step}-frame step)")
     out = {"impl": "reference", "metric": METRIC, "value": value, "unit": "path samples/s", "n_gpus": args.gpus,
            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * sum(times) / args.steps,
            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
            "data": "synthetic (procedural SDF scene, seeded camera)",
-           "config": {"workload": WORKLOAD, "width": host.width, "height": host.height, "spp_per_step": 1,
-                      "device": "host CPU"},
+           "config": {"workload": WORKLOAD, "width": host.width, "height": host.height,
+                      "spp_per_step": args.spp_per_step, "device": "host CPU"},
            "cpu_baseline": {"value": value, "unit": "path samples/s", "cores": os.cpu_count(), "kind": kind,
                             "sample": sample},
            "e2e": {"value": value, "unit": "path samples/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
@@ -300,6 +303,7 @@ def gpu_arm(args, rank, world, local_rank):
         per_launch_ms = statistics.mean(step_ms)
         achieved = fpp * samples_per_step / (per_launch_ms / 1000.0) / 1e12
         kname = "pt_frame_mega" if kernel_used == "mega" else "pt_wavefront"
+        frame_traffic = traffic_from_profiles(kname)  # DRAM bytes of one 1080p frame (ncu summary)
         cpu = None if args.no_cpu_baseline else cpu_baseline(host, args.cpu_seconds)
         out = {
             "metric": METRIC, "value": value, "unit": "path samples/s", "n_gpus": world, "steps": args.steps,
@@ -314,7 +318,7 @@ def gpu_arm(args, rank, world, local_rank):
                     "d2h_bytes_per_step": W * H * 16},
             "gpu_launches": int(launches),
             "roofline": {"bound": "fp32", "achieved": achieved, "peak": peak_tflops, "unit": "TFLOP/s",
-                         "frac": achieved / peak_tflops, "traffic": traffic_from_profiles(kname),
+                         "frac": achieved / peak_tflops, "traffic": frame_traffic * fps if frame_traffic else None,
                          "flops_per_path": fpp, "special_ops_per_path": spp_special,
                          "peak_source": "measured FFMA microbenchmark in this run (snelly_measure_fp32_peak)"},
             "clocks": clk,

@@ -366,13 +366,11 @@ int Context::enqueue_frames(Job& j, int frames) {
   int njobs = 1;
   void* gparams = j.gparams.ptr;
   void* args[] = {&tables, &bstart, &njobs, &gparams};
-  for (int f = 0; f < frames; ++f) {
+  const bool wavefront = j.desc.mode == SNELLY_MODE_PT && j.kernel_mode == SNELLY_KERNEL_WAVEFRONT && m.f_wf_generate;
+  if (wavefront && (rc = enqueue_wavefront_frames(j, frames))) return rc;  // every frame, pipelined by pixel range
+  for (int f = 0; f < frames && !wavefront; ++f) {
     if (j.desc.mode == SNELLY_MODE_PT) {
-      if (j.kernel_mode == SNELLY_KERNEL_WAVEFRONT && m.f_wf_generate) {
-        rc = enqueue_wavefront_frame(j);
-      } else {
-        rc = launch(m.f_frame_mega, j.blocks, SNELLY_BLOCK, args);
-      }
+      rc = launch(m.f_frame_mega, j.blocks, SNELLY_BLOCK, args);
     } else if (j.desc.mode == SNELLY_MODE_PTSIMPLE) {
       if (!m.f_ptsimple) return fail(SNELLY_EINVAL, "the simplified path tracer is not available in this module");
       rc = launch(m.f_ptsimple, j.blocks, SNELLY_BLOCK, args);

@@ -147,7 +147,7 @@ struct Context {
   // wavefront integrator (wavefront.cpp)
   int alloc_wavefront(Job& j);
   void release_wavefront(Job& j);
-  int enqueue_wavefront_frame(Job& j);
+  int enqueue_wavefront_frames(Job& j, int frames);
   int autotune(Job& j);
 };
 

@@ -2,6 +2,7 @@
 // the per-path state and queues in HBM, and the stage launches of one frame on one or more
 // concurrent streams.
 #include <algorithm>
+#include <thread>
 
 #include "runtime_internal.h"
 
@@ -66,10 +67,11 @@ void Context::release_wavefront(Job& j) {
   j.wf_parts = 0;
 }
 
-int Context::enqueue_wavefront_frame(Job& j) {
+int Context::enqueue_wavefront_frames(Job& j, int frames) {
   Module& m = *j.module;
   if (!j.wf.ptr || j.wf_parts < 1 || !m.f_wf_generate || !m.f_wf_extend || !m.f_wf_shade)
     return fail(SNELLY_EINVAL, "wavefront integrator not available for this job");
+  if (frames <= 0) return SNELLY_OK;
   const int parts = j.wf_parts;
   // streams and events, created on first use; part 0 runs on the context stream
   wf_streams[0] = stream;
@@ -97,61 +99,79 @@ int Context::enqueue_wavefront_frame(Job& j) {
     launches++;
     return SNELLY_OK;
   };
-  int rc;
-  for (int k = 0; k < parts; ++k) {
-    WfBuffers B = j.wfb[k];
-    void* gargs[] = {&jobs, &gparams, &B};
-    if ((rc = launch_on(k, m.f_wf_generate, (B.paths + SNELLY_BLOCK - 1) / SNELLY_BLOCK, gargs))) return rc;
-  }
-  // Iterations: the first `budgeted` ones park the slowest rays when their work runs out; after
-  // them every iteration advances every path by one vertex, so `nominal` more always finish the
-  // frame. Beyond the nominal count, iterations go in pairs, each followed by a read of every
-  // part's paths-left count; the host waits for the reads of the pair before last, so the GPU
-  // always has the next pair queued, and stops once they all show zero (an extra pair then finds
-  // empty queues and returns at once). Each part's launches go to its own stream in order.
+  // Per frame and part: generate, then iterations of (extend, shade). The first `budgeted`
+  // iterations park the slowest rays when their work runs out; after them every iteration
+  // advances every path by one vertex, so `nominal` more always finish the frame. Beyond the
+  // nominal count, a part's iterations go in pairs, each followed by a read of its paths-left
+  // count; a part gets its next pair once the read of the pair before last has landed, so its
+  // stream always has a pair queued, and it moves on to its next frame once a read shows zero (an
+  // extra pair then finds empty queues and returns at once). The parts are independent pixel
+  // ranges on their own streams, so a part that finishes a frame early starts the next one while
+  // the others still trace the stragglers of theirs; the host serves whichever part's read has
+  // landed and never waits on one part while another could be fed.
   const int nominal = j.scene->opts.max_bounces + 2;
   const int budgeted = wf_park_iters >= 0 ? std::min(wf_park_iters, 8 * nominal) : 3 * nominal;
   const int max_iters = budgeted + nominal;
   if (max_iters + 2 > WF_MAX_ITERS) return fail(SNELLY_EINVAL, "too many wavefront iterations for max_bounces");
   const int extend_blocks = sm_count * m.extend_blocks_per_sm, shade_blocks = sm_count * 4;
-  int it = 0;
-  auto pair = [&]() -> int {
+  struct PartRun {
+    int frame = 0, it = 0, checks = 0;
+    bool started = false;
+  } run[SNELLY_WF_MAX_PARTS];
+  auto pair = [&](int k) -> int {
+    WfBuffers B = j.wfb[k];
+    int it = run[k].it;
     int drain = it < budgeted ? wf_drain_steps : 0;
-    for (int k = 0; k < parts; ++k) {
-      WfBuffers B = j.wfb[k];
-      void* eargs[] = {&B, &it, &drain};
-      int r = launch_on(k, m.f_wf_extend, extend_blocks, eargs);
-      if (r) return r;
-      void* sargs[] = {&jobs, &gparams, &B, &it};
-      r = launch_on(k, m.f_wf_shade, shade_blocks, sargs);
-      if (r) return r;
-    }
-    ++it;
+    void* eargs[] = {&B, &it, &drain};
+    int r = launch_on(k, m.f_wf_extend, extend_blocks, eargs);
+    if (r) return r;
+    void* sargs[] = {&jobs, &gparams, &B, &it};
+    r = launch_on(k, m.f_wf_shade, shade_blocks, sargs);
+    if (r) return r;
+    ++run[k].it;
     return SNELLY_OK;
   };
-  while (it < nominal)
-    if ((rc = pair())) return rc;
-  int checks = 0;
-  while (it < max_iters) {
-    if ((rc = pair())) return rc;
-    if ((rc = pair())) return rc;
-    const int slot = checks & 1;
-    for (int k = 0; k < parts; ++k)
+  int rc, active = parts;
+  while (active > 0) {
+    bool progress = false;
+    for (int k = 0; k < parts; ++k) {
+      PartRun& R = run[k];
+      if (R.frame >= frames) continue;
+      if (!R.started) {  // the part's next frame: camera rays, then the unpolled iterations
+        WfBuffers B = j.wfb[k];
+        void* gargs[] = {&jobs, &gparams, &B};
+        if ((rc = launch_on(k, m.f_wf_generate, (B.paths + SNELLY_BLOCK - 1) / SNELLY_BLOCK, gargs))) return rc;
+        R.started = true;
+        R.it = 0;
+        R.checks = 0;
+        while (R.it < nominal)
+          if ((rc = pair(k))) return rc;
+        progress = true;
+        continue;
+      }
+      bool frame_done = R.it >= max_iters;
+      if (!frame_done && R.checks >= 2) {  // the older of the part's two outstanding reads
+        const int prev = R.checks & 1;
+        const cudaError_t q = cudaEventQuery(poll_done[prev][k]);
+        if (q == cudaErrorNotReady) continue;  // the part still has two pairs queued: serve the others
+        if (q != cudaSuccess) return fail(SNELLY_EDEVICE, std::string("wavefront progress wait failed: ") + cudaGetErrorString(q));
+        frame_done = poll_host[prev * SNELLY_WF_MAX_PARTS + k] == 0;
+      }
+      progress = true;
+      if (frame_done) {
+        R.started = false;
+        if (++R.frame >= frames) --active;
+        continue;
+      }
+      if ((rc = pair(k)) || (rc = pair(k))) return rc;
+      const int slot = R.checks & 1;
       if (cudaMemcpyAsync(poll_host + slot * SNELLY_WF_MAX_PARTS + k, j.wfb[k].cnt + WF_LEFT, sizeof(int),
                           cudaMemcpyDeviceToHost, wf_streams[k]) != cudaSuccess ||
           cudaEventRecord(poll_done[slot][k], wf_streams[k]) != cudaSuccess)
         return fail(SNELLY_EDEVICE, "wavefront progress read failed");
-    ++checks;
-    if (checks >= 2) {
-      const int prev = (checks - 2) & 1;
-      int left = 0;
-      for (int k = 0; k < parts; ++k) {
-        if (cudaEventSynchronize(poll_done[prev][k]) != cudaSuccess)
-          return fail(SNELLY_EDEVICE, "wavefront progress wait failed");
-        left += poll_host[prev * SNELLY_WF_MAX_PARTS + k];
-      }
-      if (left == 0) break;
+      ++R.checks;
     }
+    if (!progress) std::this_thread::yield();  // every part has work queued
   }
   // later work on the context stream (resolve, readback) waits for every part
   for (int k = 1; k < parts; ++k) {
@@ -194,7 +214,7 @@ int Context::autotune(Job& j) {
     for (int k = 0; k < 2 && !rc; ++k) {
       for (int f = 0; f < 3 && !rc; ++f) {
         if (f == 1) cudaEventRecord(e0, stream);
-        rc = k == 0 ? launch(j.module->f_frame_mega, j.blocks, SNELLY_BLOCK, margs) : enqueue_wavefront_frame(j);
+        rc = k == 0 ? launch(j.module->f_frame_mega, j.blocks, SNELLY_BLOCK, margs) : enqueue_wavefront_frames(j, 1);
       }
       cudaEventRecord(e1, stream);
       if (!rc && cudaEventSynchronize(e1) != cudaSuccess) rc = fail(SNELLY_EDEVICE, "autotune timing failed");
