@@ -116,17 +116,24 @@ int Context::enqueue_wavefront_frames(Job& j, int frames) {
   const int extend_blocks = sm_count * m.extend_blocks_per_sm, shade_blocks = sm_count * 4;
   struct PartRun {
     int frame = 0, it = 0, checks = 0;
+    int left = 0;  // paths of the frame not finished at the latest read (an upper bound afterwards)
     bool started = false;
   } run[SNELLY_WF_MAX_PARTS];
   auto pair = [&](int k) -> int {
     WfBuffers B = j.wfb[k];
     int it = run[k].it;
     int drain = it < budgeted ? wf_drain_steps : 0;
+    // Both stages take their work from device-side counters whatever their grid. Once a read has
+    // shown few paths left, smaller grids do the same work without launching blocks that would
+    // find nothing to do: at most 3 rays (continuation, sky and sun shadows) per unfinished path.
+    const long long left = run[k].left;
+    const int eb = (int)std::max<long long>(sm_count, std::min<long long>(extend_blocks, (3 * left + SNELLY_BLOCK - 1) / SNELLY_BLOCK));
+    const int sb = (int)std::max<long long>(sm_count, std::min<long long>(shade_blocks, (left + SNELLY_BLOCK - 1) / SNELLY_BLOCK));
     void* eargs[] = {&B, &it, &drain};
-    int r = launch_on(k, m.f_wf_extend, extend_blocks, eargs);
+    int r = launch_on(k, m.f_wf_extend, eb, eargs);
     if (r) return r;
     void* sargs[] = {&jobs, &gparams, &B, &it};
-    r = launch_on(k, m.f_wf_shade, shade_blocks, sargs);
+    r = launch_on(k, m.f_wf_shade, sb, sargs);
     if (r) return r;
     ++run[k].it;
     return SNELLY_OK;
@@ -144,6 +151,7 @@ int Context::enqueue_wavefront_frames(Job& j, int frames) {
         R.started = true;
         R.it = 0;
         R.checks = 0;
+        R.left = B.paths;
         while (R.it < nominal)
           if ((rc = pair(k))) return rc;
         progress = true;
@@ -155,7 +163,8 @@ int Context::enqueue_wavefront_frames(Job& j, int frames) {
         const cudaError_t q = cudaEventQuery(poll_done[prev][k]);
         if (q == cudaErrorNotReady) continue;  // the part still has two pairs queued: serve the others
         if (q != cudaSuccess) return fail(SNELLY_EDEVICE, std::string("wavefront progress wait failed: ") + cudaGetErrorString(q));
-        frame_done = poll_host[prev * SNELLY_WF_MAX_PARTS + k] == 0;
+        R.left = poll_host[prev * SNELLY_WF_MAX_PARTS + k];
+        frame_done = R.left == 0;
       }
       progress = true;
       if (frame_done) {
