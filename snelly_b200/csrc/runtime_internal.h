@@ -125,7 +125,7 @@ struct Context {
   std::string csrc_dir, kernel_dir, include_dir, cache_dir;
   std::vector<BatchLane> lanes;  // batch streams (created on first use)
   std::map<std::string, int> tuned;  // autotuner decisions: (module, image-size class) -> integrator
-  int wf_drain_steps = 64;           // steps an extend warp marches once its work runs out (SNELLY_WF_DRAIN)
+  int wf_drain_steps = 32;           // steps an extend warp marches once its work runs out (SNELLY_WF_DRAIN)
   int wf_park_iters = -1;            // iterations that may park rays; -1: 3 x (max_bounces + 2) (SNELLY_WF_PARK_ITERS)
   int wf_split = 3;                  // wavefront pixel ranges run concurrently (SNELLY_WF_SPLIT)
   int* poll_host = nullptr;          // pinned words the wavefront's paths-left reads land in
