@@ -7,7 +7,8 @@ optional `syncShader(snelly, shader)`, `getLengthScale()`, `getMinLengthScale()`
 `getMaxLengthScale()`, `envMap()`, `preframeCallback`, `postframeCallback`, `isReady`.
 `Snelly(scene)` then exposes the same objects (`getRenderer()`, `getCamera()`, `getControls()`,
 `getMaterials()`, ...) with the same property names, defaults and unit conventions (log10 powers,
-log-sqrt(2) aperture). Each `render()` call renders one progressive frame on the GPU.
+log-sqrt(2) aperture). `render(n)` renders n progressive frames on the GPU, each as one call of the
+reference's Renderer.render (callbacks, maxSpp and per-frame uniform changes included).
 """
 import ctypes
 import json
