@@ -124,8 +124,10 @@ def flops_per_path(host):
 
 
 def cpu_sampler(host, prefer_reference=True):
-    """A callable running `n` random pixels x 1 frame of the workload on all host cores, and its
-    kind ("reference": the reference's shader built for the CPU; "port": the oracle)."""
+    """A callable running `n` random pixels x 1 frame of the workload on every host core, its kind
+    ("reference": the reference's shader built for the CPU; "port": the oracle), and a callable
+    giving the threads the last run used. With the prebuilt reference library nothing of the
+    package's own native code is loaded: pixels are seeded by the numpy restatement."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle
     W, H = host.width, host.height
@@ -134,44 +136,52 @@ def cpu_sampler(host, prefer_reference=True):
     if prefer_reference:
         try:
             import build_ref
-            ref = build_ref.ref_for(host, name="bench_c1", prebuilt_only=not os.path.isdir(
-                os.path.join(build_ref.REF_ROOT, "shaders")))
+            ref = build_ref.ref_for(host, name="bench_c1", prebuilt_only=not build_ref.have_reference())
         except Exception:
             ref = None
-    lib = oracle.OracleLib(host.sceneObj.shader(), host.scene_opts())
     if ref is not None:
         rlib, p, tables, keep = ref
         calls = host.scene_uniforms()
 
         def run(n):
             pix = np.sort(rs.choice(W * H, n, replace=False))
-            rng0 = lib.seed(host.seed, pix)
+            rng0 = oracle.seed_pixels(host.seed, pix)
             t = time.perf_counter()
-            rlib.render(p, calls, tables, W, H, pix, 1, rng0)
+            rlib.render(p, calls, tables, W, H, pix, 1, rng0, threads=0)
             return time.perf_counter() - t
-        return run, "reference", (keep,)
+        return run, "reference", rlib.last_team, (keep,)
+    lib = oracle.OracleLib(host.sceneObj.shader(), host.scene_opts())
     p, keep = oracle.host_params(host)
     sh = host.scene_shader()
     ub = oracle.pack_uniforms(lib.cpp, sh.calls, sh.textures)
 
     def run(n):
         pix = np.sort(rs.choice(W * H, n, replace=False))
-        rng0 = lib.seed(host.seed, pix)
+        rng0 = oracle.seed_pixels(host.seed, pix)
         t = time.perf_counter()
-        lib.render(p, ub, W, H, pix, 1, rng0)
+        lib.render(p, ub, W, H, pix, 1, rng0, threads=0)
         return time.perf_counter() - t
-    return run, "port", (keep,)
+    return run, "port", lib.last_team, (keep,)
 
 
 def cpu_baseline(host, budget_s):
-    run, kind, keep = cpu_sampler(host)
+    run, kind, team, keep = cpu_sampler(host)
     t = run(2000)  # calibration
     rate = 2000 / max(t, 1e-6)
     n = int(min(host.width * host.height, max(2000, rate * budget_s)))
     dt = run(n)
-    return {"value": n / dt, "unit": "path samples/s", "cores": os.cpu_count(), "kind": kind,
+    cores = team()
+    return {"value": n / dt, "unit": "path samples/s", "cores": cores, "kind": kind,
             "sample": f"{n} random pixels of the {host.width}x{host.height} workload, 1 frame each "
-                      f"({dt:.1f} s on {os.cpu_count()} host threads)"}
+                      f"({dt:.1f} s on {cores} host threads of {os.cpu_count()})"}
+
+
+def workload_config(args, width, height):
+    """The workload's definition, printed identically by both arms."""
+    return {"workload": WORKLOAD, "width": width, "height": height, "spp_per_step": max(1, args.spp_per_step),
+            "image_spp": 64, "max_bounces": 8, "max_march_steps": 512, "dispersive": True,
+            "l2": "flushed between timed steps (256 MiB write); path state 0.7 GB > L2",
+            "parallelism": f"replicas x{args.gpus}"}
 
 
 def traffic_from_profiles(kernel_name):
@@ -195,22 +205,26 @@ def reference_arm(args, rank):
         return
     from snelly_b200.testing import HostSnelly
     host = HostSnelly(workload_scene(args))
-    run, kind, keep = cpu_sampler(host)
+    run, kind, team, keep = cpu_sampler(host)
     t = run(1000)
     per_step = int(min(host.width * host.height, max(1000, (1000 / max(t, 1e-6)) * args.cpu_seconds / max(1, args.steps))))
     for _ in range(args.warmup):
         run(min(per_step, 2000))
     times = [run(per_step) for _ in range(args.steps)]
     value = per_step * args.steps / sum(times)
+    cores = team()
     sample = (f"{per_step} random pixels x 1 frame per step of the {host.width}x{host.height} workload "
-              f"(a bounded sample of its {args.spp_per_step}-frame step)")
+              f"(a bounded sample of its {args.spp_per_step}-frame step; {cores} host threads of {os.cpu_count()})")
+    native = [l.split()[-1] for l in open("/proc/self/maps") if "libsnelly" in l] if os.path.exists("/proc/self/maps") else []
     out = {"impl": "reference", "metric": METRIC, "value": value, "unit": "path samples/s", "n_gpus": args.gpus,
            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * sum(times) / args.steps,
            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-           "data": "synthetic (procedural SDF scene, seeded camera)",
-           "config": {"workload": WORKLOAD, "width": host.width, "height": host.height,
-                      "spp_per_step": args.spp_per_step, "device": "host CPU"},
-           "cpu_baseline": {"value": value, "unit": "path samples/s", "cores": os.cpu_count(), "kind": kind,
+           "data": "synthetic (procedural SDF scene, seeded camera; no dataset)",
+           "config": workload_config(args, host.width, host.height),
+           "impl_detail": {"device": "host CPU", "program": "the reference's path tracer shader built for the CPU"
+                           if kind == "reference" else "the oracle's restatement of the path tracer",
+                           "package_native_code_loaded": sorted(set(native))},
+           "cpu_baseline": {"value": value, "unit": "path samples/s", "cores": cores, "kind": kind,
                             "sample": sample},
            "e2e": {"value": value, "unit": "path samples/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(out), flush=True)
@@ -310,10 +324,8 @@ def gpu_arm(args, rank, world, local_rank):
             "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic (procedural SDF scene, seeded camera; no dataset)",
-            "config": {"workload": WORKLOAD, "width": W, "height": H, "spp_per_step": fps, "image_spp": 64,
-                       "max_bounces": 8, "max_march_steps": 512, "dispersive": True,
-                       "kernel": kernel_used, "kernel_choice": args.kernel, "math": "fast",
-                       "l2": "flushed between timed steps (256 MiB write)", "parallelism": f"replicas x{world}"},
+            "config": workload_config(args, W, H),
+            "impl_detail": {"device": "B200", "kernel": kernel_used, "kernel_choice": args.kernel, "math": "fast"},
             "e2e": {"value": e2e_value, "unit": "path samples/s", "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": W * H * 16},
             "gpu_launches": int(launches),

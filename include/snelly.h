@@ -238,8 +238,10 @@ int snelly_inverse_cdf(const snelly_spectrum* s, float* out);
  * not call cudaFree, which synchronises the whole device. Its scratch is a fixed 160 KiB of
  * file-scope device memory per device (4096 partial records), so it handles jobs of at most
  * 4096 x 2048 = 8,388,608 pixels and returns SNELLY_EINVAL, naming the limit, for larger ones.
- * The first call on a device looks up the scratch address (cudaGetSymbolAddress, with that device
- * made current for the lookup); make that first call before any stream capture. The scratch is
+ * The first call through a context looks up the scratch address (cudaGetSymbolAddress, with the
+ * context's device made current for the lookup) and keeps it with the context; make that first
+ * call before any stream capture. After a device reset every context on that device is invalid,
+ * this address included: create a new context, whose first call looks it up again. The scratch is
  * shared by every context and thread of the process on that device, so overlapping calls race;
  * calls through one context are serialised by the context. It clears its completion counter
  * before each launch and allocates nothing (no cudaMalloc, cudaFree or allocating library call). */

@@ -29,7 +29,12 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
-REF_ROOT = os.environ.get("SNELLY_REFERENCE", "/root/reference")
+REF_ROOT = os.environ.get("SNELLY_REFERENCE", "")  # the reference checkout; unset: prebuilt libraries only
+
+
+def have_reference():
+    """True when $SNELLY_REFERENCE names a checkout of the reference (its shaders/ folder)."""
+    return bool(REF_ROOT) and os.path.isdir(os.path.join(REF_ROOT, "shaders"))
 OUT = os.path.join(HERE, "_ref")
 sys.path.insert(0, HERE)
 sys.path.insert(0, ROOT)
@@ -219,6 +224,7 @@ class RefLib:
             L.ref_render.argtypes = [vp, sz, sz, sz, i32, i32, vp, i32, i32, vp, vp, i32]
             L.ref_render.restype = i32
         L.ref_block_size.restype = sz
+        L.ref_last_team.restype = i32
         self.lib = L
         self.layout, self.size = self._layout(cpp)
 
@@ -266,6 +272,10 @@ class RefLib:
                 off = self.layout[name][1]
                 buf[off:off + 32] = O.sampler_record(self.layout[name][0], arr, linear)
         return bytes(buf)
+
+    def last_team(self):
+        """Threads the last render / pick call ran on."""
+        return int(self.lib.ref_last_team())
 
     def pick(self, params, scene_calls, tables, width, pixels, threads=0, scene_textures=None):
         """The pick program at the centre of each listed pixel: (n, 2) distance and material."""
@@ -333,7 +343,7 @@ def ref_for(snelly, name=None, prebuilt_only=False, program="pathtracer"):
     args = (snelly.sceneObj.shader(), snelly.scene_opts(), p.dieleModel, p.dieleNumCoeffs)
     lib = RefLib.load(name, *args, program=program) if name else None
     if lib is None:
-        if prebuilt_only or not os.path.isdir(os.path.join(REF_ROOT, "shaders")):
+        if prebuilt_only or not have_reference():
             return None
         lib = RefLib(*args, name=name, program=program)
     return lib, p, tables, (xyz, icdf, metal_n, metal_k, env)

@@ -201,6 +201,7 @@ class OracleLib:
         L.oracle_rand.restype = ctypes.c_float
         L.oracle_uniform_block_size.restype = ctypes.c_size_t
         L.oracle_counts.argtypes = [vp, vp]
+        L.oracle_last_team.restype = i32
         self.lib = L
 
     def counts(self):
@@ -231,6 +232,10 @@ class OracleLib:
         for k, p in enumerate(pixels):
             self.lib.oracle_seed(seed, int(p), out[k].ctypes.data)
         return out
+
+    def last_team(self):
+        """Threads the last render / firsthit call ran on."""
+        return int(self.lib.oracle_last_team())
 
     def render(self, params, uniforms, width, height, pixels, frames, rng, threads=0):
         """Render `frames` frames of the listed pixels. Returns (xyz_sum float64 (n,3),
@@ -271,6 +276,37 @@ class OracleLib:
         p = np.asarray(params, np.float32)
         assert self.lib.oracle_tonemap(a.ctypes.data, len(a), p.ctypes.data, out.ctypes.data) == 0
         return out
+
+
+_RNG_MODULI = np.array([4194287, 4194277, 4194191, 4194167], np.uint64)
+
+
+def seed_pixels(seed, pixels):
+    """The per-pixel RNG seeding of the CUDA path tracer (oracle_seed, restated in numpy so that
+    a process can seed without loading any compiled library): lane k of pixel i is
+    1 + (z_k mod (m_k - 1)) for successive SplitMix64 outputs z_k of the stream keyed by
+    splitmix64(seed) ^ i. Returns (n, 4) uint32."""
+    M = (1 << 64) - 1
+
+    def nxt(s):
+        s = (s + 0x9E3779B97F4A7C15) & M
+        z = s
+        z = ((z ^ (z >> 30)) * 0xBF58476D1CE4E5B9) & M
+        z = ((z ^ (z >> 27)) * 0x94D049BB133111EB) & M
+        return s, z ^ (z >> 31)
+
+    _, k0 = nxt(int(seed) & M)
+    with np.errstate(over="ignore"):
+        key = np.uint64(k0) ^ np.asarray(pixels, np.uint64)
+        out = np.empty((len(key), 4), np.uint32)
+        for lane in range(4):
+            key = key + np.uint64(0x9E3779B97F4A7C15)
+            z = key.copy()
+            z = (z ^ (z >> np.uint64(30))) * np.uint64(0xBF58476D1CE4E5B9)
+            z = (z ^ (z >> np.uint64(27))) * np.uint64(0x94D049BB133111EB)
+            z = z ^ (z >> np.uint64(31))
+            out[:, lane] = (np.uint64(1) + z % (_RNG_MODULI[lane] - np.uint64(1))).astype(np.uint32)
+    return out
 
 
 def host_params(snelly):

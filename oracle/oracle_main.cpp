@@ -31,9 +31,26 @@ uint64_t splitmix_next(uint64_t& s) {
   return z ^ (z >> 31);
 }
 
+// Threads of one render call: `threads` if positive, else every processor. Given as the
+// parallel region's num_threads clause, so that no call changes the process-wide OpenMP setting
+// that other libraries in the process (the reference build, torch) read.
+int team_size(int threads) {
+#ifdef _OPENMP
+  return threads > 0 ? threads : omp_get_num_procs();
+#else
+  (void)threads;
+  return 1;
+#endif
+}
+
+int g_last_team = 0;  // threads the last render call ran on
+
 }  // namespace
 
 extern "C" {
+
+// Threads the last oracle_render / oracle_firsthit call ran on.
+int oracle_last_team(void) { return g_last_team; }
 
 void oracle_seed(uint64_t seed, uint64_t pixel, uint32_t* out4) {
   static const uint32_t m[4] = {4194287u, 4194277u, 4194191u, 4194167u};
@@ -81,10 +98,15 @@ int oracle_render(const SnellyParams* P, const void* uniforms, int width, int he
                   int frames, uint32_t* rng, double* xyz_sum, float* mean, int threads) {
   (void)height;
   const glsl::SceneUniforms& U = *reinterpret_cast<const glsl::SceneUniforms*>(uniforms);
+  const int nt = team_size(threads);
+  g_last_team = 1;
+#pragma omp parallel num_threads(nt)
+  {
 #ifdef _OPENMP
-  if (threads > 0) omp_set_num_threads(threads);
-#pragma omp parallel for schedule(dynamic, 16)
+#pragma omp single nowait
+    g_last_team = omp_get_num_threads();
 #endif
+#pragma omp for schedule(dynamic, 16)
   for (int k = 0; k < n; ++k) {
     int idx = pixels[k];
     int x = idx % width, y = idx / width;
@@ -109,6 +131,7 @@ int oracle_render(const SnellyParams* P, const void* uniforms, int width, int he
     rng[4 * k + 2] = (uint32_t)glsl::s_tofloat(rnd.z);
     rng[4 * k + 3] = (uint32_t)glsl::s_tofloat(rnd.w);
   }
+  }  // omp parallel
   return 0;
 }
 
@@ -121,10 +144,15 @@ int oracle_firsthit(const SnellyParams* P, const void* uniforms, int mode, int w
   (void)height;
   if (mode < 1 || mode > 4) return -1;
   const glsl::SceneUniforms& U = *reinterpret_cast<const glsl::SceneUniforms*>(uniforms);
+  const int nt = team_size(threads);
+  g_last_team = 1;
+#pragma omp parallel num_threads(nt)
+  {
 #ifdef _OPENMP
-  if (threads > 0) omp_set_num_threads(threads);
-#pragma omp parallel for schedule(dynamic, 16)
+#pragma omp single nowait
+    g_last_team = omp_get_num_threads();
 #endif
+#pragma omp for schedule(dynamic, 16)
   for (int k = 0; k < n; ++k) {
     int idx = pixels[k];
     int x = idx % width, y = idx / width;
@@ -172,6 +200,7 @@ int oracle_firsthit(const SnellyParams* P, const void* uniforms, int mode, int w
     rng[4 * k + 2] = (uint32_t)glsl::s_tofloat(rnd.z);
     rng[4 * k + 3] = (uint32_t)glsl::s_tofloat(rnd.w);
   }
+  }  // omp parallel
   return 0;
 }
 

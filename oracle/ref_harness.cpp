@@ -17,6 +17,23 @@ namespace glsl {
 
 extern "C" size_t ref_block_size(void) { return sizeof(glsl::RefShaderUniforms); }
 
+namespace {
+// Threads of one call: `threads` if positive, else every processor, given as the parallel
+// region's num_threads clause so that no call changes the process-wide OpenMP setting.
+int team_size(int threads) {
+#ifdef _OPENMP
+  return threads > 0 ? threads : omp_get_num_procs();
+#else
+  (void)threads;
+  return 1;
+#endif
+}
+int g_last_team = 0;
+}  // namespace
+
+// Threads the last ref_render / ref_pick call ran on.
+extern "C" int ref_last_team(void) { return g_last_team; }
+
 #ifdef REF_TONEMAP
 // The tonemapper program (built with -DREF_TONEMAP): the Radiance texture bound to each input
 // texel in turn (1x1 NEAREST); out: g_outputColor per texel.
@@ -44,11 +61,14 @@ extern "C" int ref_tonemap(const void* block, size_t block_bytes, size_t off_rad
 extern "C" int ref_pick(const void* block, size_t block_bytes, size_t off_mouse, int width, const int* pixels, int n,
                         float* out, int threads) {
   if (block_bytes != sizeof(glsl::RefShaderUniforms)) return -1;
-#ifdef _OPENMP
-  if (threads > 0) omp_set_num_threads(threads);
-#endif
-#pragma omp parallel
+  const int nt = team_size(threads);
+  g_last_team = 1;
+#pragma omp parallel num_threads(nt)
   {
+#ifdef _OPENMP
+#pragma omp single nowait
+    g_last_team = omp_get_num_threads();
+#endif
     std::vector<unsigned char> local(block_bytes + 16);
     unsigned char* lb = local.data();
 #pragma omp for schedule(dynamic, 16)
@@ -75,11 +95,14 @@ extern "C" int ref_render(const void* block, size_t block_bytes, size_t off_radi
                           int height, const int* pixels, int n, int frames, uint32_t* rng, float* mean, int threads) {
   (void)height;
   if (block_bytes != sizeof(glsl::RefShaderUniforms)) return -1;
-#ifdef _OPENMP
-  if (threads > 0) omp_set_num_threads(threads);
-#endif
-#pragma omp parallel
+  const int nt = team_size(threads);
+  g_last_team = 1;
+#pragma omp parallel num_threads(nt)
   {
+#ifdef _OPENMP
+#pragma omp single nowait
+    g_last_team = omp_get_num_threads();
+#endif
     std::vector<unsigned char> local(block_bytes + 16);
     unsigned char* lb = local.data();
     float rad[4], st[4];

@@ -248,10 +248,6 @@ int snelly_selftest(snelly_ctx* ctx, int which, uint64_t* mismatches) {
   return SNELLY_OK;
 }
 
-// Device address of g_static_stats_scratch per device, looked up once (with that device current).
-static std::mutex g_static_scratch_mu;
-static StaticStatsScratch* g_static_scratch_ptr[64];
-
 int snelly_image_stats_static(snelly_ctx* ctx, uint64_t job_id, double* out5) {
   if (!ctx || !out5) return snelly::fail(SNELLY_EINVAL, "null argument to snelly_image_stats_static");
   snelly::Context& c = *ctx->c;
@@ -264,24 +260,22 @@ int snelly_image_stats_static(snelly_ctx* ctx, uint64_t job_id, double* out5) {
     return snelly::fail(SNELLY_EINVAL, "snelly_image_stats_static handles at most " + std::to_string(kStaticStatsMaxPixels) +
                                            " pixels (its fixed scratch has " + std::to_string(kStaticStatsMaxBlocks) +
                                            " partial records); this job has " + std::to_string(npix));
-  if (c.device < 0 || c.device >= 64) return snelly::fail(SNELLY_EINVAL, "device index out of range");
-  StaticStatsScratch* scratch = nullptr;
-  {
-    std::lock_guard<std::mutex> g(g_static_scratch_mu);
-    if (!g_static_scratch_ptr[c.device]) {
-      int prev = -1;
-      cudaError_t e = cudaGetDevice(&prev);
-      if (e == cudaSuccess && prev != c.device) e = cudaSetDevice(c.device);
-      void* p = nullptr;
-      if (e == cudaSuccess) e = cudaGetSymbolAddress(&p, g_static_stats_scratch);
-      if (prev >= 0 && prev != c.device) cudaSetDevice(prev);
-      if (e != cudaSuccess || !p)
-        return snelly::fail(SNELLY_EDEVICE, std::string("cudaGetSymbolAddress of the statistics scratch: ") +
-                                                cudaGetErrorString(e));
-      g_static_scratch_ptr[c.device] = (StaticStatsScratch*)p;
-    }
-    scratch = g_static_scratch_ptr[c.device];
+  // The device address of the file-scope scratch, looked up at the context's first call (with the
+  // context's device current) and kept with the context: a context created after a device reset
+  // looks it up again.
+  if (!c.static_stats_scratch) {
+    int prev = -1;
+    cudaError_t e = cudaGetDevice(&prev);
+    if (e == cudaSuccess && prev != c.device) e = cudaSetDevice(c.device);
+    void* p = nullptr;
+    if (e == cudaSuccess) e = cudaGetSymbolAddress(&p, g_static_stats_scratch);
+    if (prev >= 0 && prev != c.device) cudaSetDevice(prev);
+    if (e != cudaSuccess || !p)
+      return snelly::fail(SNELLY_EDEVICE, std::string("cudaGetSymbolAddress of the statistics scratch: ") +
+                                              cudaGetErrorString(e));
+    c.static_stats_scratch = p;
   }
+  StaticStatsScratch* scratch = (StaticStatsScratch*)c.static_stats_scratch;
   const int blocks = (int)std::max<long long>(1, (npix + kStaticStatsPixelsPerBlock - 1) / kStaticStatsPixelsPerBlock);
   cudaError_t e = cudaMemsetAsync(&scratch->done_blocks, 0, sizeof(unsigned int), c.stream);
   if (e == cudaSuccess) {
@@ -299,15 +293,21 @@ int snelly_image_stats_static(snelly_ctx* ctx, uint64_t job_id, double* out5) {
 int snelly_flush_l2(snelly_ctx* ctx, size_t bytes) {
   if (!ctx) return snelly::fail(SNELLY_EINVAL, "null argument");
   snelly::Context& c = *ctx->c;
-  static thread_local void* buf = nullptr;
-  static thread_local size_t have = 0;
-  if (have < bytes) {
-    if (buf) cudaFree(buf);
-    buf = nullptr;
-    if (cudaMalloc(&buf, bytes) != cudaSuccess) return snelly::fail(SNELLY_EDEVICE, "cudaMalloc failed");
-    have = bytes;
+  std::lock_guard<std::mutex> lk(c.mu);
+  if (c.flush_bytes < bytes) {  // the context's buffer, grown on demand and freed with the context
+    if (c.flush_buf) {
+      cudaStreamSynchronize(c.stream);
+      cudaFree(c.flush_buf);
+    }
+    c.flush_buf = nullptr;
+    c.flush_bytes = 0;
+    if (cudaMalloc(&c.flush_buf, bytes) != cudaSuccess) {
+      c.flush_buf = nullptr;
+      return snelly::fail(SNELLY_EDEVICE, "cudaMalloc failed");
+    }
+    c.flush_bytes = bytes;
   }
-  l2_flush_kernel<<<c.sm_count * 4, 256, 0, c.stream>>>((float4*)buf, bytes / 16, 0.0f);
+  l2_flush_kernel<<<c.sm_count * 4, 256, 0, c.stream>>>((float4*)c.flush_buf, bytes / 16, 0.0f);
   c.launches += 1;
   if (cudaGetLastError() != cudaSuccess) return snelly::fail(SNELLY_EDEVICE, "flush launch failed");
   return SNELLY_OK;

@@ -68,7 +68,8 @@ typedef struct WfBuffers {
   int* qa[2];       // active-path queues (continuation rays)
   int* qs[2];       // shadow-ray queues (path * 2 + light)
   int* qc[2];       // parked-ray queues (ray ids: 2 * path + light, or 2 * paths + path)
-  int* qshade;      // shade queue, 4 segments of `paths` entries: finish/miss, surface, metal, dielectric
+  int* qshade[2];   // shade queues [2] (ping-pong by iteration parity), 4 segments of `paths`
+                    // entries each: finish/miss, surface, metal, dielectric
   int* cnt;         // counters (WF_*)
   int paths;
   int pixel_begin;

@@ -311,7 +311,7 @@ extern "C" __global__ void __launch_bounds__(SNELLY_BLOCK) snelly_wf_extend(WfBu
       }
       for (int sgi = 0; sgi < 4; ++sgi) {
         int slot = warp_append(qcnt + sgi, seg == sgi);
-        if (slot >= 0) B.qshade[sgi * B.paths + slot] = path;
+        if (slot >= 0) B.qshade[cur][sgi * B.paths + slot] = path;
       }
       const int r = sidx >= 0 ? sidx : P2 + path;
       if (park) B.mt[r] = make_float4(t, sgn, __int_as_float(n), 0.0f);
@@ -348,7 +348,7 @@ extern "C" __global__ void __launch_bounds__(SNELLY_BLOCK, SNELLY_SHADE_MIN_BLOC
     if (valid) {
       int seg = w < n0 ? 0 : (w < n0 + n1 ? 1 : (w < n0 + n1 + n2 ? 2 : 3));
       int off = w - (seg == 0 ? 0 : (seg == 1 ? n0 : (seg == 2 ? n0 + n1 : n0 + n1 + n2)));
-      path = B.qshade[seg * B.paths + off];
+      path = B.qshade[cur][seg * B.paths + off];
       int4 info = B.info[path];
       float4 cm = B.cmf[path];
       Ctx c{P, gparams, sc, 0, cm.w, ld3(cm), make_frame(v3(P.sunDir))};
@@ -446,8 +446,10 @@ extern "C" __global__ void __launch_bounds__(SNELLY_BLOCK, SNELLY_SHADE_MIN_BLOC
       int ss = warp_append(cnt + WF_S + nxt, (push_shadow >> l) & 1);
       if (ss >= 0) B.qs[nxt][ss] = 2 * path + l;
     }
+    // a path with no ray to wait for goes straight to the next shade stage's queue (the other
+    // buffer: this launch is still reading its own)
     int ds = warp_append(cnt + WF_Q + 4 * nxt, push_direct);
-    if (ds >= 0) B.qshade[ds] = path;
+    if (ds >= 0) B.qshade[nxt][ds] = path;
     unsigned fin = __ballot_sync(WF_FULL, finished);
     if (fin && (int)(threadIdx.x & 31) == __ffs(fin) - 1) atomicSub(cnt + WF_LEFT, __popc(fin));
   }

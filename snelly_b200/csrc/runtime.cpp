@@ -4,11 +4,13 @@
 // module cache (one module per scene source + compile-time options), scenes, jobs and their
 // device buffers, and an HBM budget that every allocation is checked against.
 #include <cuda_runtime.h>
+#include <dirent.h>
 #include <dlfcn.h>
 #include <nvrtc.h>
 #include <sys/stat.h>
 #include <unistd.h>
 
+#include <algorithm>
 #include <atomic>
 #include <cstdio>
 #include <cstring>
@@ -241,11 +243,21 @@ int Context::compile_module(const std::string& src, int math_mode, std::shared_p
   std::vector<std::string> opts = nvrtc_options(kernel_dir, csrc_dir, include_dir, math_mode);
   std::string key_text = src;
   for (auto& o : opts) key_text += "\n" + o;
-  // the kernel sources are part of the cache key
-  for (const char* f : {"pt_kernels.cu", "pt_integrator.cuh", "pt_device.cuh", "pt_wavefront.cuh", "pt_firsthit.cuh",
-                        "pt_launch.h"})
-    key_text += read_file(kernel_dir + "/" + f);
-  key_text += read_file(csrc_dir + "/glslcompat.h") + read_file(include_dir + "/snelly_params.h");
+  // the cache key covers every source the program includes (all of the kernel directory, the
+  // GLSL compatibility header and its swizzle table, the parameter block) and the compiler version
+  std::vector<std::string> kfiles;
+  if (DIR* d = opendir(kernel_dir.c_str())) {
+    while (dirent* e = readdir(d))
+      if (e->d_name[0] != '.') kfiles.push_back(e->d_name);
+    closedir(d);
+  }
+  std::sort(kfiles.begin(), kfiles.end());
+  for (auto& f : kfiles) key_text += "\n//" + f + "\n" + read_file(kernel_dir + "/" + f);
+  key_text += read_file(csrc_dir + "/glslcompat.h") + read_file(csrc_dir + "/glsl_swizzles.inc") +
+              read_file(include_dir + "/snelly_params.h");
+  int nv_major = 0, nv_minor = 0;
+  nvrtcVersion(&nv_major, &nv_minor);
+  key_text += "\nnvrtc " + std::to_string(nv_major) + "." + std::to_string(nv_minor);
   std::string key = hex64(fnv1a(key_text));
   auto it = module_cache.find(key);
   if (it != module_cache.end()) {
@@ -254,24 +266,36 @@ int Context::compile_module(const std::string& src, int math_mode, std::shared_p
   }
   std::vector<char> cubin;
   std::string cache_path = cache_dir.empty() ? "" : cache_dir + "/" + key + ".cubin";
+  bool from_cache = false;
   if (!cache_path.empty() && file_exists(cache_path)) {
     std::ifstream in(cache_path, std::ios::binary);
     cubin.assign(std::istreambuf_iterator<char>(in), std::istreambuf_iterator<char>());
-  }
-  if (cubin.empty()) {
-    int rc = nvrtc_cubin(src, opts, &cubin, log);
-    if (rc) return rc;
-    if (!cache_path.empty()) {
-      std::string tmp = cache_path + ".tmp" + std::to_string((long)getpid());
-      std::ofstream o(tmp, std::ios::binary);
-      o.write(cubin.data(), (std::streamsize)cubin.size());
-      o.close();
-      rename(tmp.c_str(), cache_path.c_str());
-    }
+    from_cache = !cubin.empty();
   }
   auto m = std::make_shared<Module>();
   m->key = key;
-  RT_TRY(cudaLibraryLoadData(&m->lib, cubin.data(), nullptr, nullptr, 0, nullptr, nullptr, 0));
+  for (int attempt = 0;; ++attempt) {
+    if (cubin.empty()) {
+      int rc = nvrtc_cubin(src, opts, &cubin, log);
+      if (rc) return rc;
+      from_cache = false;
+      if (!cache_path.empty()) {  // written whole to a temporary file, then renamed into place
+        std::string tmp = cache_path + ".tmp" + std::to_string((long)getpid());
+        std::ofstream o(tmp, std::ios::binary);
+        o.write(cubin.data(), (std::streamsize)cubin.size());
+        o.close();
+        if (o.good()) rename(tmp.c_str(), cache_path.c_str());
+        else unlink(tmp.c_str());
+      }
+    }
+    cudaError_t lr = cudaLibraryLoadData(&m->lib, cubin.data(), nullptr, nullptr, 0, nullptr, nullptr, 0);
+    if (lr == cudaSuccess) break;
+    cudaGetLastError();
+    if (!from_cache || attempt > 0)
+      return fail(SNELLY_EDEVICE, std::string("cudaLibraryLoadData: ") + cudaGetErrorString(lr));
+    unlink(cache_path.c_str());  // an unusable cached cubin (truncated, or from another build): compile again
+    cubin.clear();
+  }
   struct Fn {
     const char* name;
     cudaKernel_t* f;
@@ -509,6 +533,7 @@ Context::~Context() {
   if (copy_stream) cudaStreamSynchronize(copy_stream);
   release(xyz);
   release(stats_scratch);
+  if (flush_buf) cudaFree(flush_buf);
   if (poll_host) cudaFreeHost(poll_host);
   for (auto& row : poll_done)
     for (auto& e : row)

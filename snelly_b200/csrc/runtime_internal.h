@@ -133,6 +133,9 @@ struct Context {
   cudaStream_t wf_streams[SNELLY_WF_MAX_PARTS] = {};  // [0] is the context stream
   cudaEvent_t wf_fork = nullptr, wf_join[SNELLY_WF_MAX_PARTS] = {};
   DevBuf stats_scratch;          // image-statistics partial sums
+  void* static_stats_scratch = nullptr;  // device address of the allocation-free statistics scratch
+  void* flush_buf = nullptr;     // L2 eviction buffer of snelly_flush_l2 (freed with the context)
+  size_t flush_bytes = 0;
 
   ~Context();
   int alloc(DevBuf& b, size_t bytes);

@@ -18,9 +18,9 @@ int Context::alloc_wavefront(Job& j) {
   int parts = std::max(1, std::min(wf_split, SNELLY_WF_MAX_PARTS));
   if (P < (size_t)parts * 65536) parts = 1;  // small images: one part keeps each launch full
   // per path: 17 float4 arrays + info + rng + parked-ray state (3 per path), shadow flags, pending
-  // count, int queues (2 active, 2 x 2 shadow, 2 x 3 parked, 4 shade); per part: counters and
-  // the 256-byte alignment of its 30 sub-buffers
-  size_t bytes = (19 * 16 + 3 * 16 + 2 + 4 + (2 + 2 * 2 + 2 * 3 + 4) * 4) * P +
+  // count, int queues (2 active, 2 x 2 shadow, 2 x 3 parked, 2 x 4 shade); per part: counters
+  // and the 256-byte alignment of its 31 sub-buffers
+  size_t bytes = (19 * 16 + 3 * 16 + 2 + 4 + (2 + 2 * 2 + 2 * 3 + 2 * 4) * 4) * P +
                  (size_t)parts * (4 * WF_COUNTERS + 32 * 256);
   int rc = alloc(j.wf, bytes);
   if (rc) return rc;
@@ -49,7 +49,8 @@ int Context::alloc_wavefront(Job& j) {
     B.qa[1] = (int*)take(4 * Pk);
     B.qs[0] = (int*)take(8 * Pk);
     B.qs[1] = (int*)take(8 * Pk);
-    B.qshade = (int*)take(16 * Pk);
+    B.qshade[0] = (int*)take(16 * Pk);
+    B.qshade[1] = (int*)take(16 * Pk);
     B.cnt = (int*)take(4 * WF_COUNTERS);
     B.shadow = (unsigned char*)take(2 * Pk);
     B.paths = (int)Pk;

@@ -62,7 +62,9 @@ def extract(ref):
 
 
 def main():
-    ref = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    ref = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("SNELLY_REFERENCE", "")
+    if not ref:
+        sys.exit("usage: extract_tables.py <reference checkout> (or set $SNELLY_REFERENCE)")
     xyz, metals, registered, dielectrics = extract(ref)
     out = {
         "source": "portsmouth/snelly js/color.js, js/materials.js",

@@ -66,6 +66,29 @@ float SDF_SURFACE(vec3 X)
         return 1.0e-4
 
 
+class LowSunNoSky(PlainSphere):
+    """C0's sphere and ground under a low sun (latitude 8 degrees) and no sky, maxBounces 2:
+    surface vertices that face away from the sun sample no light at all, so a path whose last
+    vertex is one of them finishes with no shadow ray to trace."""
+
+    def __init__(self, width=None, height=None, sun_latitude=8.0):
+        super().__init__(width, height)
+        self.sun_latitude = sun_latitude
+
+    def init(self, snelly):
+        super().init(snelly)
+        r = snelly.getRenderer()
+        r.maxBounces = 2
+        r.skyPower = -7.0         # off
+        r.sunPower = math.log10(20.0)
+        r.sunAngularSize = 3.0
+        r.sunLatitude = self.sun_latitude
+        r.sunLongitude = 120.0
+
+    def after_init(self, snelly):
+        pass
+
+
 def c1_camera(seed=2):
     """Camera pose of C1 drawn from `seed`: a point at distance U(4.5, 6) from the look-at point
     (0.6, 0, 0), azimuth U(60, 120) degrees about +y from the +x axis (so the sponge and the gold
@@ -671,4 +694,5 @@ float SDF_SURFACE(vec3 X)
 
 
 SCENES = {"c0": PlainSphere, "c1": DispersiveFractal, "c2": VolumetricSubsurface, "atmosphere": AtmosphereLights,
-          "hooks": HooksAndMaps, "mesh": MeshLike, "envmap": EnvMapLit, "turntable": Turntable}
+          "hooks": HooksAndMaps, "mesh": MeshLike, "envmap": EnvMapLit, "turntable": Turntable,
+          "lowsun": LowSunNoSky}

@@ -1,7 +1,7 @@
 """Generate the golden fixtures of tests/golden/ from the reference itself.
 
-Run in a checkout that has the reference at /root/reference (or $SNELLY_REFERENCE):
-    python tests/golden/make_golden.py
+Run with $SNELLY_REFERENCE naming a checkout of the reference:
+    SNELLY_REFERENCE=<checkout> python tests/golden/make_golden.py
 
 * pt_<case>.npz: the reference's own path tracer shader (shaders/pathtracer-fragment-shader.glsl,
   built for the CPU by oracle/build_ref.py) rendering a small image of one of the package's
@@ -131,6 +131,7 @@ def make_tonemap():
 
 
 def make_cie():
+    assert build_ref.have_reference(), "set $SNELLY_REFERENCE to a checkout of the reference"
     path = os.path.join(build_ref.REF_ROOT, "scripts", "color", "lin2012xyz2e_fine_7sf.csv")
     rows = [r for r in csv.reader(open(path))]
     lam = np.array([float(r[0]) for r in rows])
@@ -142,6 +143,8 @@ def make_cie():
 
 
 if __name__ == "__main__":
+    if not build_ref.have_reference():
+        sys.exit("set $SNELLY_REFERENCE to a checkout of the reference")
     only = sys.argv[1:]
     if not only or "cie" in only:
         make_cie()
