@@ -15,6 +15,11 @@ host memory, which overlaps the next step's frame), wall clock until every image
 `--impl reference` times the reference's own shader built for the host CPU
 (oracle/_ref, else the oracle port) on a bounded pixel sample per step, all host threads.
 
+`latency` (rank 0): the metric's second half, batched vs plain: the first --latency-jobs render
+jobs of the heterogeneous batch draw (seed 4: 128^2..1024^2, four scenes, 4..64 spp), rendered
+one after another through the single-job path and then all at once in batched launches, with
+path samples/s and p50/p99 time to target spp (every job submitted at t = 0) for both.
+
 Multi-GPU: replicas (one job per GPU, no collective): `value` sums all ranks' samples over the
 slowest rank's time.
 """
@@ -52,6 +57,9 @@ def parse():
     ap.add_argument("--height", type=int, default=1080)
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="budget of the CPU baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--latency-jobs", type=int, default=32,
+                    help="jobs of the heterogeneous batch draw (seed 4) for the batched-vs-plain latency block "
+                         "(0: skip it)")
     return ap.parse_args()
 
 
@@ -263,6 +271,7 @@ def gpu_arm(args, rank, world, local_rank):
     s.pathtracer.kernelMode = {"auto": N.KERNEL_AUTO, "mega": N.KERNEL_MEGA, "wavefront": N.KERNEL_WAVEFRONT}[args.kernel]
     s.render(0)  # compile, allocate, seed (and, for --kernel auto, the autotuner's trial frames)
     kernel_used = "wavefront" if ctx.job_kernel(s.job_id()) == N.KERNEL_WAVEFRONT else "mega"
+    wf_config = ctx.job_wavefront_config(s.job_id()) if kernel_used == "wavefront" else None
     W, H = s.width, s.height
     fps = max(1, args.spp_per_step)
     samples_per_step = W * H * int(round(s.pathtracer.maxSamplesPerFrame)) * fps
@@ -310,6 +319,12 @@ def gpu_arm(args, rank, world, local_rank):
     e2e_value = world * samples_per_step * args.steps / e2e_s
     assert all(np.isfinite(p).all() for p in pinned)
 
+    latency = None
+    if rank == 0 and args.latency_jobs > 0:
+        from snelly_b200 import batchbench
+        jobs = batchbench.job_set(args.latency_jobs, 4)
+        latency = {"workload": f"the first {args.latency_jobs} jobs of the heterogeneous batch draw (seed 4)"}
+        latency.update(batchbench.measure(ctx, jobs))
     if rank == 0:
         from snelly_b200.testing import HostSnelly
         host = HostSnelly(workload_scene(args))
@@ -325,7 +340,8 @@ def gpu_arm(args, rank, world, local_rank):
             "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic (procedural SDF scene, seeded camera; no dataset)",
             "config": workload_config(args, W, H),
-            "impl_detail": {"device": "B200", "kernel": kernel_used, "kernel_choice": args.kernel, "math": "fast"},
+            "impl_detail": {"device": "B200", "kernel": kernel_used, "kernel_choice": args.kernel, "math": "fast",
+                            "wavefront_config": wf_config},
             "e2e": {"value": e2e_value, "unit": "path samples/s", "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": W * H * 16},
             "gpu_launches": int(launches),
@@ -335,6 +351,7 @@ def gpu_arm(args, rank, world, local_rank):
                          "peak_source": "measured FFMA microbenchmark in this run (snelly_measure_fp32_peak)"},
             "clocks": clk,
             "cpu_baseline": cpu,
+            "latency": latency,
         }
         print(json.dumps(out), flush=True)
     if dist is not None:

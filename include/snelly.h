@@ -199,9 +199,16 @@ int snelly_pick(snelly_ctx* ctx, uint64_t scene_id, const snelly_render_desc* de
  * may be NULL. Waits for the job. */
 int snelly_readback_state(snelly_ctx* ctx, uint64_t job_id, uint32_t* rng, float* acc, float* comp, double* acc64);
 /* The integrator a job's frames run: SNELLY_KERNEL_MEGA or SNELLY_KERNEL_WAVEFRONT (a scene
- * created with SNELLY_KERNEL_AUTO gets the autotuner's choice for its module and image size:
- * one warm-up and two timed frames of each integrator, once per size class). */
+ * created with SNELLY_KERNEL_AUTO gets the autotuner's choice for its module and image size, once
+ * per size class: the wavefront's launch configuration by one pass of coordinate descent, each
+ * candidate timed over a warm-up frame and about 5 ms of frames, then the path-per-thread
+ * kernel). No counterpart in the reference, which has one fragment program. */
 int snelly_job_kernel(snelly_ctx* ctx, uint64_t job_id, int* kernel_mode);
+/* A wavefront job's launch configuration, SNELLY_WF_CONFIG_FIELDS ints: concurrent pixel ranges,
+ * per-material shade launches (0/1), drain steps before parking, sphere-tracing steps between
+ * refills, work items claimed per warp, idle lanes that trigger a refill, threads per block. */
+#define SNELLY_WF_CONFIG_FIELDS 7
+int snelly_job_wavefront_config(snelly_ctx* ctx, uint64_t job_id, int* out);
 /* Start a job from saved state instead of seeding (resume). */
 int snelly_restore(snelly_ctx* ctx, uint64_t scene_id, const snelly_render_desc* desc, const uint32_t* rng,
                    const float* acc, const float* comp, uint64_t* job_id);

@@ -57,7 +57,9 @@ def assemble(glsl, opts):
     for key, name in (("SDF_SURFACE(", "HAS_SURFACE"), ("SDF_METAL(", "HAS_METAL"), ("SDF_DIELECTRIC(", "HAS_DIELECTRIC")):
         if key in glsl:
             d.append(name)
-    if opts.has_atmosphere:
+    if "VOLUME_EXTINCTION(" in glsl:  # the heterogeneous-medium extension replaces the atmosphere
+        d.append("HAS_HETERO_VOLUME")
+    elif opts.has_atmosphere:
         d.append("HAS_ATMOSPHERE")
     if opts.has_fog:
         d.append("HAS_FOG")

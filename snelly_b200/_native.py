@@ -134,6 +134,7 @@ def lib():
         "snelly_selftest": (i32, [vp, i32, P(u64)]),
         "snelly_png_unfilter": (i32, [vp, sz, i32, i32, i32, vp]),
         "snelly_job_kernel": (i32, [vp, u64, P(i32)]),
+        "snelly_job_wavefront_config": (i32, [vp, u64, P(i32)]),
         "snelly_image_stats_static": (i32, [vp, u64, P(ctypes.c_double)]),
         "snelly_tonemap": (i32, [vp, u64, P(TonemapParams), vp, sz, i32]),
         "snelly_pick": (i32, [vp, u64, P(RenderDesc), ctypes.c_float, ctypes.c_float, P(ctypes.c_float),

@@ -6,13 +6,15 @@ spp uniform in {4..64}, bounce limits uniform in {4..12}, camera poses on a sphe
 U(4, 8) looking at the origin.
 
 * plain: the single-job path, one job after another: render(spp) then read the image back.
-* batched: every job resident at once; each tick advances all unfinished jobs by one frame with
-  snelly_advance_batch (jobs of one scene module share launches of the path-per-thread kernel,
-  modules overlap on separate streams), and a job is read back when it reaches its spp.
+* batched: every job resident at once; each tick advances all unfinished jobs by up to 8 frames
+  with snelly_advance_batch (the autotuner's wavefront jobs run concurrently as pixel ranges on
+  their own streams; the rest share path-per-thread launches per scene module, modules on separate
+  streams), and a job is read back when it reaches its spp.
+Both use the autotuner's integrator and launch configuration per (scene, image-size class).
 
 `python -m snelly_b200.batchbench` prints one JSON line: path samples per second of both, their
-ratio, per-job time-to-target percentiles of the batched run, and a check that the images are the
-same in both runs.
+ratio, per-job time-to-target percentiles of both (every job submitted at t = 0), and a check that
+the images are the same in both runs.
 """
 import argparse
 import json
@@ -63,34 +65,43 @@ def warm(ctx, jobs, kernel):
 
 
 def run_plain(ctx, jobs, kernel, keep=None):
+    """One job after another through the single-job path; returns (path samples, seconds, per-job
+    times to target measured from the start)."""
     ctx.sync()
     t0 = time.perf_counter()
-    samples = 0
+    samples, done_at = 0, []
     for j in jobs:
         s = _snelly(ctx, j, kernel)
         s.render(j["spp"])
         img = s.readback()
         samples += s.width * s.height * j["spp"]
+        done_at.append(time.perf_counter() - t0)
         if keep is not None:
             keep[j["id"]] = img
         ctx.destroy_job(s.job_id())
-    return samples, time.perf_counter() - t0
+    return samples, time.perf_counter() - t0, np.array(done_at)
 
 
-def run_batched(ctx, jobs, keep=None):
+def run_batched(ctx, jobs, kernel=N.KERNEL_AUTO, frames_per_tick=8, keep=None):
+    """Every job resident at once. Each tick advances every unfinished job by up to
+    `frames_per_tick` frames in one snelly_advance_batch call (the autotuner's wavefront jobs as
+    concurrent pixel ranges on their own streams, the rest in shared path-per-thread launches per
+    scene module); a job is read back once it reaches its spp. Returns (path samples, seconds,
+    per-job times to target)."""
     ctx.sync()
     t0 = time.perf_counter()
     active = {}
     for j in jobs:
-        s = _snelly(ctx, j, N.KERNEL_MEGA)
+        s = _snelly(ctx, j, kernel)
         s.render(0)
         active[s.job_id()] = (j, s, [0])
     samples, done_at = 0, []
     while active:
-        ctx.advance_batch({jid: 1 for jid in active})
+        step = {jid: min(frames_per_tick, j["spp"] - n[0]) for jid, (j, s, n) in active.items()}
+        ctx.advance_batch(step)
         finished = []
         for jid, (j, s, n) in active.items():
-            n[0] += 1
+            n[0] += step[jid]
             if n[0] >= j["spp"]:
                 finished.append(jid)
         for jid in finished:
@@ -104,33 +115,41 @@ def run_batched(ctx, jobs, keep=None):
     return samples, time.perf_counter() - t0, np.array(done_at)
 
 
+def measure(ctx, jobs, frames_per_tick=8, check_images=True):
+    """Plain and batched runs of `jobs` (both with the autotuner's integrator per job): the dict
+    the JSON line reports."""
+    warm(ctx, jobs, N.KERNEL_AUTO)
+    plain_imgs, batch_imgs = ({}, {}) if check_images else (None, None)
+    ps, pt, pdone = run_plain(ctx, jobs, N.KERNEL_AUTO, plain_imgs)
+    bs, bt, bdone = run_batched(ctx, jobs, N.KERNEL_AUTO, frames_per_tick, batch_imgs)
+    out = {
+        "jobs": len(jobs), "path_samples": bs, "pixels": int(sum(j["res"] ** 2 for j in jobs)),
+        "plain": {"seconds": pt, "samples_per_s": ps / pt, "time_to_target_p50_s": float(np.percentile(pdone, 50)),
+                  "time_to_target_p99_s": float(np.percentile(pdone, 99))},
+        "batched": {"seconds": bt, "samples_per_s": bs / bt, "frames_per_tick": frames_per_tick,
+                    "time_to_target_p50_s": float(np.percentile(bdone, 50)),
+                    "time_to_target_p99_s": float(np.percentile(bdone, 99))},
+        "batched_over_plain": (bs / bt) / (ps / pt),
+        "scenes": {n: sum(1 for j in jobs if j["name"] == n) for n in SCENE_NAMES},
+    }
+    if check_images:
+        same = sum(int(np.array_equal(plain_imgs[k], batch_imgs[k])) for k in plain_imgs)
+        out["images_identical_plain_vs_batched"] = f"{same}/{len(plain_imgs)}"
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--jobs", type=int, default=256)
     ap.add_argument("--seed", type=int, default=4)
     ap.add_argument("--max-res", type=int, default=1024)
+    ap.add_argument("--frames-per-tick", type=int, default=8)
     args = ap.parse_args()
     ctx = api.Context(0)
     jobs = job_set(args.jobs, args.seed, res_range=(128, args.max_res))
-    warm(ctx, jobs, N.KERNEL_AUTO)
-    warm(ctx, jobs, N.KERNEL_MEGA)
-    plain_imgs, batch_imgs = {}, {}
-    ps, pt = run_plain(ctx, jobs, N.KERNEL_MEGA, plain_imgs)
-    ps_auto, pt_auto = run_plain(ctx, jobs, N.KERNEL_AUTO)
-    bs, bt, done = run_batched(ctx, jobs, batch_imgs)
-    same = sum(int(np.array_equal(plain_imgs[k], batch_imgs[k])) for k in plain_imgs)
-    print(json.dumps({
-        "metric": "heterogeneous batch: path samples/s, batched vs plain", "jobs": len(jobs),
-        "path_samples": bs, "pixels": int(sum(j["res"] ** 2 for j in jobs)),
-        "plain": {"seconds": pt, "samples_per_s": ps / pt, "kernel": "path-per-thread"},
-        "plain_autotuned": {"seconds": pt_auto, "samples_per_s": ps_auto / pt_auto},
-        "batched": {"seconds": bt, "samples_per_s": bs / bt,
-                    "time_to_target_p50_s": float(np.percentile(done, 50)),
-                    "time_to_target_p99_s": float(np.percentile(done, 99))},
-        "batched_over_plain": (bs / bt) / (ps / pt), "batched_over_plain_autotuned": (bs / bt) / (ps_auto / pt_auto),
-        "images_identical_plain_vs_batched": f"{same}/{len(plain_imgs)}",
-        "scenes": {n: sum(1 for j in jobs if j["name"] == n) for n in SCENE_NAMES},
-    }))
+    out = {"metric": "heterogeneous batch: path samples/s and time to target, batched vs plain"}
+    out.update(measure(ctx, jobs, args.frames_per_tick))
+    print(json.dumps(out))
 
 
 if __name__ == "__main__":

@@ -52,3 +52,33 @@ def build(force=False, verbose=False):
 
 if __name__ == "__main__":
     build(force="--force" in sys.argv, verbose=True)
+
+
+def _compile_one(item):
+    glsl, opts_bytes = item
+    from snelly_b200 import _native as N
+    opts = N.SceneOpts.from_buffer_copy(opts_bytes)
+    N.compile_check(glsl, opts)
+    return True
+
+
+def prebuild_modules(hosts, math_modes=(0, 1), workers=None):
+    """NVRTC-compile the scene modules of `hosts` (host-mirror Snelly objects) for sm_100a in each
+    math mode (0 fast, 1 IEEE-strict), in parallel, into the in-tree module cache
+    (snelly_b200/_build/kcache), where a context on a GPU machine finds them instead of compiling.
+    Returns the number of distinct modules."""
+    import concurrent.futures as cf
+    import multiprocessing as mp
+    items = {}
+    for h in hosts:
+        glsl = h.sceneObj.shader()
+        for mm in math_modes:
+            o = h.scene_opts()
+            o.math_mode = mm
+            o.kernel_mode = 0
+            items[(glsl, bytes(o))] = True
+    work = list(items)
+    with cf.ProcessPoolExecutor(max_workers=workers or min(8, os.cpu_count() or 1),
+                                mp_context=mp.get_context("spawn")) as ex:
+        list(ex.map(_compile_one, work))
+    return len(work)

@@ -681,7 +681,7 @@ SD_FN vec3 perturb_normal(const Ctx& c, const vec3& X, const Frame& f, int mat) 
 #endif
 
 // ---- atmosphere slab (PT:971-1026) --------------------------------------------------------------
-#ifdef HAS_ATMOSPHERE
+#if defined(HAS_ATMOSPHERE) || defined(HAS_HETERO_VOLUME)
 SD_FN bool atmosphere_segment(const Ctx& c, const vec3& p, const vec3& d, float len, float& t0, float& t1) {
   vec3 inv = 1.0f / d;
   vec3 lo = (v3(c.P.atmosphereBoundsMin) * c.P.lengthScale - p) * inv;
@@ -700,9 +700,119 @@ SD_FN bool atmosphere_segment(const Ctx& c, const vec3& p, const vec3& d, float 
 }
 #endif
 
-// Transmittance along a segment known to be free of geometry (PT:1003-1026).
-SD_FN Rad transmittance_free(const Ctx& c, const vec3& p, const vec3& d, float len) {
+#ifdef HAS_HETERO_VOLUME
+// ---- heterogeneous medium (an extension of this build) ----------------------------------------
+// The reference appends default bodies for VOLUME_EXTINCTION, VOLUME_EXTINCTION_MAX,
+// VOLUME_SCATTERING_COLOR, VOLUME_ABSORPTION_COLOR and VOLUME_ANISOTROPY (js/renderer.js:258-262)
+// but its path tracer never calls them. When a scene defines VOLUME_EXTINCTION itself, the
+// atmosphere's box holds a medium with grey extinction VOLUME_EXTINCTION(e, X), e the atmosphere's
+// extinction per unit length (the rgb mean of atmosphereExtinctionCoeffRGB / (atmosphereMFP *
+// lengthScale)), bounded by the majorant VOLUME_EXTINCTION_MAX(e); single-scattering albedo
+// sc / (sc + ab) of the two colour hooks (given the atmosphere's scattering and absorption
+// coefficients), projected on the beam's wavelength; Henyey-Greenstein phase function with
+// g = VOLUME_ANISOTROPY(atmosphereAnisotropy, X). It takes the homogeneous atmosphere's place.
+// Collisions are found by delta tracking with the path's random numbers; transmittance along
+// shadow rays is estimated by ratio tracking with random numbers hashed from the shadow ray's own
+// origin and direction, so the estimate does not depend on when the ray is resolved.
+#define HV_MAX_STEPS 4096
+SD_FN float hv_extinction_ui(const Ctx& c) {
+  const vec3 e = v3(c.P.atmosphereExtinctionCoeffRGB);
+  return (e.x + e.y + e.z) / 3.0f / (c.P.atmosphereMFP * c.P.lengthScale);
+}
+// An xorshift-multiply integer mix (two rounds), for the ratio-tracking streams.
+SD_FN unsigned hv_mix(unsigned x) {
+  x ^= x >> 16;
+  x *= 0x7feb352du;
+  x ^= x >> 15;
+  x *= 0x846ca68bu;
+  x ^= x >> 16;
+  return x;
+}
+SD_FN unsigned hv_seed(const vec3& p, const vec3& d) {
+  unsigned h = 0x2545f491u;
+  const float v[6] = {p.x, p.y, p.z, d.x, d.y, d.z};
+  for (int k = 0; k < 6; ++k) h = hv_mix(h ^ (unsigned)__float_as_int(v[k]));
+  return h;
+}
+SD_FN float hv_uniform(unsigned& h) {  // in [0, 1), 24 bits
+  h = hv_mix(h + 0x9e3779b9u);
+  return float(h >> 8) * (1.0f / 16777216.0f);
+}
+// Ratio-tracking estimate of the medium's transmittance along [p, p + len d] (Russian roulette
+// once it falls below 0.1 keeps it unbiased and bounded).
+SD_FN float hv_transmittance(const Ctx& c, const vec3& p, const vec3& d, float len) {
+  float t0, t1;
+  if (!atmosphere_segment(c, p, d, len, t0, t1)) return 1.0f;
+  const float e = hv_extinction_ui(c);
+  const float mx = c.sc.VOLUME_EXTINCTION_MAX(e);
+  if (!(mx > 0.0f)) return 1.0f;
+  unsigned h = hv_seed(p, d);
+  float T = 1.0f, t = t0;
+  for (int k = 0; k < HV_MAX_STEPS; ++k) {
+    t -= logf(1.0f - hv_uniform(h)) / mx;
+    if (t >= t1) break;
+    T *= 1.0f - glsl::clamp(c.sc.VOLUME_EXTINCTION(e, p + t * d) / mx, 0.0f, 1.0f);
+    if (T < 0.1f) {
+      if (hv_uniform(h) < 0.5f) return 0.0f;
+      T *= 2.0f;
+    }
+  }
+  return T;
+}
+// Delta tracking along [p, p + len d] with the path's random numbers: true and the collision
+// point when the path scatters in the medium before the segment's end.
+SD_FN bool hv_collision(const Ctx& c, const vec3& p, const vec3& d, float len, Rng& g, vec3& ps) {
+  float t0, t1;
+  if (!atmosphere_segment(c, p, d, len, t0, t1)) return false;
+  const float e = hv_extinction_ui(c);
+  const float mx = c.sc.VOLUME_EXTINCTION_MAX(e);
+  if (!(mx > 0.0f)) return false;
+  float t = t0;
+  for (int k = 0; k < HV_MAX_STEPS; ++k) {
+    t -= logf(1.0f - rand01(g)) / mx;
+    if (t >= t1) return false;
+    const vec3 x = p + t * d;
+    if (rand01(g) * mx < c.sc.VOLUME_EXTINCTION(e, x)) {
+      ps = x;
+      return true;
+    }
+  }
+  return false;
+}
+// Henyey-Greenstein direction about `dir` by inversion of its distribution (pdf hg_phase).
+SD_FN vec3 hv_sample_hg(const vec3& dir, float g, Rng& rng) {
+  float ct;
+  const float u = rand01(rng);
+  if (fabsf(g) < 1.0e-3f) {
+    ct = 1.0f - 2.0f * u;
+  } else {
+    const float q = (1.0f - g * g) / (1.0f - g + 2.0f * g * u);
+    ct = glsl::clamp((1.0f + g * g - q * q) / (2.0f * g), -1.0f, 1.0f);
+  }
+  const float st = sqrtf(fmaxf(0.0f, 1.0f - ct * ct));
+  const float phi = 2.0f * kPi * rand01(rng);
+  Frame f = make_frame(dir);
+  return ct * dir + st * (cosf(phi) * f.t + sinf(phi) * f.b);
+}
+// Uniform direction on the sphere (pdf 1 / 4 pi).
+SD_FN vec3 hv_sample_sphere(Rng& g) {
+  const float z = 1.0f - 2.0f * rand01(g);
+  const float r = sqrtf(fmaxf(0.0f, 1.0f - z * z));
+  const float phi = 2.0f * kPi * rand01(g);
+  return vec3(r * cosf(phi), r * sinf(phi), z);
+}
+#endif
+
+// Transmittance along a segment known to be free of geometry (PT:1003-1026). `medium`: include
+// the heterogeneous medium's ratio-tracking estimate (shadow rays); the path's own segments leave
+// it out, since delta tracking has already decided whether the path crosses the medium.
+SD_FN Rad transmittance_free(const Ctx& c, const vec3& p, const vec3& d, float len, bool medium = true) {
   Rad Tr = Rad(1.0f);
+#ifdef HAS_HETERO_VOLUME
+  if (medium) Tr = Rad(hv_transmittance(c, p, d, len));
+#else
+  (void)medium;
+#endif
 #ifdef HAS_ATMOSPHERE
   Rad ext = vol_extinction(c);
   if (glsl::length(ext) == 0.0f) return Rad(1.0f);

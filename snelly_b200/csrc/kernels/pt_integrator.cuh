@@ -390,13 +390,132 @@ SD_FN Rad resolve_deferred(const Ctx& c, const DeferredNee& nd, const bool occlu
   return nd.thr * glsl::min(Rad(c.P.radianceClamp), Ld);
 }
 
-enum { VERTEX_CONTINUE = 0, VERTEX_DONE = 1 };
+enum { VERTEX_CONTINUE = 0, VERTEX_DONE = 1, VERTEX_SSS = 2 };
+
+// A surface vertex that chose the subsurface walk: what the rest of the vertex needs.
+struct SssEntry {
+  Frame fr;     // shading frame at the entry point
+  vec3 ngW;     // geometric normal there
+  Rad ssAlb;    // subsurface albedo
+  float probSSS;
+};
+
+#ifdef HAS_SURFACE
+// The rest of a vertex that chose the subsurface walk (PT:1866-1918): the walk to an exit point,
+// the exit's direct light and the Lambertian continuation direction.
+SD_FN int sss_step(const Ctx& c, PathState& s, const SssEntry& e, Rng& g) {
+  const SnellyParams& P = c.P;
+  Rad walkThr = Rad(0.0f);
+  vec3 pExit(0.0f);
+  Frame fw = e.fr;
+  fw.n = e.ngW;  // geometric normal for the entry (the tangents stay those of the shading frame)
+  if (!sss_walk(c, s.pW, fw, g, e.ssAlb, walkThr, pExit)) return VERTEX_DONE;
+  s.pW = pExit;
+  vec3 nW = sdf_normal(c.job, pExit, MAT_SURFA);
+  Frame fe = make_frame(nW);
+  float bsdfPdf = 0.0f;
+  vec3 dExit = sample_cosine(g, bsdfPdf);
+  vec3 woW = to_world(dExit, fe);
+  s.rayDir = woW;
+  s.thr *= walkThr;
+  float skyPdf = 0.0f, sunPdf = 0.0f, sphPdf = 0.0f;
+  Rad dAlbExit = surf_diffuse(c, s.pW, nW, -s.rayDir);
+  if (!s.inDiele) s.L += s.thr * sss_exit_radiance(c, pExit, fe, g, dAlbExit, skyPdf, sunPdf, sphPdf);
+  s.misSky = balance(bsdfPdf, skyPdf);
+  s.misSun = balance(bsdfPdf, sunPdf);
+#ifdef HAS_SPHERE_LIGHT
+  s.misSph = balance(bsdfPdf, sphPdf);
+#endif
+  Rad lobe = glsl::mix(Rad(1.0f), dAlbExit, P.subsurfaceDiffuseWeight) / kPi;
+  Rad fop = glsl::min(Rad(P.radianceClamp), lobe / fmaxf(kPdfEps, bsdfPdf));
+  s.thr *= fop * fabsf(glsl::dot(woW, nW)) / fmaxf(kPdfEps, e.probSSS);
+  s.pW += nW * glsl::sign(glsl::dot(s.rayDir, nW)) * 3.0f * P.minLengthScale;
+  if (maxc(s.thr) < kThroughputEps) return VERTEX_DONE;
+  return VERTEX_CONTINUE;
+}
+#endif
+
+#ifdef HAS_HETERO_VOLUME
+// A scattering event of the heterogeneous medium at ps (an extension of this build, see
+// pt_device.cuh): the single-scattering albedo, next-event estimation of sky (uniform sphere), sun
+// and sphere light through the phase function with the balance heuristic against the phase
+// function's pdf, and a continuation direction drawn from the phase function (whose weight is one).
+SD_FN int hv_scatter(const Ctx& c, PathState& s, const vec3& ps, Rng& g) {
+  const SnellyParams& P = c.P;
+  const vec3 sca = c.sc.VOLUME_SCATTERING_COLOR(v3(P.atmosphereScatteringCoeffRGB), ps);
+  const vec3 ab = c.sc.VOLUME_ABSORPTION_COLOR(v3(P.atmosphereExtinctionCoeffRGB) - v3(P.atmosphereScatteringCoeffRGB), ps);
+  const vec3 ext = sca + ab;
+  const vec3 a(ext.x > 0.0f ? sca.x / ext.x : 0.0f, ext.y > 0.0f ? sca.y / ext.y : 0.0f, ext.z > 0.0f ? sca.z / ext.z : 0.0f);
+  s.thr *= albedo(a, c.cmf);
+  const float gph = c.sc.VOLUME_ANISOTROPY(P.atmosphereAnisotropy, ps);
+  const vec3 d = s.rayDir;
+  Rad Ld = Rad(0.0f);
+  const float skyPdf = 1.0f / (4.0f * kPi);
+  float sunPdf = 0.0f, sphPdf = 0.0f;
+  if (P.skyPower > kRadianceEps) {
+    const vec3 wo = hv_sample_sphere(g);
+    Rad Li = sky_radiance(c, wo);
+    if (avg(Li) > kRadianceEps) {
+      Li = shadow_scale(c, Li, transmittance(c, ps, wo, P.maxLengthScale));
+      if (avg(Li) > kRadianceEps) {
+        const float ph = hg_phase(glsl::dot(d, wo), gph);
+        Ld += ph * Li / skyPdf * balance(skyPdf, ph);
+      }
+    }
+  }
+  if (P.sunPower > kRadianceEps) {
+    const vec3 wo = sample_sun_dir(c, g, sunPdf);
+    Rad Li = sun_radiance(c, wo);
+    if (avg(Li) > kRadianceEps) {
+      Li = shadow_scale(c, Li, transmittance(c, ps, wo, P.maxLengthScale));
+      if (avg(Li) > kRadianceEps) {
+        const float ph = hg_phase(glsl::dot(d, wo), gph);
+        Ld += ph * Li / fmaxf(kPdfEps, sunPdf) * balance(sunPdf, ph);
+      }
+    }
+  }
+#ifdef HAS_SPHERE_LIGHT
+  if (P.sphereLightPower > kRadianceEps) {
+    vec3 pHit;
+    Rad Li = sample_sphere_light(c, g, ps, pHit, sphPdf);
+    if (avg(Li) > kRadianceEps) {
+      const float dist = fmaxf(0.0f, glsl::length(pHit - ps) - 3.0f * P.minLengthScale);
+      const vec3 wo = glsl::normalize(pHit - ps);
+      Li = shadow_scale(c, Li, transmittance(c, ps, wo, dist));
+      if (avg(Li) > kRadianceEps) {
+        const float ph = hg_phase(glsl::dot(d, wo), gph);
+        Ld += ph * Li / fmaxf(kPdfEps, sphPdf) * balance(sphPdf, ph);
+      }
+    }
+  }
+#endif
+  s.L += s.thr * glsl::min(Rad(P.radianceClamp), Ld);
+  const vec3 wo = hv_sample_hg(d, gph, g);
+  const float php = hg_phase(glsl::dot(d, wo), gph);
+  s.misSky = P.skyPower > kRadianceEps ? balance(php, skyPdf) : 1.0f;
+  s.misSun = balance(php, sunPdf);
+  s.misSph = balance(php, sphPdf);
+  s.pW = ps;
+  s.rayDir = wo;
+  return maxc(s.thr) < kThroughputEps ? VERTEX_DONE : VERTEX_CONTINUE;
+}
+#endif
 
 // Everything of one loop iteration of the camera path after the ray has been traced (`h`).
-// With `nd` non-null the surface vertex's sky/sun next-event estimate is deferred into it.
-SD_FN int vertex_step(const Ctx& c, PathState& s, const Hit& h, int vertex, Rng& g, DeferredNee* nd) {
+// With `nd` non-null the surface vertex's sky/sun next-event estimate is deferred into it; with
+// `sss` non-null a vertex that chooses the subsurface walk stops before it, fills `sss` and
+// returns VERTEX_SSS (the walk stage finishes it with sss_step).
+SD_FN int vertex_step(const Ctx& c, PathState& s, const Hit& h, int vertex, Rng& g, DeferredNee* nd,
+                      SssEntry* sss = nullptr) {
   const SnellyParams& P = c.P;
   (void)vertex;
+#ifdef HAS_HETERO_VOLUME
+  {  // the medium before the hit (or the escape): a collision makes this a scattering vertex
+    vec3 ps(0.0f);
+    const float seg = h.hit ? glsl::length(h.p - s.pW) : P.maxLengthScale;
+    if (hv_collision(c, s.pW, s.rayDir, seg, g, ps)) return hv_scatter(c, s, ps, g);
+  }
+#endif
   float rayLength = P.maxLengthScale;
   if (h.hit) {
     rayLength = glsl::length(h.p - s.pW);
@@ -409,14 +528,14 @@ SD_FN int vertex_step(const Ctx& c, PathState& s, const Hit& h, int vertex, Rng&
     Rad LiSph = (P.sphereLightPower < kRadianceEps) ? Rad(0.0f) : sphere_light_hit(c, s.pW, s.rayDir, pLight);
     if (avg(LiSph) > kRadianceEps) {
       segLen = glsl::length(pLight - s.pW);
-      Tr = transmittance_free(c, s.pW, s.rayDir, segLen);
+      Tr = transmittance_free(c, s.pW, s.rayDir, segLen, false);
       float sp = scatter_prob(c, Tr);
       s.L += s.thr * Tr * s.misSph * LiSph / (1.0f - sp);
     } else
 #endif
     {
       segLen = P.maxLengthScale;
-      Tr = transmittance_free(c, s.pW, s.rayDir, segLen);
+      Tr = transmittance_free(c, s.pW, s.rayDir, segLen, false);
       float sp = scatter_prob(c, Tr);
       if (avg(Tr) > kRadianceEps) {
         if (!(vertex == 0 && !P.envMapVisible) && s.misSky > 0.0f)
@@ -455,7 +574,7 @@ SD_FN int vertex_step(const Ctx& c, PathState& s, const Hit& h, int vertex, Rng&
       float segLen = glsl::length(pLight - s.pW);
       if (segLen < rayLength) {
         hitSphereLight = true;
-        Tr = transmittance_free(c, s.pW, s.rayDir, segLen);
+        Tr = transmittance_free(c, s.pW, s.rayDir, segLen, false);
         s.L += s.thr * Tr * s.misSph * LiSph;
 #ifdef HAS_ATMOSPHERE
         if (vertex < 2) s.L += s.thr * atm_inscatter(c, s.pW, s.rayDir, segLen, g);
@@ -469,7 +588,7 @@ SD_FN int vertex_step(const Ctx& c, PathState& s, const Hit& h, int vertex, Rng&
 #endif
 #ifdef HAS_ATMOSPHERE
   if (vertex < 2) s.L += s.thr * atm_inscatter(c, s.pW, s.rayDir, rayLength, g);
-  if (!hitSphereLight) Tr = transmittance_free(c, s.pW, s.rayDir, rayLength);
+  if (!hitSphereLight) Tr = transmittance_free(c, s.pW, s.rayDir, rayLength, false);
   if (s.atmScatters + 1 < MAX_ATMOSPHERE_SCATTERS) {
     float sp = scatter_prob(c, Tr);
     if (sp > rand01(g)) {
@@ -483,7 +602,7 @@ SD_FN int vertex_step(const Ctx& c, PathState& s, const Hit& h, int vertex, Rng&
     s.thr /= fmaxf(kDenomTol, 1.0f - sp);
   }
   if (hitSphereLight) return VERTEX_DONE;
-  s.thr *= transmittance_free(c, s.pW, s.rayDir, rayLength);
+  s.thr *= transmittance_free(c, s.pW, s.rayDir, rayLength, false);
 #endif
 
   // surface interaction (PT:1782-1794)
@@ -543,34 +662,16 @@ SD_FN int vertex_step(const Ctx& c, PathState& s, const Hit& h, int vertex, Rng&
 #endif
   }
 #ifdef HAS_SURFACE
-  else {
-    // subsurface random walk to a new vertex (PT:1866-1918)
-    Rad walkThr = Rad(0.0f);
-    vec3 pExit(0.0f);
-    Frame fw = fr;
-    fw.n = ngW;  // geometric normal for the entry (the tangents stay those of the shading frame)
-    if (!sss_walk(c, s.pW, fw, g, ssAlb, walkThr, pExit)) return VERTEX_DONE;
-    s.pW = pExit;
-    nW = sdf_normal(c.job, pExit, MAT_SURFA);
-    Frame fe = make_frame(nW);
-    float bsdfPdf = 0.0f;
-    vec3 dExit = sample_cosine(g, bsdfPdf);
-    vec3 woW = to_world(dExit, fe);
-    s.rayDir = woW;
-    s.thr *= walkThr;
-    float skyPdf = 0.0f, sunPdf = 0.0f, sphPdf = 0.0f;
-    Rad dAlbExit = surf_diffuse(c, s.pW, nW, -s.rayDir);
-    if (!s.inDiele) s.L += s.thr * sss_exit_radiance(c, pExit, fe, g, dAlbExit, skyPdf, sunPdf, sphPdf);
-    s.misSky = balance(bsdfPdf, skyPdf);
-    s.misSun = balance(bsdfPdf, sunPdf);
-#ifdef HAS_SPHERE_LIGHT
-    s.misSph = balance(bsdfPdf, sphPdf);
-#endif
-    Rad lobe = glsl::mix(Rad(1.0f), dAlbExit, P.subsurfaceDiffuseWeight) / kPi;
-    Rad fop = glsl::min(Rad(P.radianceClamp), lobe / fmaxf(kPdfEps, bsdfPdf));
-    s.thr *= fop * fabsf(glsl::dot(woW, nW)) / fmaxf(kPdfEps, probSSS);
-    s.pW += nW * glsl::sign(glsl::dot(s.rayDir, nW)) * 3.0f * P.minLengthScale;
+  else {  // subsurface random walk to a new vertex (PT:1866-1918)
+    SssEntry e{fr, ngW, ssAlb, probSSS};
+    if (sss) {
+      *sss = e;
+      return VERTEX_SSS;
+    }
+    return sss_step(c, s, e, g);
   }
+#else
+  (void)sss;
 #endif
   if (maxc(s.thr) < kThroughputEps) return VERTEX_DONE;
   return VERTEX_CONTINUE;
@@ -594,24 +695,38 @@ SD_FN Rad camera_path(const Ctx& c, vec3 pW, vec3 rayDir, Rng& g) {
   return s.L;
 }
 
-// Wavelength for this pixel and frame (PT:1936-1947): the inverse CDF of the emission spectrum
-// at a stratum centre in [0.1, 0.9]; returns the CIE XYZ weights at that wavelength.
-SD_FN vec3 pick_wavelength(Ctx& c, Rng& g) {
+// The wavelength at parameter w in [0, 1] of 390..750 nm: sets c.lambda and the normalised rgb
+// colour-matching weights c.cmf, returns the CIE XYZ weights (PT:1940-1947). The wavefront
+// stores w per path and rebuilds these from it in each stage.
+SD_FN vec3 wavelength_at(Ctx& c, float w) {
 #ifdef DISPERSION_ENABLED
-  const SnellyParams& P = c.P;
-  float ns = float(P.wavelengthSamples);
-  float xi = 0.1f + 0.8f * (0.5f + glsl::s_floor(ns * rand01(g))) / ns;
-  float w = table1(c.Pg->icdfTable, SNELLY_ICDF_SAMPLES, xi);
   c.lambda = 390.0f + (750.0f - 390.0f) * w;
   vec3 xyz = table_xyz(c.Pg->xyzTable, w);
   c.cmf = xyz_to_rgb_normalized(xyz);
   return xyz;
 #else
-  (void)g;
+  (void)w;
   c.lambda = 390.0f + (750.0f - 390.0f) * 0.5f;
   c.cmf = vec3(0.0f);
   return vec3(0.0f);
 #endif
+}
+
+// Wavelength for this pixel and frame (PT:1936-1947): the inverse CDF of the emission spectrum
+// at a stratum centre in [0.1, 0.9]; returns the CIE XYZ weights at that wavelength, and its
+// parameter w in `w_out`.
+SD_FN vec3 pick_wavelength(Ctx& c, Rng& g, float* w_out = nullptr) {
+#ifdef DISPERSION_ENABLED
+  const SnellyParams& P = c.P;
+  float ns = float(P.wavelengthSamples);
+  float xi = 0.1f + 0.8f * (0.5f + glsl::s_floor(ns * rand01(g))) / ns;
+  float w = table1(c.Pg->icdfTable, SNELLY_ICDF_SAMPLES, xi);
+#else
+  (void)g;
+  float w = 0.5f;
+#endif
+  if (w_out) *w_out = w;
+  return wavelength_at(c, w);
 }
 
 // A scene's CONSTRUCT_PRIMARY_RAY hook works on the reference's float RNG state; the integer

@@ -35,33 +35,21 @@ typedef struct JobRec {
   float pick_x, pick_y;  // (gl_FragCoord units of a frame of params.resolution)
 } JobRec;
 
-// Wavefront path state and queues of one job (structure of arrays, one element per path =
-// pixel of the frame; device pointers). Layout shared with the host (wavefront.cpp).
+// Wavefront path state and queues of one job (device pointers). Layout shared with the host
+// (wavefront.cpp). A path's state is one contiguous record of `rec_f4` float4 slots (the slot
+// map is in pt_wavefront.cuh), so that a stage reading it touches a few whole 32-byte sectors
+// wherever the path sits in the queue it came from.
 #define WF_A 0      // active-path queue counts [2] (ping-pong by iteration parity)
 #define WF_S 2      // shadow-ray queue counts [2]
 #define WF_C 4      // parked-ray queue counts [2]
 #define WF_LEFT 6   // paths of the frame not finished yet
 #define WF_Q 8      // shade-queue segment counts [2][4]
-#define WF_HEAD 16  // extend work heads, one per iteration
+#define WF_SSS 16   // subsurface-walk queue count (filled by the shade stage, read by the walk stage)
+#define WF_HEAD 17  // extend work heads, one per iteration
 #define WF_MAX_ITERS 300
 #define WF_COUNTERS (WF_HEAD + WF_MAX_ITERS)
 typedef struct WfBuffers {
-  float4* pos;      // path vertex pW (xyz)
-  float4* dir;      // ray direction (xyz)
-  float4* thr;      // throughput (Rad in xyz)
-  float4* rad;      // accumulated radiance L
-  float4* cmf;      // rgb colour-matching weights (xyz), wavelength (w)
-  float4* mis;      // MIS weights sky, sun, sphere
-  float4* xyzw;     // XYZ weights of the wavelength (xyz)
-  int4* info;       // vertex, atmosphere scatters, flags, unused
-  uint4* rng;       // RNG lanes during the frame
-  float4* hit;      // continuation hit position (xyz), encoded material + hit flag (w)
-  float4* nee_org;  // shadow-ray origin
-  float4* nee_thr;  // throughput at the vertex of the pending estimate
-  float4* nee_extra;  // sphere-light term (already shadowed)
-  float4* nee_dir[2];  // sky, sun shadow directions (xyz) and lengths (w)
-  float4* nee_c[2];    // unoccluded contributions
-  float4* nee_li[2];   // unshadowed radiance (gate)
+  float4* rec;      // path records, rec_f4 float4 slots per path
   float4* mt;       // march state of a parked ray (distance, sign, step count), by ray id
   unsigned char* shadow;  // occlusion result per shadow ray (2 per path)
   int* pend;        // rays each path waits for
@@ -70,7 +58,10 @@ typedef struct WfBuffers {
   int* qc[2];       // parked-ray queues (ray ids: 2 * path + light, or 2 * paths + path)
   int* qshade[2];   // shade queues [2] (ping-pong by iteration parity), 4 segments of `paths`
                     // entries each: finish/miss, surface, metal, dielectric
+  int* qsss;        // paths whose surface vertex chose the subsurface walk (one iteration's)
   int* cnt;         // counters (WF_*)
   int paths;
   int pixel_begin;
+  int rec_f4;       // float4 slots per path record (checked against the module's layout)
+  int slot;         // the job's constant-memory parameter and uniform slot
 } WfBuffers;

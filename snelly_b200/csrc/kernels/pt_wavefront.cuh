@@ -19,31 +19,207 @@
 #include "pt_integrator.cuh"
 #include "pt_launch.h"
 
-#ifndef WF_REFILL
-#define WF_REFILL 4  // idle lanes of a warp that trigger a refill
-#endif
-#ifndef WF_GRAB
-#define WF_GRAB 32  // work items a warp claims from the global head at a time
-#endif
-#ifndef WF_CHUNK
-#define WF_CHUNK 8  // sphere-tracing steps between refills
-#endif
 #define WF_FULL 0xffffffffu
 
 namespace sdev {
 
 enum { WF_INDIELE = 1, WF_FINISHING = 2, WF_NEE = 4, WF_NEE_SKY = 8, WF_NEE_SUN = 16 };
 
+// ---- the path record ----------------------------------------------------------------------------
+// One path's state: WF_REC float4 slots, contiguous. Slots a stage reads together sit in the same
+// 32-byte sectors: extend reads R_POS + R_DIR (one sector) for a continuation ray, R_NORG and one
+// shadow direction for a shadow ray; shade reads R_POS..R_INFO (96 bytes) and, when the previous
+// vertex deferred its light estimate, R_NORG..R_NC. The colour-matching weights are rebuilt from
+// the wavelength parameter w (in R_INFO.w) instead of being stored. With a surface material the
+// record ends with the subsurface-walk hand-over (R_S0..), written only by paths that take it.
 #ifdef DISPERSION_ENABLED
-SD_FN Rad ld_rad(const float4& v) { return v.x; }
-SD_FN float4 st_rad(const Rad& r) { return make_float4(r, 0.0f, 0.0f, 0.0f); }
+enum {
+  R_POS = 0,    // vertex pW (xyz), throughput (w)
+  R_DIR = 1,    // ray direction (xyz), radiance L (w)
+  R_HIT = 2,    // continuation hit position (xyz), encoded hit flag and material (w)
+  R_MIS = 3,    // MIS weights sky, sun, sphere (xyz), deferred estimate's sphere-light term (w)
+  R_RNG = 4,    // RNG lanes
+  R_INFO = 5,   // vertex, atmosphere scatters, flags, wavelength parameter w (float bits)
+  R_NORG = 6,   // shadow-ray origin (xyz), throughput at the deferred estimate's vertex (w)
+  R_NDIR = 7,   // [2] sky, sun shadow directions (xyz) and lengths (w)
+  R_NC = 9,     // unoccluded contributions c0, c1 and unshadowed radiance li0, li1
+  R_S0 = 10,    // subsurface entry: shading normal (xyz), probSSS (w)
+  R_S1 = 11,    // tangent (xyz), subsurface albedo (w)
+  R_S2 = 12,    // bitangent (xyz)
+  R_S3 = 13,    // geometric normal (xyz)
+  R_BASE = 10
+};
 #else
-SD_FN Rad ld_rad(const float4& v) { return vec3(v.x, v.y, v.z); }
-SD_FN float4 st_rad(const Rad& r) { return make_float4(r.x, r.y, r.z, 0.0f); }
+enum {
+  R_POS = 0,    // pW (xyz), misSky (w)
+  R_DIR = 1,    // ray direction (xyz), misSun (w)
+  R_HIT = 2,    // hit position (xyz), encoded hit (w)
+  R_THR = 3,    // throughput (xyz), misSph (w)
+  R_L = 4,      // radiance (xyz)
+  R_RNG = 5,
+  R_INFO = 6,   // vertex, atmosphere scatters, flags, unused
+  R_NORG = 7,   // shadow-ray origin (xyz)
+  R_NDIR = 8,   // [2] shadow directions and lengths
+  R_NTHR = 10,  // throughput at the deferred estimate's vertex
+  R_NEXTRA = 11,  // sphere-light term
+  R_NC = 12,    // [2] unoccluded contributions
+  R_NLI = 14,   // [2] unshadowed radiance
+  R_S0 = 16,    // shading normal (xyz), probSSS (w)
+  R_S1 = 17,    // tangent
+  R_S2 = 18,    // bitangent
+  R_S3 = 19,    // geometric normal
+  R_S4 = 20,    // subsurface albedo (xyz)
+  R_BASE = 16
+};
 #endif
+#ifdef HAS_SURFACE
+#ifdef DISPERSION_ENABLED
+#define WF_REC 14
+#else
+#define WF_REC 21
+#endif
+#else
+#define WF_REC R_BASE
+#endif
+
 SD_FN vec3 ld3(const float4& v) { return vec3(v.x, v.y, v.z); }
 SD_FN float4 st3(const vec3& v, float w = 0.0f) { return make_float4(v.x, v.y, v.z, w); }
 SD_FN unsigned lanemask_lt() { return (1u << (threadIdx.x & 31)) - 1u; }
+SD_FN float4* rec_of(float4* rec, int path) { return rec + (size_t)path * WF_REC; }
+// One of a ping-pong pair of queues. A select, not an index: a kernel parameter block indexed with
+// a run-time value is copied to local memory.
+SD_FN int* pp(int* const (&q)[2], int k) { return k ? q[1] : q[0]; }
+
+// The part of PathState a path carries between stages, and its bookkeeping.
+struct WfState {
+  PathState s;
+  Rng g;
+  int vertex, flags;
+  float w;  // wavelength parameter
+};
+
+SD_FN void load_state(const float4* r, WfState& st) {
+  float4 a = r[R_POS], b = r[R_DIR];
+  uint4 q = *reinterpret_cast<const uint4*>(r + R_RNG);
+  int4 in = *reinterpret_cast<const int4*>(r + R_INFO);
+  st.s.pW = ld3(a);
+  st.s.rayDir = ld3(b);
+#ifdef DISPERSION_ENABLED
+  float4 m = r[R_MIS];
+  st.s.thr = a.w;
+  st.s.L = b.w;
+  st.s.misSky = m.x;
+  st.s.misSun = m.y;
+  st.s.misSph = m.z;
+#else
+  float4 t = r[R_THR], l = r[R_L];
+  st.s.thr = ld3(t);
+  st.s.L = ld3(l);
+  st.s.misSky = a.w;
+  st.s.misSun = b.w;
+  st.s.misSph = t.w;
+#endif
+  st.g.s[0] = q.x; st.g.s[1] = q.y; st.g.s[2] = q.z; st.g.s[3] = q.w;
+  st.vertex = in.x;
+  st.s.atmScatters = in.y;
+  st.flags = in.z;
+  st.w = __int_as_float(in.w);
+  st.s.inDiele = in.z & WF_INDIELE;
+}
+
+SD_FN void store_state(float4* r, const WfState& st, float nee_extra_w = 0.0f) {
+  (void)nee_extra_w;
+#ifdef DISPERSION_ENABLED
+  r[R_POS] = st3(st.s.pW, st.s.thr);
+  r[R_DIR] = st3(st.s.rayDir, st.s.L);
+  r[R_MIS] = make_float4(st.s.misSky, st.s.misSun, st.s.misSph, nee_extra_w);
+#else
+  r[R_POS] = st3(st.s.pW, st.s.misSky);
+  r[R_DIR] = st3(st.s.rayDir, st.s.misSun);
+  r[R_THR] = st3(st.s.thr, st.s.misSph);
+  r[R_L] = st3(st.s.L);
+#endif
+  *reinterpret_cast<uint4*>(r + R_RNG) = make_uint4(st.g.s[0], st.g.s[1], st.g.s[2], st.g.s[3]);
+  *reinterpret_cast<int4*>(r + R_INFO) = make_int4(st.vertex, st.s.atmScatters, st.flags, __float_as_int(st.w));
+}
+
+// The deferred next-event estimate of a path's previous vertex.
+SD_FN void store_nee(float4* r, const DeferredNee& nd) {
+#ifdef DISPERSION_ENABLED
+  r[R_NORG] = st3(nd.org, nd.thr);
+  r[R_NC] = make_float4(nd.c[0], nd.c[1], nd.li[0], nd.li[1]);
+#else
+  r[R_NORG] = st3(nd.org);
+  r[R_NTHR] = st3(nd.thr);
+  r[R_NEXTRA] = st3(nd.extra);
+  for (int l = 0; l < 2; ++l) {
+    r[R_NC + l] = st3(nd.c[l]);
+    r[R_NLI + l] = st3(nd.li[l]);
+  }
+#endif
+  for (int l = 0; l < 2; ++l)
+    if (nd.pending[l]) r[R_NDIR + l] = st3(nd.dir[l], nd.dist[l]);
+}
+SD_FN void load_nee(const float4* r, DeferredNee& nd, int flags) {
+  float4 o = r[R_NORG];
+  nd.org = ld3(o);
+#ifdef DISPERSION_ENABLED
+  float4 cc = r[R_NC];
+  nd.thr = o.w;
+  nd.extra = r[R_MIS].w;
+  nd.c[0] = cc.x;
+  nd.c[1] = cc.y;
+  nd.li[0] = cc.z;
+  nd.li[1] = cc.w;
+#else
+  nd.thr = ld3(r[R_NTHR]);
+  nd.extra = ld3(r[R_NEXTRA]);
+  for (int l = 0; l < 2; ++l) {
+    nd.c[l] = ld3(r[R_NC + l]);
+    nd.li[l] = ld3(r[R_NLI + l]);
+  }
+#endif
+  for (int l = 0; l < 2; ++l) {
+    nd.pending[l] = flags & (l == 0 ? WF_NEE_SKY : WF_NEE_SUN);
+    if (nd.pending[l]) {
+      float4 dd = r[R_NDIR + l];
+      nd.dir[l] = ld3(dd);
+      nd.dist[l] = dd.w;
+    }
+  }
+}
+
+#ifdef HAS_SURFACE
+SD_FN void store_sss(float4* r, const SssEntry& e) {
+#ifdef DISPERSION_ENABLED
+  r[R_S0] = st3(e.fr.n, e.probSSS);
+  r[R_S1] = st3(e.fr.t, e.ssAlb);
+  r[R_S2] = st3(e.fr.b);
+  r[R_S3] = st3(e.ngW);
+#else
+  r[R_S0] = st3(e.fr.n, e.probSSS);
+  r[R_S1] = st3(e.fr.t);
+  r[R_S2] = st3(e.fr.b);
+  r[R_S3] = st3(e.ngW);
+  r[R_S4] = st3(e.ssAlb);
+#endif
+}
+SD_FN SssEntry load_sss(const float4* r) {
+  SssEntry e;
+  float4 a = r[R_S0], b = r[R_S1];
+  e.fr.n = ld3(a);
+  e.probSSS = a.w;
+  e.fr.t = ld3(b);
+  e.fr.b = ld3(r[R_S2]);
+  e.ngW = ld3(r[R_S3]);
+#ifdef DISPERSION_ENABLED
+  e.ssAlb = b.w;
+#else
+  e.ssAlb = ld3(r[R_S4]);
+#endif
+  return e;
+}
+#endif
 
 // Warp-aggregated append: every lane calls it; lanes with `on` get consecutive slots.
 SD_FN int warp_append(int* counter, bool on) {
@@ -91,12 +267,20 @@ SD_FN void finish_path(const JobRec& J, const WfBuffers& B, int path, const Rad&
 
 }  // namespace sdev
 
+// Record layout the host allocates for (float4 slots per path).
+extern "C" __constant__ int snelly_wf_rec_f4 = WF_REC;
+
 extern "C" __global__ void __launch_bounds__(SNELLY_BLOCK) snelly_wf_generate(const JobRec* __restrict__ jobs,
                                                                            const SnellyParams* __restrict__ gparams,
                                                                            WfBuffers B) {
   using namespace sdev;
   const JobRec& J = jobs[0];
   int path = blockIdx.x * blockDim.x + threadIdx.x;
+  if (B.rec_f4 != snelly_wf_rec_f4) {  // buffers laid out for another record size: trace nothing
+    if (path == 0)
+      for (int k = 0; k < WF_COUNTERS; ++k) B.cnt[k] = 0;
+    return;
+  }
   if (path == 0) {
     for (int k = 0; k < WF_COUNTERS; ++k) B.cnt[k] = 0;
     B.cnt[WF_A + 0] = B.paths;
@@ -104,32 +288,25 @@ extern "C" __global__ void __launch_bounds__(SNELLY_BLOCK) snelly_wf_generate(co
   }
   if (path >= B.paths) return;
   long long i = (long long)B.pixel_begin + path;
-  const SnellyParams& P = c_params[0];
+  const SnellyParams& P = c_params[B.slot];
   uint4 r4 = J.rng[i];
-  Rng g;
-  g.s[0] = r4.x; g.s[1] = r4.y; g.s[2] = r4.z; g.s[3] = r4.w;
-  Scene sc(uniforms_of(0));
+  WfState st;
+  st.g.s[0] = r4.x; st.g.s[1] = r4.y; st.g.s[2] = r4.z; st.g.s[3] = r4.w;
+  Scene sc(uniforms_of(B.slot));
   sc.INIT();
-  Ctx c{P, gparams, sc, 0, 0.0f, vec3(0.0f), Frame()};
+  Ctx c{P, gparams, sc, B.slot, 0.0f, vec3(0.0f), Frame()};
   const int W = J.width;
   const int x = int(i % W), y = int(i / W);
-  vec3 xyzw = pick_wavelength(c, g);
+  pick_wavelength(c, st.g, &st.w);
   c.sun = make_frame(v3(P.sunDir));
-  float jx = 0.5f * P.filterRadius * tent(rand01(g));
-  float jy = 0.5f * P.filterRadius * tent(rand01(g));
+  float jx = 0.5f * P.filterRadius * tent(rand01(st.g));
+  float jy = 0.5f * P.filterRadius * tent(rand01(st.g));
   vec3 start, dir;
-  primary_ray_hook(c, vec2(float(x) + 0.5f, float(y) + 0.5f) + vec2(jx, jy), g, start, dir);
-  PathState s;
-  start_path(c, s, start, dir);
-  B.pos[path] = st3(s.pW);
-  B.dir[path] = st3(s.rayDir);
-  B.thr[path] = st_rad(s.thr);
-  B.rad[path] = st_rad(s.L);
-  B.cmf[path] = st3(c.cmf, c.lambda);
-  B.mis[path] = make_float4(1.0f, 1.0f, 1.0f, 0.0f);
-  B.xyzw[path] = st3(xyzw);
-  B.info[path] = make_int4(0, 0, s.inDiele ? WF_INDIELE : 0, 0);
-  B.rng[path] = make_uint4(g.s[0], g.s[1], g.s[2], g.s[3]);
+  primary_ray_hook(c, vec2(float(x) + 0.5f, float(y) + 0.5f) + vec2(jx, jy), st.g, start, dir);
+  start_path(c, st.s, start, dir);
+  st.vertex = 0;
+  st.flags = st.s.inDiele ? WF_INDIELE : 0;
+  store_state(rec_of(B.rec, path), st);
   B.pend[path] = 1;  // the camera ray
   B.qa[0][path] = path;
 }
@@ -137,12 +314,13 @@ extern "C" __global__ void __launch_bounds__(SNELLY_BLOCK) snelly_wf_generate(co
 // Trace the rays of iteration `it`: the continuation rays of the active paths, the pending shadow
 // rays of their previous vertex, and rays an earlier iteration set aside unfinished.
 //
-// Every pass of the loop runs up to WF_CHUNK sphere-tracing steps, each evaluating the scene SDFs
+// Every pass of the loop runs up to `chunk` sphere-tracing steps, each evaluating the scene SDFs
 // once for every lane that holds a ray; a ray's first evaluation (at its origin, which fixes the
 // marching sign, PT:888-900) is such a step too, so refilled lanes march in step with the rest of
-// the warp. Idle lanes are refilled when at least WF_REFILL of them are idle, or when none of the
-// warp is busy, from a range of WF_GRAB items the warp claims from the global work head with one
-// atomic. Once the work of the iteration is exhausted, a warp marches at most `drain` more steps
+// the warp. Idle lanes are refilled when at least `refill` of them are idle, or when none of the
+// warp is busy, from a range of `grab` items the warp claims from the global work head with one
+// atomic (all three chosen by the host's autotuner; 8, 32 and 4 by default). Once the work of the
+// iteration is exhausted, a warp marches at most `drain` more steps
 // (0: no limit) and then parks its unfinished rays (distance, sign, step count) for the next
 // iteration, so no launch waits for the few longest rays. The march of a ray is the same sequence
 // of operations however it is split, so results do not depend on where it was interrupted.
@@ -150,23 +328,25 @@ extern "C" __global__ void __launch_bounds__(SNELLY_BLOCK) snelly_wf_generate(co
 // A path is shaded once all its rays (continuation and shadows) are done: each finished ray
 // decrements the path's pending count, and the last one queues the path for shading in the
 // shade-queue segment of its continuation hit's material (misses and finishing paths: segment 0).
-extern "C" __global__ void __launch_bounds__(SNELLY_BLOCK) snelly_wf_extend(WfBuffers B, int it, int drain) {
+extern "C" __global__ void __launch_bounds__(SNELLY_BLOCK) snelly_wf_extend(WfBuffers B, int it, int drain, int chunk,
+                                                                                  int grab, int refill) {
   using namespace sdev;
-  const SnellyParams& P = c_params[0];
-  Scene sc(uniforms_of(0));
+  const SnellyParams& P = c_params[B.slot];
+  Scene sc(uniforms_of(B.slot));
   sc.INIT();
   int* cnt = B.cnt;
   const int cur = it & 1, nxt = cur ^ 1;
   if (blockIdx.x == 0 && threadIdx.x == 0) {  // queues the next shade stage and iteration fill
     cnt[WF_A + nxt] = 0;
     cnt[WF_S + nxt] = 0;
+    cnt[WF_SSS] = 0;
     for (int k = 0; k < 4; ++k) cnt[WF_Q + 4 * nxt + k] = 0;
   }
   const int nA = cnt[WF_A + cur], nS = cnt[WF_S + cur], nC = cnt[WF_C + cur];
   const int total = nA + nS + nC;
-  const int* qa = B.qa[cur];
-  const int* qs = B.qs[cur];
-  const int* qc = B.qc[cur];
+  const int* qa = pp(B.qa, cur);
+  const int* qs = pp(B.qs, cur);
+  const int* qc = pp(B.qc, cur);
   int* qcnt = cnt + WF_Q + 4 * cur;
   const float minMarch = P.minLengthScale;
   const float maxLen = P.maxLengthScale;
@@ -188,13 +368,13 @@ extern "C" __global__ void __launch_bounds__(SNELLY_BLOCK) snelly_wf_extend(WfBu
     const bool want = !has;
     const unsigned need = __ballot_sync(WF_FULL, want);
     const unsigned busy = __ballot_sync(WF_FULL, has);
-    if (!wdone && need && (__popc(need) >= WF_REFILL || !busy)) {
+    if (!wdone && need && (__popc(need) >= refill || !busy)) {
       if (wbase >= wlim) {
         int nb = 0;
-        if ((threadIdx.x & 31) == 0) nb = atomicAdd(cnt + WF_HEAD + it, WF_GRAB);
+        if ((threadIdx.x & 31) == 0) nb = atomicAdd(cnt + WF_HEAD + it, grab);
         nb = __shfl_sync(WF_FULL, nb, 0);
         wbase = nb;
-        wlim = min(nb + WF_GRAB, total);
+        wlim = min(nb + grab, total);
         wdone = nb >= total;
       }
       const int w = wbase + __popc(need & lanemask_lt());
@@ -213,14 +393,16 @@ extern "C" __global__ void __launch_bounds__(SNELLY_BLOCK) snelly_wf_extend(WfBu
         if (r >= P2) {
           path = r - P2;
           sidx = -1;
-          o = ld3(B.pos[path]);
-          d = ld3(B.dir[path]);
+          const float4* rp = rec_of(B.rec, path);
+          o = ld3(rp[R_POS]);
+          d = ld3(rp[R_DIR]);
           maxd = maxLen;
         } else {
           sidx = r;
           path = sidx >> 1;
-          o = ld3(B.nee_org[path]);
-          float4 dd = B.nee_dir[sidx & 1][path];
+          const float4* rp = rec_of(B.rec, path);
+          o = ld3(rp[R_NORG]);
+          float4 dd = rp[R_NDIR + (sidx & 1)];
           d = ld3(dd);
           maxd = dd.w;
         }
@@ -234,8 +416,8 @@ extern "C" __global__ void __launch_bounds__(SNELLY_BLOCK) snelly_wf_extend(WfBu
         }
       }
     }
-    // ---- up to WF_CHUNK sphere-tracing steps (PT:888-919); a lane stops when its ray is done ----
-    for (int k = 0; k < WF_CHUNK && has && !done; ++k) {
+    // ---- up to `chunk` sphere-tracing steps (PT:888-919); a lane stops when its ray is done ----
+    for (int k = 0; k < chunk && has && !done; ++k) {
       const vec3 p = first ? o : o + t * d;
       float sdf = 1.0e20f;
       int m = MAT_INVAL;
@@ -288,13 +470,13 @@ extern "C" __global__ void __launch_bounds__(SNELLY_BLOCK) snelly_wf_extend(WfBu
         }
       }
     }
-    if (wdone) drained += WF_CHUNK;
+    if (wdone) drained += chunk;
     const bool park = drain > 0 && drained >= drain && has && !done;  // set aside for the next iteration
     // ---- results ---------------------------------------------------------------------------
     if (__any_sync(WF_FULL, done || park)) {
       int seg = -1;
       if (done) {
-        if (sidx < 0) B.hit[path] = st3(o + t * d, enc_hit(res_hit, res_mat));
+        if (sidx < 0) rec_of(B.rec, path)[R_HIT] = st3(o + t * d, enc_hit(res_hit, res_mat));
         else B.shadow[sidx] = res_hit ? 1 : 0;
         __threadfence();
         if (atomicSub(B.pend + path, 1) == 1) {  // the path's last ray: queue it for shading
@@ -304,153 +486,243 @@ extern "C" __global__ void __launch_bounds__(SNELLY_BLOCK) snelly_wf_extend(WfBu
             h = res_hit;
             hm = res_mat;
           } else {
-            dec_hit(__ldcg(&B.hit[path].w), h, hm);
+            dec_hit(__ldcg(&rec_of(B.rec, path)[R_HIT].w), h, hm);
           }
           seg = !h ? 0 : (hm == MAT_SURFA ? 1 : (hm == MAT_METAL ? 2 : (hm == MAT_DIELE ? 3 : 0)));
         }
       }
       for (int sgi = 0; sgi < 4; ++sgi) {
         int slot = warp_append(qcnt + sgi, seg == sgi);
-        if (slot >= 0) B.qshade[cur][sgi * B.paths + slot] = path;
+        if (slot >= 0) pp(B.qshade, cur)[sgi * B.paths + slot] = path;
       }
       const int r = sidx >= 0 ? sidx : P2 + path;
       if (park) B.mt[r] = make_float4(t, sgn, __int_as_float(n), 0.0f);
       int slot = warp_append(cnt + WF_C + nxt, park);
-      if (slot >= 0) B.qc[nxt][slot] = r;
+      if (slot >= 0) pp(B.qc, nxt)[slot] = r;
       if (done || park) has = false;
     }
     if (wdone && !__any_sync(WF_FULL, has)) break;
   }
 }
 
-// Shade every path the extend stage of iteration `it` queued, and count the frame's paths down.
-extern "C" __global__ void __launch_bounds__(SNELLY_BLOCK, SNELLY_SHADE_MIN_BLOCKS) snelly_wf_shade(const JobRec* __restrict__ jobs,
-                                                                        const SnellyParams* __restrict__ gparams,
-                                                                        WfBuffers B, int it) {
-  using namespace sdev;
+// ---- shading -------------------------------------------------------------------------------------
+namespace sdev {
+
+// Shade one queued path of iteration `it`: resolve the previous vertex's deferred next-event
+// estimate with its shadow results, run the vertex (vertex_step) with the sky/sun shadow rays
+// deferred, and queue what the path waits for next. MAT is the material every path of the calling
+// kernel hit (MAT_INVAL: read it from the record). Returns true when the path finished.
+template <int MAT>
+SD_FN void shade_path(const JobRec& J, const SnellyParams* gparams, const WfBuffers& B, Scene& sc, int path, int nxt,
+                      bool& push_active, int& push_shadow, bool& push_direct, bool& push_sss, bool& finished) {
+  const SnellyParams& P = c_params[B.slot];
+  float4* r = rec_of(B.rec, path);
+  WfState st;
+  load_state(r, st);
+  Ctx c{P, gparams, sc, B.slot, 0.0f, vec3(0.0f), make_frame(v3(P.sunDir))};
+  const vec3 xyzw = wavelength_at(c, st.w);
+  int flags = st.flags;
+  if (flags & WF_NEE) {  // the previous vertex's next-event estimate, now that its shadows are traced
+    DeferredNee nd;
+    load_nee(r, nd, flags);
+    bool occ[2] = {false, false};
+    for (int l = 0; l < 2; ++l)
+      if (nd.pending[l]) occ[l] = B.shadow[2 * path + l];
+    st.s.L += resolve_deferred(c, nd, occ);
+    flags &= ~(WF_NEE | WF_NEE_SKY | WF_NEE_SUN);
+  }
+  bool continues = false;
+  float extra_w = 0.0f;
+  if (flags & WF_FINISHING) {
+    finished = true;
+  } else {
+    float4 hw = r[R_HIT];
+    Hit h;
+    h.p = ld3(hw);
+    dec_hit(hw.w, h.hit, h.mat);
+    if (MAT != MAT_INVAL) {  // every path of this kernel hit material MAT
+      h.hit = true;
+      h.mat = MAT;
+    }
+    DeferredNee nd;
+    nd.any = false;
+#ifdef HAS_SURFACE
+    SssEntry se;
+    int rv = vertex_step(c, st.s, h, st.vertex, st.g, &nd, &se);
+    if (rv == VERTEX_SSS) {  // the walk stage finishes this vertex
+      store_sss(r, se);
+      st.flags = (flags & ~WF_INDIELE) | (st.s.inDiele ? WF_INDIELE : 0);
+      store_state(r, st);
+      push_sss = true;
+      return;
+    }
+#else
+    int rv = vertex_step(c, st.s, h, st.vertex, st.g, &nd);
+#endif
+    ++st.vertex;
+    finished = rv == VERTEX_DONE || st.vertex > max_bounces(P) || maxc(st.s.thr) < kThroughputEps;
+    continues = !finished;
+    if (nd.any) {
+      flags |= WF_NEE;
+      for (int l = 0; l < 2; ++l)
+        if (nd.pending[l]) {
+          flags |= (l == 0 ? WF_NEE_SKY : WF_NEE_SUN);
+          push_shadow |= 1 << l;
+        }
+      store_nee(r, nd);
+#ifdef DISPERSION_ENABLED
+      extra_w = nd.extra;
+#endif
+      if (finished) flags |= WF_FINISHING;  // one more pass to resolve the shadows
+      finished = false;
+    }
+  }
+  st.s.inDiele ? (flags |= WF_INDIELE) : (flags &= ~WF_INDIELE);
+  if (finished) {
+    finish_path(J, B, path, st.s.L, xyzw, st.g);
+    return;
+  }
+  st.flags = flags;
+  store_state(r, st, extra_w);
+  // rays the path waits for: its continuation (unless it only resolves its shadows) and its
+  // shadow rays; a path with none goes straight to the next shade stage
+  const int nrays = (continues ? 1 : 0) + __popc(push_shadow);
+  if (!continues) r[R_HIT] = make_float4(0.0f, 0.0f, 0.0f, enc_hit(false, MAT_INVAL));
+  B.pend[path] = nrays;
+  push_active = continues;
+  push_direct = nrays == 0;
+  (void)nxt;
+}
+
+// Queue the outcome of a warp's shaded paths for the next iteration, and count finished paths.
+SD_FN void shade_push(const WfBuffers& B, int* cnt, int nxt, int path, bool push_active, int push_shadow,
+                      bool push_direct, bool push_sss, bool finished) {
+  int slot = warp_append(cnt + WF_A + nxt, push_active);
+  if (slot >= 0) pp(B.qa, nxt)[slot] = path;
+  for (int l = 0; l < 2; ++l) {
+    int ss = warp_append(cnt + WF_S + nxt, (push_shadow >> l) & 1);
+    if (ss >= 0) pp(B.qs, nxt)[ss] = 2 * path + l;
+  }
+  // a path with no ray to wait for goes straight to the next shade stage's queue (the other
+  // buffer: this iteration's shade launches are still reading their own)
+  int ds = warp_append(cnt + WF_Q + 4 * nxt, push_direct);
+  if (ds >= 0) pp(B.qshade, nxt)[ds] = path;
+  int ws = warp_append(cnt + WF_SSS, push_sss);
+  if (ws >= 0) B.qsss[ws] = path;
+  unsigned fin = __ballot_sync(WF_FULL, finished);
+  if (fin && (int)(threadIdx.x & 31) == __ffs(fin) - 1) atomicSub(cnt + WF_LEFT, __popc(fin));
+}
+
+// The shade stage over segments [seg_lo, seg_hi] of iteration `it`'s shade queue.
+template <int MAT>
+SD_FN void shade_segments(const JobRec* jobs, const SnellyParams* gparams, const WfBuffers& B, int it, int seg_lo,
+                          int seg_hi) {
   const JobRec& J = jobs[0];
-  const SnellyParams& P = c_params[0];
   int* cnt = B.cnt;
   const int cur = it & 1, nxt = cur ^ 1;
-  const int* qc = cnt + WF_Q + 4 * cur;
-  const int n0 = qc[0], n1 = qc[1], n2 = qc[2], n3 = qc[3];
+  const int* qn = cnt + WF_Q + 4 * cur;
+  const int n0 = seg_lo <= 0 ? qn[0] : 0;
+  const int n1 = seg_lo <= 1 && seg_hi >= 1 ? qn[1] : 0;
+  const int n2 = seg_lo <= 2 && seg_hi >= 2 ? qn[2] : 0;
+  const int n3 = seg_hi >= 3 ? qn[3] : 0;
   const int total = n0 + n1 + n2 + n3;
   if (blockIdx.x == 0 && threadIdx.x == 0) cnt[WF_C + cur] = 0;  // filled again by the next extend stage
-  Scene sc(uniforms_of(0));
+  Scene sc(uniforms_of(B.slot));
   sc.INIT();
   const int stride = gridDim.x * blockDim.x;
   for (int base = blockIdx.x * blockDim.x; base < total; base += stride) {
-    int w = base + threadIdx.x;
-    bool valid = w < total;
+    const int w = base + threadIdx.x;
     int path = 0;
-    bool push_active = false, push_direct = false, finished = false;
+    bool push_active = false, push_direct = false, push_sss = false, finished = false;
     int push_shadow = 0;  // bit 0: sky, bit 1: sun
-    if (valid) {
-      int seg = w < n0 ? 0 : (w < n0 + n1 ? 1 : (w < n0 + n1 + n2 ? 2 : 3));
-      int off = w - (seg == 0 ? 0 : (seg == 1 ? n0 : (seg == 2 ? n0 + n1 : n0 + n1 + n2)));
-      path = B.qshade[cur][seg * B.paths + off];
-      int4 info = B.info[path];
-      float4 cm = B.cmf[path];
-      Ctx c{P, gparams, sc, 0, cm.w, ld3(cm), make_frame(v3(P.sunDir))};
-      PathState s;
-      s.pW = ld3(B.pos[path]);
-      s.rayDir = ld3(B.dir[path]);
-      s.thr = ld_rad(B.thr[path]);
-      s.L = ld_rad(B.rad[path]);
-      float4 mw = B.mis[path];
-      s.misSky = mw.x;
-      s.misSun = mw.y;
-      s.misSph = mw.z;
-      s.atmScatters = info.y;
-      s.inDiele = info.z & WF_INDIELE;
-      uint4 r4 = B.rng[path];
-      Rng g;
-      g.s[0] = r4.x; g.s[1] = r4.y; g.s[2] = r4.z; g.s[3] = r4.w;
-      int flags = info.z;
-      if (flags & WF_NEE) {  // the previous vertex's next-event estimate, now that its shadows are traced
-        DeferredNee nd;
-        nd.org = ld3(B.nee_org[path]);
-        nd.thr = ld_rad(B.nee_thr[path]);
-        nd.extra = ld_rad(B.nee_extra[path]);
-        bool occ[2] = {false, false};
-        for (int l = 0; l < 2; ++l) {
-          nd.pending[l] = flags & (l == 0 ? WF_NEE_SKY : WF_NEE_SUN);
-          if (nd.pending[l]) {
-            float4 dd = B.nee_dir[l][path];
-            nd.dir[l] = ld3(dd);
-            nd.dist[l] = dd.w;
-            nd.c[l] = ld_rad(B.nee_c[l][path]);
-            nd.li[l] = ld_rad(B.nee_li[l][path]);
-            occ[l] = B.shadow[2 * path + l];
-          }
-        }
-        s.L += resolve_deferred(c, nd, occ);
-        flags &= ~(WF_NEE | WF_NEE_SKY | WF_NEE_SUN);
-      }
-      bool continues = false;
-      if (flags & WF_FINISHING) {
-        finished = true;
-      } else {
-        float4 hw = B.hit[path];
-        Hit h;
-        h.p = ld3(hw);
-        dec_hit(hw.w, h.hit, h.mat);
-        int vertex = info.x;
-        DeferredNee nd;
-        nd.any = false;
-        int r = vertex_step(c, s, h, vertex, g, &nd);
-        ++vertex;
-        finished = r == VERTEX_DONE || vertex > max_bounces(P) || maxc(s.thr) < kThroughputEps;
-        continues = !finished;
-        if (nd.any) {
-          flags |= WF_NEE;
-          B.nee_org[path] = st3(nd.org);
-          B.nee_thr[path] = st_rad(nd.thr);
-          B.nee_extra[path] = st_rad(nd.extra);
-          for (int l = 0; l < 2; ++l)
-            if (nd.pending[l]) {
-              flags |= (l == 0 ? WF_NEE_SKY : WF_NEE_SUN);
-              B.nee_dir[l][path] = st3(nd.dir[l], nd.dist[l]);
-              B.nee_c[l][path] = st_rad(nd.c[l]);
-              B.nee_li[l][path] = st_rad(nd.li[l]);
-              push_shadow |= 1 << l;
-            }
-          if (finished) flags |= WF_FINISHING;  // one more pass to resolve the shadows
-          finished = false;
-        }
-        info.x = vertex;
-      }
-      s.inDiele ? (flags |= WF_INDIELE) : (flags &= ~WF_INDIELE);
-      if (finished) {
-        finish_path(J, B, path, s.L, ld3(B.xyzw[path]), g);
-      } else {
-        B.pos[path] = st3(s.pW);
-        B.dir[path] = st3(s.rayDir);
-        B.thr[path] = st_rad(s.thr);
-        B.rad[path] = st_rad(s.L);
-        B.mis[path] = make_float4(s.misSky, s.misSun, s.misSph, 0.0f);
-        B.info[path] = make_int4(info.x, s.atmScatters, flags, 0);
-        B.rng[path] = make_uint4(g.s[0], g.s[1], g.s[2], g.s[3]);
-        // rays the path waits for: its continuation (unless it only resolves its shadows) and
-        // its shadow rays; a path with none goes straight to the next shade stage
-        const int nrays = (continues ? 1 : 0) + __popc(push_shadow);
-        if (!continues) B.hit[path] = make_float4(0.0f, 0.0f, 0.0f, enc_hit(false, MAT_INVAL));
-        B.pend[path] = nrays;
-        push_active = continues;
-        push_direct = nrays == 0;
-      }
+    if (w < total) {
+      const int seg = w < n0 ? 0 : (w < n0 + n1 ? 1 : (w < n0 + n1 + n2 ? 2 : 3));
+      const int off = w - (seg == 0 ? 0 : (seg == 1 ? n0 : (seg == 2 ? n0 + n1 : n0 + n1 + n2)));
+      path = pp(B.qshade, cur)[seg * B.paths + off];
+      shade_path<MAT>(J, gparams, B, sc, path, nxt, push_active, push_shadow, push_direct, push_sss, finished);
     }
-    int slot = warp_append(cnt + WF_A + nxt, push_active);
-    if (slot >= 0) B.qa[nxt][slot] = path;
-    for (int l = 0; l < 2; ++l) {
-      int ss = warp_append(cnt + WF_S + nxt, (push_shadow >> l) & 1);
-      if (ss >= 0) B.qs[nxt][ss] = 2 * path + l;
-    }
-    // a path with no ray to wait for goes straight to the next shade stage's queue (the other
-    // buffer: this launch is still reading its own)
-    int ds = warp_append(cnt + WF_Q + 4 * nxt, push_direct);
-    if (ds >= 0) B.qshade[nxt][ds] = path;
-    unsigned fin = __ballot_sync(WF_FULL, finished);
-    if (fin && (int)(threadIdx.x & 31) == __ffs(fin) - 1) atomicSub(cnt + WF_LEFT, __popc(fin));
+    shade_push(B, cnt, nxt, path, push_active, push_shadow, push_direct, push_sss, finished);
   }
 }
+
+}  // namespace sdev
+
+// Shade every path the extend stage of iteration `it` queued (all four segments in one launch).
+extern "C" __global__ void __launch_bounds__(SNELLY_BLOCK, SNELLY_SHADE_MIN_BLOCKS) snelly_wf_shade(
+    const JobRec* __restrict__ jobs, const SnellyParams* __restrict__ gparams, WfBuffers B, int it) {
+  sdev::shade_segments<sdev::MAT_INVAL>(jobs, gparams, B, it, 0, 3);
+}
+
+// The same stage as one launch per queue segment, each compiled for its material only (fewer
+// registers and no material dispatch): misses and finishing paths, surface, metal, dielectric.
+// The host runs them back to back in place of snelly_wf_shade when the autotuner prefers it.
+#ifndef SNELLY_SHADE_SEG_MIN_BLOCKS
+#define SNELLY_SHADE_SEG_MIN_BLOCKS 4
+#endif
+extern "C" __global__ void __launch_bounds__(SNELLY_BLOCK, SNELLY_SHADE_SEG_MIN_BLOCKS) snelly_wf_shade_miss(
+    const JobRec* __restrict__ jobs, const SnellyParams* __restrict__ gparams, WfBuffers B, int it) {
+  sdev::shade_segments<sdev::MAT_INVAL>(jobs, gparams, B, it, 0, 0);
+}
+#ifdef HAS_SURFACE
+extern "C" __global__ void __launch_bounds__(SNELLY_BLOCK, SNELLY_SHADE_SEG_MIN_BLOCKS) snelly_wf_shade_surface(
+    const JobRec* __restrict__ jobs, const SnellyParams* __restrict__ gparams, WfBuffers B, int it) {
+  sdev::shade_segments<sdev::MAT_SURFA>(jobs, gparams, B, it, 1, 1);
+}
+#endif
+#ifdef HAS_METAL
+extern "C" __global__ void __launch_bounds__(SNELLY_BLOCK, SNELLY_SHADE_SEG_MIN_BLOCKS) snelly_wf_shade_metal(
+    const JobRec* __restrict__ jobs, const SnellyParams* __restrict__ gparams, WfBuffers B, int it) {
+  sdev::shade_segments<sdev::MAT_METAL>(jobs, gparams, B, it, 2, 2);
+}
+#endif
+#ifdef HAS_DIELECTRIC
+extern "C" __global__ void __launch_bounds__(SNELLY_BLOCK, SNELLY_SHADE_SEG_MIN_BLOCKS) snelly_wf_shade_dielectric(
+    const JobRec* __restrict__ jobs, const SnellyParams* __restrict__ gparams, WfBuffers B, int it) {
+  sdev::shade_segments<sdev::MAT_DIELE>(jobs, gparams, B, it, 3, 3);
+}
+#endif
+
+#ifdef HAS_SURFACE
+// The subsurface-walk stage of iteration `it` (PT:1464-1593, 1866-1918): the surface vertices the
+// shade stage handed over walk inside SDF_SURFACE to an exit point, take its direct light and
+// continue from there. One thread per path over the walk queue, so a warp holds only walking
+// paths; the walk's own marches and the exit's shadow rays are traced inline.
+extern "C" __global__ void __launch_bounds__(SNELLY_BLOCK, SNELLY_SHADE_MIN_BLOCKS) snelly_wf_sss(
+    const JobRec* __restrict__ jobs, const SnellyParams* __restrict__ gparams, WfBuffers B, int it) {
+  using namespace sdev;
+  const JobRec& J = jobs[0];
+  const SnellyParams& P = c_params[B.slot];
+  int* cnt = B.cnt;
+  const int nxt = (it & 1) ^ 1;
+  const int total = cnt[WF_SSS];
+  Scene sc(uniforms_of(B.slot));
+  sc.INIT();
+  const int stride = gridDim.x * blockDim.x;
+  for (int base = blockIdx.x * blockDim.x; base < total; base += stride) {
+    const int w = base + threadIdx.x;
+    int path = 0;
+    bool push_active = false, finished = false;
+    if (w < total) {
+      path = B.qsss[w];
+      float4* r = rec_of(B.rec, path);
+      WfState st;
+      load_state(r, st);
+      Ctx c{P, gparams, sc, B.slot, 0.0f, vec3(0.0f), make_frame(v3(P.sunDir))};
+      const vec3 xyzw = wavelength_at(c, st.w);
+      const SssEntry e = load_sss(r);
+      int rv = sss_step(c, st.s, e, st.g);
+      ++st.vertex;
+      finished = rv == VERTEX_DONE || st.vertex > max_bounces(P) || maxc(st.s.thr) < kThroughputEps;
+      if (finished) {
+        finish_path(J, B, path, st.s.L, xyzw, st.g);
+      } else {
+        st.s.inDiele ? (st.flags |= WF_INDIELE) : (st.flags &= ~WF_INDIELE);
+        store_state(r, st);
+        B.pend[path] = 1;
+        push_active = true;
+      }
+    }
+    shade_push(B, cnt, nxt, path, push_active, 0, false, false, finished);
+  }
+}
+#endif

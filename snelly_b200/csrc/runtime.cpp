@@ -147,7 +147,12 @@ int assemble_scene(const std::string& glsl, const snelly_scene_opts& o, SceneSou
   if (r.has_surface) d << "#define HAS_SURFACE\n";
   if (r.has_metal) d << "#define HAS_METAL\n";
   if (r.has_dielectric) d << "#define HAS_DIELECTRIC\n";
-  if (o.has_atmosphere) d << "#define HAS_ATMOSPHERE\n";
+  // A scene that defines VOLUME_EXTINCTION itself has a heterogeneous medium in the atmosphere's
+  // box (an extension of this build: the reference declares the hook but never calls it), which
+  // takes the place of the homogeneous atmosphere.
+  const bool hetero = glsl.find("VOLUME_EXTINCTION(") != std::string::npos;
+  if (hetero) d << "#define HAS_HETERO_VOLUME\n";
+  else if (o.has_atmosphere) d << "#define HAS_ATMOSPHERE\n";
   if (o.has_fog) d << "#define HAS_FOG\n";
   if (r.has_volume_emission) d << "#define HAS_VOLUME_EMISSION\n";
   d << "#define HAS_GEOMETRY\n";
@@ -193,8 +198,10 @@ static uint64_t fnv1a(const std::string& s, uint64_t h = 1469598103934665603ull)
 
 static std::vector<std::string> nvrtc_options(const std::string& kernel_dir, const std::string& csrc_dir,
                                               const std::string& include_dir, int math_mode) {
+  // --ptxas-options=-v: the log lists registers, spills and shared memory per kernel
   std::vector<std::string> opts = {"--gpu-architecture=sm_100a", "-std=c++17", "-default-device", "-lineinfo",
-                                   "-diag-suppress=550,177", "-I" + kernel_dir, "-I" + csrc_dir, "-I" + include_dir};
+                                   "-diag-suppress=550,177", "--ptxas-options=-v", "-I" + kernel_dir, "-I" + csrc_dir,
+                                   "-I" + include_dir};
   if (math_mode == SNELLY_MATH_STRICT) {
     opts.push_back("--fmad=false");
     opts.push_back("--prec-div=true");
@@ -202,6 +209,13 @@ static std::vector<std::string> nvrtc_options(const std::string& kernel_dir, con
     opts.push_back("--ftz=false");
   } else {
     opts.push_back("--use_fast_math");
+  }
+  // extra compiler options, space-separated (e.g. -DWF_CHUNK=4 or --ptxas-options=-v); they are
+  // part of the module cache key
+  if (const char* x = getenv("SNELLY_NVRTC_EXTRA")) {
+    std::istringstream in(x);
+    std::string o;
+    while (in >> o) opts.push_back(o);
   }
   return opts;
 }
@@ -239,12 +253,15 @@ static std::string read_file(const std::string& path) {
   return ss.str();
 }
 
-int Context::compile_module(const std::string& src, int math_mode, std::shared_ptr<Module>* out, std::string* log) {
-  std::vector<std::string> opts = nvrtc_options(kernel_dir, csrc_dir, include_dir, math_mode);
+// Cache key of a module: its program source, the compiler options but the include paths, every source file the program
+// includes (all of the kernel directory, the GLSL compatibility header and its swizzle table, the
+// parameter block) and the NVRTC version.
+static std::string module_key(const std::string& src, const std::vector<std::string>& opts,
+                              const std::string& kernel_dir, const std::string& csrc_dir,
+                              const std::string& include_dir) {
   std::string key_text = src;
-  for (auto& o : opts) key_text += "\n" + o;
-  // the cache key covers every source the program includes (all of the kernel directory, the
-  // GLSL compatibility header and its swizzle table, the parameter block) and the compiler version
+  for (auto& o : opts)  // include paths differ between machines; the files they hold are hashed below
+    if (o.compare(0, 2, "-I") != 0) key_text += "\n" + o;
   std::vector<std::string> kfiles;
   if (DIR* d = opendir(kernel_dir.c_str())) {
     while (dirent* e = readdir(d))
@@ -258,7 +275,23 @@ int Context::compile_module(const std::string& src, int math_mode, std::shared_p
   int nv_major = 0, nv_minor = 0;
   nvrtcVersion(&nv_major, &nv_minor);
   key_text += "\nnvrtc " + std::to_string(nv_major) + "." + std::to_string(nv_minor);
-  std::string key = hex64(fnv1a(key_text));
+  return hex64(fnv1a(key_text));
+}
+
+// Store a compiled module under its key: written whole to a temporary file, then renamed.
+static void cache_store(const std::string& cache_path, const std::vector<char>& cubin) {
+  if (cache_path.empty()) return;
+  std::string tmp = cache_path + ".tmp" + std::to_string((long)getpid());
+  std::ofstream o(tmp, std::ios::binary);
+  o.write(cubin.data(), (std::streamsize)cubin.size());
+  o.close();
+  if (o.good()) rename(tmp.c_str(), cache_path.c_str());
+  else unlink(tmp.c_str());
+}
+
+int Context::compile_module(const std::string& src, int math_mode, std::shared_ptr<Module>* out, std::string* log) {
+  std::vector<std::string> opts = nvrtc_options(kernel_dir, csrc_dir, include_dir, math_mode);
+  const std::string key = module_key(src, opts, kernel_dir, csrc_dir, include_dir);
   auto it = module_cache.find(key);
   if (it != module_cache.end()) {
     *out = it->second;
@@ -279,14 +312,7 @@ int Context::compile_module(const std::string& src, int math_mode, std::shared_p
       int rc = nvrtc_cubin(src, opts, &cubin, log);
       if (rc) return rc;
       from_cache = false;
-      if (!cache_path.empty()) {  // written whole to a temporary file, then renamed into place
-        std::string tmp = cache_path + ".tmp" + std::to_string((long)getpid());
-        std::ofstream o(tmp, std::ios::binary);
-        o.write(cubin.data(), (std::streamsize)cubin.size());
-        o.close();
-        if (o.good()) rename(tmp.c_str(), cache_path.c_str());
-        else unlink(tmp.c_str());
-      }
+      cache_store(cache_path, cubin);
     }
     cudaError_t lr = cudaLibraryLoadData(&m->lib, cubin.data(), nullptr, nullptr, 0, nullptr, nullptr, 0);
     if (lr == cudaSuccess) break;
@@ -306,8 +332,11 @@ int Context::compile_module(const std::string& src, int math_mode, std::shared_p
              {"snelly_wf_generate", &m->f_wf_generate, false},
              {"snelly_wf_extend", &m->f_wf_extend, false},
              {"snelly_wf_shade", &m->f_wf_shade, false},
-             {"snelly_wf_shadow", &m->f_wf_shadow, false},
-             {"snelly_wf_accumulate", &m->f_wf_accumulate, false},
+             {"snelly_wf_shade_miss", &m->f_wf_shade_seg[0], false},
+             {"snelly_wf_shade_surface", &m->f_wf_shade_seg[1], false},
+             {"snelly_wf_shade_metal", &m->f_wf_shade_seg[2], false},
+             {"snelly_wf_shade_dielectric", &m->f_wf_shade_seg[3], false},
+             {"snelly_wf_sss", &m->f_wf_sss, false},
              {"snelly_firsthit", &m->f_firsthit, false},
              {"snelly_ptsimple", &m->f_ptsimple, false}};
   for (auto& f : fns) {
@@ -325,8 +354,18 @@ int Context::compile_module(const std::string& src, int math_mode, std::shared_p
       m->extend_blocks_per_sm = nb;
     else
       cudaGetLastError();
+    nb = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, (const void*)m->f_wf_extend, 64, 0) == cudaSuccess && nb > 0)
+      m->extend_blocks_per_sm64 = nb;
+    else
+      cudaGetLastError();
   }
   size_t sz = 0;
+  if (m->f_wf_generate) {  // the path-record size the wavefront kernels were compiled for
+    int* rp = nullptr;
+    RT_TRY(cudaLibraryGetGlobal((void**)&rp, &sz, m->lib, "snelly_wf_rec_f4"));
+    RT_TRY(cudaMemcpy(&m->wf_rec_f4, rp, sizeof(int), cudaMemcpyDeviceToHost));
+  }
   RT_TRY(cudaLibraryGetGlobal((void**)&m->c_params, &sz, m->lib, "c_params"));
   RT_TRY(cudaLibraryGetGlobal((void**)&m->c_uniforms, &m->c_uniforms_bytes, m->lib, "c_uniforms"));
   m->slot_uniform_bytes = m->c_uniforms_bytes / SNELLY_MAX_BATCH;
@@ -413,17 +452,31 @@ int Context::enqueue_frames(Job& j, int frames) {
   return SNELLY_OK;
 }
 
-// Batched frames (see snelly_advance_batch). Jobs are grouped by module; each group gets a lane
-// (stream + device tables); per frame, one launch covers the group's jobs that still need frames.
+// Batched frames (see snelly_advance_batch). Jobs the autotuner gave the wavefront run as pixel
+// ranges on their own streams, all of them at once (enqueue_wavefront). The others are grouped by
+// module; each group gets a lane (stream + device tables); per frame, one path-per-thread launch
+// covers the group's jobs that still need frames. Lanes and wavefront ranges run concurrently; a
+// module's wavefront jobs take over its constant-memory slots after its lane is done.
 int Context::advance_batch(const std::vector<Job*>& js, const std::vector<int>& frames) {
   std::map<Module*, std::vector<size_t>> groups;
-  for (size_t k = 0; k < js.size(); ++k)
-    if (frames[k] > 0) groups[js[k]->module].push_back(k);
+  std::vector<Job*> wjobs;
+  std::vector<int> wframes;
+  for (size_t k = 0; k < js.size(); ++k) {
+    if (frames[k] <= 0) continue;
+    Job& j = *js[k];
+    if (j.desc.mode == SNELLY_MODE_PT && j.kernel_mode == SNELLY_KERNEL_WAVEFRONT && j.module->f_wf_generate) {
+      wjobs.push_back(&j);
+      wframes.push_back(frames[k]);
+    } else {
+      groups[j.module].push_back(k);
+    }
+  }
   // all earlier work on the main stream (job seeding, single-job frames) comes first
   cudaEvent_t start;
   RT_TRY(cudaEventCreateWithFlags(&start, cudaEventDisableTiming));
   RT_TRY(cudaEventRecord(start, stream));
   size_t lane_idx = 0;
+  std::map<Module*, cudaEvent_t> after;
   for (auto& g : groups) {
     Module& m = *g.first;
     std::vector<size_t>& idx = g.second;
@@ -507,10 +560,30 @@ int Context::advance_batch(const std::vector<Job*>& js, const std::vector<int>& 
     }
     BatchLane& L = lanes[lane_idx];
     RT_TRY(cudaEventRecord(L.done, L.stream));
-    RT_TRY(cudaStreamWaitEvent(stream, L.done, 0));
+    after[&m] = L.done;
     ++lane_idx;
   }
-  // later main-stream work (and every job's completion event) is ordered after all lanes
+  // the wavefront jobs, overlapping the lanes (a module's after its lane, for the slots)
+  int rc = enqueue_wavefront(wjobs, wframes, after);
+  if (rc) {
+    cudaEventDestroy(start);
+    return rc;
+  }
+  for (size_t l = 0; l < lane_idx; ++l) RT_TRY(cudaStreamWaitEvent(stream, lanes[l].done, 0));
+  for (size_t q = 0; q < wjobs.size(); ++q) {  // each wavefront job's mean image
+    Job& j = *wjobs[q];
+    void* tables = j.tables.ptr;
+    void* bstart = (char*)j.tables.ptr + 128;
+    int one = 1;
+    void* rargs[] = {&tables, &bstart, &one};
+    if (j.read_pending) RT_TRY(cudaStreamWaitEvent(stream, j.read_done, 0));  // `out` is being copied out
+    if ((rc = launch(j.module->f_resolve, j.blocks, SNELLY_BLOCK, rargs))) {
+      cudaEventDestroy(start);
+      return rc;
+    }
+    j.frames_enqueued += wframes[q];
+  }
+  // later main-stream work (and every job's completion event) is ordered after all of it
   for (size_t k = 0; k < js.size(); ++k) RT_TRY(cudaEventRecord(js[k]->done, stream));
   cudaEventDestroy(start);
   return SNELLY_OK;
@@ -535,17 +608,12 @@ Context::~Context() {
   release(stats_scratch);
   if (flush_buf) cudaFree(flush_buf);
   if (poll_host) cudaFreeHost(poll_host);
-  for (auto& row : poll_done)
-    for (auto& e : row)
-      if (e) cudaEventDestroy(e);
-  for (int k = 1; k < SNELLY_WF_MAX_PARTS; ++k)
-    if (wf_streams[k]) {
-      cudaStreamSynchronize(wf_streams[k]);
-      cudaStreamDestroy(wf_streams[k]);
-    }
+  for (auto& e : wf_events) cudaEventDestroy(e);
+  for (auto& st : wf_pool) {
+    cudaStreamSynchronize(st);
+    cudaStreamDestroy(st);
+  }
   if (wf_fork) cudaEventDestroy(wf_fork);
-  for (auto& e : wf_join)
-    if (e) cudaEventDestroy(e);
   for (auto& kv : module_cache) cudaLibraryUnload(kv.second->lib);
   if (copy_stream) cudaStreamDestroy(copy_stream);
   cudaStreamDestroy(stream);
@@ -609,9 +677,24 @@ int snelly_init(snelly_ctx** out, int device, size_t budget) {
   c->include_dir = env ? std::string(env) + "/../../include" : dir + "/../include";
   if (!file_exists(c->kernel_dir + "/pt_kernels.cu"))
     return fail(SNELLY_EINVAL, "kernel sources not found under " + c->kernel_dir);
-  if (const char* dr = getenv("SNELLY_WF_DRAIN")) c->wf_drain_steps = atoi(dr);  // 0: never park rays
   if (const char* pi = getenv("SNELLY_WF_PARK_ITERS")) c->wf_park_iters = atoi(pi);
-  if (const char* sp = getenv("SNELLY_WF_SPLIT")) c->wf_split = std::max(1, std::min(atoi(sp), SNELLY_WF_MAX_PARTS));
+  {  // wavefront defaults from the environment; those given are not tuned
+    WfConfig& d = c->wf_default;
+    struct {
+      const char* name;
+      int* field;
+      int lo, hi;
+    } knobs[] = {{"SNELLY_WF_SPLIT", &d.parts, 1, SNELLY_WF_MAX_PARTS}, {"SNELLY_WF_SHADE_SPLIT", &d.shade_split, 0, 1},
+                 {"SNELLY_WF_DRAIN", &d.drain, 0, 4096},  // 0: never park rays
+                 {"SNELLY_WF_CHUNK", &d.chunk, 1, 64}, {"SNELLY_WF_GRAB", &d.grab, 1, 1024},
+                 {"SNELLY_WF_REFILL", &d.refill, 1, 32}, {"SNELLY_WF_BLOCK", &d.block, 64, 128}};
+    for (unsigned k = 0; k < sizeof knobs / sizeof knobs[0]; ++k)
+      if (const char* v = getenv(knobs[k].name)) {
+        *knobs[k].field = std::max(knobs[k].lo, std::min(atoi(v), knobs[k].hi));
+        c->wf_fixed |= 1u << k;
+      }
+    d.block = d.block < 128 ? 64 : 128;
+  }
   const char* cdir = getenv("SNELLY_CACHE_DIR");
   c->cache_dir = cdir ? std::string(cdir) : dir + "/_build/kcache";
   mkdir((dir + "/_build").c_str(), 0755);
@@ -849,6 +932,7 @@ static int start_job(Context& c, uint64_t scene_id, const snelly_render_desc* de
   j.kernel_mode = SNELLY_KERNEL_MEGA;
   if (desc->mode == SNELLY_MODE_PT && s.kernel_mode != SNELLY_KERNEL_MEGA && j.module->f_wf_generate)
     j.kernel_mode = s.kernel_mode;
+  j.wfc = c.wf_default;
   if (j.kernel_mode != SNELLY_KERNEL_MEGA && (rc = c.alloc_wavefront(j))) return bail(rc);
   if (j.kernel_mode == SNELLY_KERNEL_AUTO && (rc = c.autotune(j))) return bail(rc);
   if (rng) {
@@ -1074,6 +1158,18 @@ int snelly_job_kernel(snelly_ctx* ctx, uint64_t job_id, int* kernel_mode) {
   return SNELLY_OK;
 }
 
+int snelly_job_wavefront_config(snelly_ctx* ctx, uint64_t job_id, int* out) {
+  if (!ctx || !out) return fail(SNELLY_EINVAL, "null argument to snelly_job_wavefront_config");
+  Context& c = *ctx->c;
+  std::lock_guard<std::mutex> lk(c.mu);
+  auto it = c.jobs.find(job_id);
+  if (it == c.jobs.end()) return fail(SNELLY_ENOTFOUND, "unknown job id");
+  const WfConfig& w = it->second.wfc;
+  const int v[SNELLY_WF_CONFIG_FIELDS] = {it->second.wf_parts, w.shade_split, w.drain, w.chunk, w.grab, w.refill, w.block};
+  for (int k = 0; k < SNELLY_WF_CONFIG_FIELDS; ++k) out[k] = v[k];
+  return SNELLY_OK;
+}
+
 int snelly_job_status(snelly_ctx* ctx, uint64_t job_id, int* enq, int* done) {
   if (!ctx) return fail(SNELLY_EINVAL, "ctx is null");
   Context& c = *ctx->c;
@@ -1152,8 +1248,15 @@ int snelly_compile_check(const char* glsl, const snelly_scene_opts* opts, char* 
   std::vector<char> cubin;
   std::string lg;
   std::vector<std::string> nopts = nvrtc_options(csrc + "/kernels", csrc, inc, opts->math_mode);
-  nopts.push_back("--ptxas-options=-v");  // the log then lists registers, spills and shared memory per kernel
-  rc = nvrtc_cubin(program_source(ss), nopts, &cubin, &lg);
+  const std::string src = program_source(ss);
+  rc = nvrtc_cubin(src, nopts, &cubin, &lg);
+  if (!rc) {  // into the module cache, where a context on a GPU machine finds it
+    const char* cdir = getenv("SNELLY_CACHE_DIR");
+    std::string cache = cdir ? std::string(cdir) : dir + "/_build/kcache";
+    mkdir((dir + "/_build").c_str(), 0755);
+    if (mkdir(cache.c_str(), 0755) == 0 || file_exists(cache))
+      cache_store(cache + "/" + module_key(src, nopts, csrc + "/kernels", csrc, inc) + ".cubin", cubin);
+  }
   if (log && log_cap) snprintf(log, log_cap, "%s", rc ? t_last_error.c_str() : lg.c_str());
   if (cubin_bytes) *cubin_bytes = cubin.size();
   return rc;

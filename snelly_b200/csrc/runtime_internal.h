@@ -53,13 +53,29 @@ struct Module {
   std::string key;
   cudaLibrary_t lib = nullptr;
   cudaKernel_t f_seed = nullptr, f_frame_mega = nullptr, f_resolve = nullptr;
-  cudaKernel_t f_wf_generate = nullptr, f_wf_extend = nullptr, f_wf_shade = nullptr, f_wf_shadow = nullptr,
-               f_wf_accumulate = nullptr;
+  cudaKernel_t f_wf_generate = nullptr, f_wf_extend = nullptr, f_wf_shade = nullptr, f_wf_sss = nullptr;
+  // the shade stage split by queue segment: misses/finishing, surface, metal, dielectric (null
+  // for a material the scene does not have)
+  cudaKernel_t f_wf_shade_seg[4] = {nullptr, nullptr, nullptr, nullptr};
+  int wf_rec_f4 = 0;  // float4 slots of the module's wavefront path record
   cudaKernel_t f_firsthit = nullptr, f_ptsimple = nullptr;
-  int extend_blocks_per_sm = 8;  // resident blocks of the persistent extend stage (occupancy query)
+  int extend_blocks_per_sm = 8;  // resident 128-thread blocks of the persistent extend stage (occupancy query)
+  int extend_blocks_per_sm64 = 16;  // the same for 64-thread blocks
   char* c_params = nullptr;  // device addresses of the constant banks
   char* c_uniforms = nullptr;
   size_t c_uniforms_bytes = 0, slot_uniform_bytes = 0;
+};
+
+// Launch configuration of a wavefront job: chosen per (scene module, image-size class) by the
+// autotuner, or the context's defaults.
+struct WfConfig {
+  int parts = 3;        // concurrent pixel ranges (one per 65,536 pixels at most)
+  int shade_split = 0;  // the shade stage as one launch per material segment
+  int drain = 32;       // steps an extend warp marches once its work runs out before parking (0: never)
+  int chunk = 8;        // sphere-tracing steps between refills of idle lanes
+  int grab = 32;        // work items a warp claims from the work head at a time
+  int refill = 4;       // idle lanes of a warp that trigger a refill
+  int block = 128;      // threads per block of the extend and shade launches (64 or 128)
 };
 
 struct Scene {
@@ -90,6 +106,7 @@ struct Job {
   DevBuf wf;  // wavefront path state and queues
   WfBuffers wfb[SNELLY_WF_MAX_PARTS]{};  // one set per pixel range, each run on its own stream
   int wf_parts = 0;
+  WfConfig wfc;  // its launch configuration
   int blocks = 0;
   int kernel_mode = SNELLY_KERNEL_MEGA;  // the integrator this job's frames run (after tuning)
   int pick_at = 0;           // a one-pixel pick job (snelly_pick)
@@ -124,14 +141,22 @@ struct Context {
   uint64_t launches = 0;
   std::string csrc_dir, kernel_dir, include_dir, cache_dir;
   std::vector<BatchLane> lanes;  // batch streams (created on first use)
-  std::map<std::string, int> tuned;  // autotuner decisions: (module, image-size class) -> integrator
-  int wf_drain_steps = 32;           // steps an extend warp marches once its work runs out (SNELLY_WF_DRAIN)
+  struct Tuned {
+    int kernel;
+    WfConfig cfg;
+  };
+  std::map<std::string, Tuned> tuned;  // autotuner decisions per (module, image-size class)
+  // Wavefront defaults; a field set from the environment (SNELLY_WF_SPLIT, SNELLY_WF_DRAIN,
+  // SNELLY_WF_SHADE_SPLIT, SNELLY_WF_CHUNK, SNELLY_WF_GRAB, SNELLY_WF_REFILL, SNELLY_WF_BLOCK) is
+  // also kept fixed by the autotuner.
+  WfConfig wf_default;
+  unsigned wf_fixed = 0;             // bit per WfConfig field, in declaration order
   int wf_park_iters = -1;            // iterations that may park rays; -1: 3 x (max_bounces + 2) (SNELLY_WF_PARK_ITERS)
-  int wf_split = 3;                  // wavefront pixel ranges run concurrently (SNELLY_WF_SPLIT)
-  int* poll_host = nullptr;          // pinned words the wavefront's paths-left reads land in
-  cudaEvent_t poll_done[2][SNELLY_WF_MAX_PARTS] = {};
-  cudaStream_t wf_streams[SNELLY_WF_MAX_PARTS] = {};  // [0] is the context stream
-  cudaEvent_t wf_fork = nullptr, wf_join[SNELLY_WF_MAX_PARTS] = {};
+  int* poll_host = nullptr;          // pinned words the wavefront's paths-left reads land in (2 per part)
+  size_t poll_cap = 0;
+  std::vector<cudaStream_t> wf_pool;  // one stream per concurrently running wavefront part
+  std::vector<cudaEvent_t> wf_events;  // per part: two progress reads and a join
+  cudaEvent_t wf_fork = nullptr;
   DevBuf stats_scratch;          // image-statistics partial sums
   void* static_stats_scratch = nullptr;  // device address of the allocation-free statistics scratch
   void* flush_buf = nullptr;     // L2 eviction buffer of snelly_flush_l2 (freed with the context)
@@ -151,7 +176,10 @@ struct Context {
   int alloc_wavefront(Job& j);
   void release_wavefront(Job& j);
   int enqueue_wavefront_frames(Job& j, int frames);
+  int enqueue_wavefront(const std::vector<Job*>& js, const std::vector<int>& frames,
+                        const std::map<Module*, cudaEvent_t>& after);
   int autotune(Job& j);
+  int time_frames(Job& j, int kernel, float* ms_per_frame);
 };
 
 int assemble_scene(const std::string& glsl, const snelly_scene_opts& o, SceneSource* out);

@@ -2,26 +2,29 @@
 // the per-path state and queues in HBM, and the stage launches of one frame on one or more
 // concurrent streams.
 #include <algorithm>
+#include <cmath>
 #include <thread>
 
 #include "runtime_internal.h"
 
 namespace snelly {
 
-// The job's pixels are split into up to wf_split contiguous ranges ("parts"), each with its own
+// The job's pixels are split into up to wfc.parts contiguous ranges ("parts"), each with its own
 // path state, queues and counters, whose stages run on their own streams: while one part's
 // extend launch drains (its last, longest rays on few lanes) or its shade stage runs, the other
 // parts' launches fill the SMs it leaves idle. A path's computation does not depend on its part.
 int Context::alloc_wavefront(Job& j) {
   if (j.scene->opts.max_samples_per_frame != 1) return SNELLY_OK;  // served by the per-pixel kernel
   const size_t P = (size_t)j.desc.width * j.desc.height;
-  int parts = std::max(1, std::min(wf_split, SNELLY_WF_MAX_PARTS));
-  if (P < (size_t)parts * 65536) parts = 1;  // small images: one part keeps each launch full
-  // per path: 17 float4 arrays + info + rng + parked-ray state (3 per path), shadow flags, pending
-  // count, int queues (2 active, 2 x 2 shadow, 2 x 3 parked, 2 x 4 shade); per part: counters
-  // and the 256-byte alignment of its 31 sub-buffers
-  size_t bytes = (19 * 16 + 3 * 16 + 2 + 4 + (2 + 2 * 2 + 2 * 3 + 2 * 4) * 4) * P +
-                 (size_t)parts * (4 * WF_COUNTERS + 32 * 256);
+  int parts = std::max(1, std::min(j.wfc.parts, SNELLY_WF_MAX_PARTS));
+  while (parts > 1 && P < (size_t)parts * 65536) --parts;  // at least 65,536 pixels per range keep each launch full
+  const int rec_f4 = j.module->wf_rec_f4;
+  if (rec_f4 <= 0) return fail(SNELLY_EDEVICE, "module has no wavefront record layout");
+  // per path: the record, parked-ray state (3 rays), shadow flags, pending count, int queues
+  // (2 active, 2 x 2 shadow, 2 x 3 parked, 2 x 4 shade, 1 subsurface walk); per part: counters
+  // and the 256-byte alignment of its 15 sub-buffers
+  size_t bytes = ((size_t)rec_f4 * 16 + 3 * 16 + 2 + 4 + (2 + 2 * 2 + 2 * 3 + 2 * 4 + 1) * 4) * P +
+                 (size_t)parts * (4 * WF_COUNTERS + 16 * 256);
   int rc = alloc(j.wf, bytes);
   if (rc) return rc;
   char* p = (char*)j.wf.ptr;
@@ -35,12 +38,8 @@ int Context::alloc_wavefront(Job& j) {
     const size_t Pk = P / parts + ((size_t)k < P % parts ? 1 : 0);
     const size_t f4 = 16 * Pk;
     WfBuffers& B = j.wfb[k];
-    float4** f4s[] = {&B.pos, &B.dir, &B.thr, &B.rad, &B.cmf, &B.mis, &B.xyzw, &B.hit, &B.nee_org, &B.nee_thr,
-                      &B.nee_extra, &B.nee_dir[0], &B.nee_dir[1], &B.nee_c[0], &B.nee_c[1], &B.nee_li[0],
-                      &B.nee_li[1]};
-    for (float4** q : f4s) *q = (float4*)take(f4);
-    B.info = (int4*)take(f4);
-    B.rng = (uint4*)take(f4);
+    B.rec = (float4*)take((size_t)rec_f4 * f4);
+    B.rec_f4 = rec_f4;
     B.mt = (float4*)take(3 * f4);
     B.pend = (int*)take(4 * Pk);
     B.qc[0] = (int*)take(12 * Pk);
@@ -51,6 +50,7 @@ int Context::alloc_wavefront(Job& j) {
     B.qs[1] = (int*)take(8 * Pk);
     B.qshade[0] = (int*)take(16 * Pk);
     B.qshade[1] = (int*)take(16 * Pk);
+    B.qsss = (int*)take(4 * Pk);
     B.cnt = (int*)take(4 * WF_COUNTERS);
     B.shadow = (unsigned char*)take(2 * Pk);
     B.paths = (int)Pk;
@@ -58,6 +58,7 @@ int Context::alloc_wavefront(Job& j) {
     begin += Pk;
   }
   j.wf_parts = parts;
+  j.wfc.parts = parts;
   if ((size_t)(p - (char*)j.wf.ptr) > bytes) return fail(SNELLY_EDEVICE, "wavefront buffer layout overflow");
   return SNELLY_OK;
 }
@@ -69,132 +70,280 @@ void Context::release_wavefront(Job& j) {
 }
 
 int Context::enqueue_wavefront_frames(Job& j, int frames) {
-  Module& m = *j.module;
-  if (!j.wf.ptr || j.wf_parts < 1 || !m.f_wf_generate || !m.f_wf_extend || !m.f_wf_shade)
-    return fail(SNELLY_EINVAL, "wavefront integrator not available for this job");
-  if (frames <= 0) return SNELLY_OK;
-  const int parts = j.wf_parts;
-  // streams and events, created on first use; part 0 runs on the context stream
-  wf_streams[0] = stream;
-  for (int k = 1; k < parts; ++k)
-    if (!wf_streams[k]) RT_TRY(cudaStreamCreateWithFlags(&wf_streams[k], cudaStreamNonBlocking));
+  std::vector<Job*> js{&j};
+  std::vector<int> fs{frames};
+  return enqueue_wavefront(js, fs, {});
+}
+
+// The wavefront frames of several jobs at once. Every job's pixel ranges ("parts") get their own
+// stream; a job's parameters and scene uniforms go to its own constant-memory slot, uploaded on
+// its first part's stream once the work it follows is done (`after`: an event per module, for
+// slots that another launch sequence of that module used). Up to SNELLY_MAX_BATCH jobs of one
+// module run concurrently; more wait for the next wave. A single job runs its first part on the
+// context stream, in slot 0 (its parameters are already uploaded there by enqueue_frames).
+//
+// Per frame and part: generate, then iterations of (extend, shade [, subsurface walk]). The first
+// `budgeted` iterations park the slowest rays when their work runs out; after them every
+// iteration advances every path by one vertex, so `nominal` more always finish the frame. Beyond
+// the nominal count, a part's iterations go in pairs, each followed by a read of its paths-left
+// count; a part gets its next pair once the read of the pair before last has landed, so its
+// stream always has a pair queued, and it moves on to its next frame once a read shows zero (an
+// extra pair then finds empty queues and returns at once). The parts are independent pixel
+// ranges, so a part that finishes a frame early starts its next one while the others still trace
+// the stragglers of theirs; the host serves whichever part's read has landed and never waits on
+// one part while another could be fed.
+int Context::enqueue_wavefront(const std::vector<Job*>& js, const std::vector<int>& frames,
+                               const std::map<Module*, cudaEvent_t>& after) {
+  for (size_t q = 0; q < js.size(); ++q) {
+    Job& j = *js[q];
+    Module& m = *j.module;
+    if (!j.wf.ptr || j.wf_parts < 1 || !m.f_wf_generate || !m.f_wf_extend || !m.f_wf_shade ||
+        m.wf_rec_f4 != j.wfb[0].rec_f4)
+      return fail(SNELLY_EINVAL, "wavefront integrator not available for this job");
+  }
+  const bool single = js.size() == 1;
+  // waves: at most SNELLY_MAX_BATCH concurrent jobs per module (one constant-memory slot each)
+  std::vector<int> wave(js.size(), 0), slot(js.size(), 0);
+  {
+    std::map<Module*, int> seen;
+    for (size_t q = 0; q < js.size(); ++q) {
+      int n = seen[js[q]->module]++;
+      wave[q] = n / SNELLY_MAX_BATCH;
+      slot[q] = n % SNELLY_MAX_BATCH;
+    }
+  }
+  const int nwaves = js.empty() ? 0 : *std::max_element(wave.begin(), wave.end()) + 1;
   if (!wf_fork) RT_TRY(cudaEventCreateWithFlags(&wf_fork, cudaEventDisableTiming));
-  for (int k = 0; k < parts; ++k)
-    if (!wf_join[k]) RT_TRY(cudaEventCreateWithFlags(&wf_join[k], cudaEventDisableTiming));
-  if (!poll_host) {
-    if (cudaMallocHost((void**)&poll_host, 2 * SNELLY_WF_MAX_PARTS * sizeof(int)) != cudaSuccess) {
+  for (int w = 0; w < nwaves; ++w) {
+    // the parts of this wave, each with a stream and two progress-read events
+    struct PartRun {
+      Job* j;
+      int k, total = 0, frame = 0, it = 0, checks = 0;
+      long long left = 0;  // paths of the frame not finished at the latest read (an upper bound afterwards)
+      bool started = false;
+      cudaStream_t st = nullptr;
+      int idx = 0;  // index into the stream / event / pinned-word pools
+    };
+    std::vector<PartRun> runs;
+    for (size_t q = 0; q < js.size(); ++q) {
+      if (wave[q] != w || frames[q] <= 0) continue;
+      for (int k = 0; k < js[q]->wf_parts; ++k) {
+        PartRun R;
+        R.j = js[q];
+        R.k = k;
+        R.total = frames[q];
+        R.idx = (int)runs.size();
+        runs.push_back(R);
+      }
+    }
+    if (runs.empty()) continue;
+    const size_t np = runs.size();
+    while (wf_pool.size() < np) {  // streams, created on first use
+      cudaStream_t st;
+      RT_TRY(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+      wf_pool.push_back(st);
+    }
+    while (wf_events.size() < 3 * np) {  // per part: two progress reads and a join
+      cudaEvent_t e;
+      RT_TRY(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+      wf_events.push_back(e);
+    }
+    if (poll_cap < 2 * np) {
+      if (poll_host) cudaFreeHost(poll_host);
       poll_host = nullptr;
-      return fail(SNELLY_EDEVICE, "pinned host allocation failed");
+      poll_cap = 0;
+      if (cudaMallocHost((void**)&poll_host, 2 * np * sizeof(int)) != cudaSuccess) {
+        poll_host = nullptr;
+        return fail(SNELLY_EDEVICE, "pinned host allocation failed");
+      }
+      poll_cap = 2 * np;
     }
-  }
-  for (auto& row : poll_done)
-    for (int k = 0; k < parts; ++k)
-      if (!row[k]) RT_TRY(cudaEventCreateWithFlags(&row[k], cudaEventDisableTiming));
-  // the other parts start after the work already on the context stream (parameter upload)
-  RT_TRY(cudaEventRecord(wf_fork, stream));
-  for (int k = 1; k < parts; ++k) RT_TRY(cudaStreamWaitEvent(wf_streams[k], wf_fork, 0));
-  void* jobs = j.tables.ptr;
-  void* gparams = j.gparams.ptr;
-  auto launch_on = [&](int k, cudaKernel_t f, int blocks, void** args) -> int {
-    RT_TRY(cudaLaunchKernel((const void*)f, dim3((unsigned)blocks), dim3(SNELLY_BLOCK), args, 0, wf_streams[k]));
-    launches++;
-    return SNELLY_OK;
-  };
-  // Per frame and part: generate, then iterations of (extend, shade). The first `budgeted`
-  // iterations park the slowest rays when their work runs out; after them every iteration
-  // advances every path by one vertex, so `nominal` more always finish the frame. Beyond the
-  // nominal count, a part's iterations go in pairs, each followed by a read of its paths-left
-  // count; a part gets its next pair once the read of the pair before last has landed, so its
-  // stream always has a pair queued, and it moves on to its next frame once a read shows zero (an
-  // extra pair then finds empty queues and returns at once). The parts are independent pixel
-  // ranges on their own streams, so a part that finishes a frame early starts the next one while
-  // the others still trace the stragglers of theirs; the host serves whichever part's read has
-  // landed and never waits on one part while another could be fed.
-  const int nominal = j.scene->opts.max_bounces + 2;
-  const int budgeted = wf_park_iters >= 0 ? std::min(wf_park_iters, 8 * nominal) : 3 * nominal;
-  const int max_iters = budgeted + nominal;
-  if (max_iters + 2 > WF_MAX_ITERS) return fail(SNELLY_EINVAL, "too many wavefront iterations for max_bounces");
-  const int extend_blocks = sm_count * m.extend_blocks_per_sm, shade_blocks = sm_count * 4;
-  struct PartRun {
-    int frame = 0, it = 0, checks = 0;
-    int left = 0;  // paths of the frame not finished at the latest read (an upper bound afterwards)
-    bool started = false;
-  } run[SNELLY_WF_MAX_PARTS];
-  auto pair = [&](int k) -> int {
-    WfBuffers B = j.wfb[k];
-    int it = run[k].it;
-    int drain = it < budgeted ? wf_drain_steps : 0;
-    // Both stages take their work from device-side counters whatever their grid. Once a read has
-    // shown few paths left, smaller grids do the same work without launching blocks that would
-    // find nothing to do: at most 3 rays (continuation, sky and sun shadows) per unfinished path.
-    const long long left = run[k].left;
-    const int eb = (int)std::max<long long>(sm_count, std::min<long long>(extend_blocks, (3 * left + SNELLY_BLOCK - 1) / SNELLY_BLOCK));
-    const int sb = (int)std::max<long long>(sm_count, std::min<long long>(shade_blocks, (left + SNELLY_BLOCK - 1) / SNELLY_BLOCK));
-    void* eargs[] = {&B, &it, &drain};
-    int r = launch_on(k, m.f_wf_extend, eb, eargs);
-    if (r) return r;
-    void* sargs[] = {&jobs, &gparams, &B, &it};
-    r = launch_on(k, m.f_wf_shade, sb, sargs);
-    if (r) return r;
-    ++run[k].it;
-    return SNELLY_OK;
-  };
-  int rc, active = parts;
-  while (active > 0) {
-    bool progress = false;
-    for (int k = 0; k < parts; ++k) {
-      PartRun& R = run[k];
-      if (R.frame >= frames) continue;
-      if (!R.started) {  // the part's next frame: camera rays, then the unpolled iterations
-        WfBuffers B = j.wfb[k];
-        void* gargs[] = {&jobs, &gparams, &B};
-        if ((rc = launch_on(k, m.f_wf_generate, (B.paths + SNELLY_BLOCK - 1) / SNELLY_BLOCK, gargs))) return rc;
-        R.started = true;
-        R.it = 0;
-        R.checks = 0;
-        R.left = B.paths;
-        while (R.it < nominal)
-          if ((rc = pair(k))) return rc;
+    for (auto& R : runs) R.st = (single && R.k == 0) ? stream : wf_pool[R.idx];
+    // every part starts after the work already on the context stream (parameter upload, seeding)
+    RT_TRY(cudaEventRecord(wf_fork, stream));
+    for (auto& R : runs)
+      if (R.st != stream) RT_TRY(cudaStreamWaitEvent(R.st, wf_fork, 0));
+    for (size_t q = 0; q < js.size(); ++q) {  // slots, and the uploads into them on each job's first part
+      if (wave[q] != w || frames[q] <= 0) continue;
+      Job& j = *js[q];
+      for (int k = 0; k < j.wf_parts; ++k) j.wfb[k].slot = single ? 0 : slot[q];
+      if (single) continue;
+      PartRun* first = nullptr;
+      for (auto& R : runs)
+        if (R.j == &j && R.k == 0) first = &R;
+      auto a = after.find(j.module);
+      if (a != after.end() && a->second) RT_TRY(cudaStreamWaitEvent(first->st, a->second, 0));
+      Module& m = *j.module;
+      RT_TRY(cudaMemcpyAsync(m.c_params + slot[q] * sizeof(SnellyParams), &j.params, sizeof(SnellyParams),
+                             cudaMemcpyHostToDevice, first->st));
+      size_t ub = std::min(j.ublock.size(), m.slot_uniform_bytes);
+      if (ub)
+        RT_TRY(cudaMemcpyAsync(m.c_uniforms + slot[q] * m.slot_uniform_bytes, j.ublock.data(), ub,
+                               cudaMemcpyHostToDevice, first->st));
+      if (j.wf_parts > 1) {  // the job's other parts read the slot too
+        cudaEvent_t up = wf_events[3 * first->idx + 2];
+        RT_TRY(cudaEventRecord(up, first->st));
+        for (auto& R : runs)
+          if (R.j == &j && R.k > 0) RT_TRY(cudaStreamWaitEvent(R.st, up, 0));
+      }
+    }
+    auto launch_on = [&](PartRun& R, cudaKernel_t f, int blocks, int threads, void** args) -> int {
+      RT_TRY(cudaLaunchKernel((const void*)f, dim3((unsigned)blocks), dim3((unsigned)threads), args, 0, R.st));
+      launches++;
+      return SNELLY_OK;
+    };
+    auto pair = [&](PartRun& R) -> int {
+      Job& j = *R.j;
+      Module& m = *j.module;
+      WfBuffers B = j.wfb[R.k];
+      void* jobs = j.tables.ptr;
+      void* gparams = j.gparams.ptr;
+      const int nominal = j.scene->opts.max_bounces + 2;
+      const int budgeted = wf_park_iters >= 0 ? std::min(wf_park_iters, 8 * nominal) : 3 * nominal;
+      int it = R.it;
+      const WfConfig& cf = j.wfc;
+      int drain = it < budgeted ? cf.drain : 0;
+      int chunk = cf.chunk, grab = cf.grab, refill = cf.refill;
+      const int bs = cf.block;
+      // Both stages take their work from device-side counters whatever their grid. Once a read has
+      // shown few paths left, smaller grids do the same work without launching blocks that would
+      // find nothing to do: at most 3 rays (continuation, sky and sun shadows) per unfinished path.
+      const long long left = R.left;
+      const long long extend_blocks = (long long)sm_count * (bs < 128 ? m.extend_blocks_per_sm64 : m.extend_blocks_per_sm);
+      const long long shade_blocks = (long long)sm_count * 4 * (128 / bs);
+      const int eb = (int)std::max<long long>(sm_count, std::min(extend_blocks, (3 * left + bs - 1) / bs));
+      const int sb = (int)std::max<long long>(sm_count, std::min(shade_blocks, (left + bs - 1) / bs));
+      const bool split = cf.shade_split && m.f_wf_shade_seg[0];
+      const bool walk = m.f_wf_sss && j.params.subsurfaceMFP > 0.0f;  // vertices may choose the walk
+      void* eargs[] = {&B, &it, &drain, &chunk, &grab, &refill};
+      int r = launch_on(R, m.f_wf_extend, eb, bs, eargs);
+      if (r) return r;
+      void* sargs[] = {&jobs, &gparams, &B, &it};
+      if (split) {  // one launch per material segment, each compiled for its material
+        for (int sg = 0; sg < 4; ++sg)
+          if (m.f_wf_shade_seg[sg] && (r = launch_on(R, m.f_wf_shade_seg[sg], sb, bs, sargs))) return r;
+      } else if ((r = launch_on(R, m.f_wf_shade, sb, bs, sargs))) {
+        return r;
+      }
+      if (walk && (r = launch_on(R, m.f_wf_sss, sb, bs, sargs))) return r;  // the subsurface walks it handed over
+      ++R.it;
+      return SNELLY_OK;
+    };
+    int rc;
+    size_t active = runs.size();
+    while (active > 0) {
+      bool progress = false;
+      for (auto& R : runs) {
+        if (R.frame >= R.total) continue;
+        Job& j = *R.j;
+        const int nominal = j.scene->opts.max_bounces + 2;
+        const int budgeted = wf_park_iters >= 0 ? std::min(wf_park_iters, 8 * nominal) : 3 * nominal;
+        const int max_iters = budgeted + nominal;
+        if (max_iters + 2 > WF_MAX_ITERS) return fail(SNELLY_EINVAL, "too many wavefront iterations for max_bounces");
+        if (!R.started) {  // the part's next frame: camera rays, then the unpolled iterations
+          WfBuffers B = j.wfb[R.k];
+          void* jobs = j.tables.ptr;
+          void* gparams = j.gparams.ptr;
+          void* gargs[] = {&jobs, &gparams, &B};
+          if ((rc = launch_on(R, j.module->f_wf_generate, (B.paths + SNELLY_BLOCK - 1) / SNELLY_BLOCK, SNELLY_BLOCK, gargs)))
+            return rc;
+          R.started = true;
+          R.it = 0;
+          R.checks = 0;
+          R.left = B.paths;
+          while (R.it < nominal)
+            if ((rc = pair(R))) return rc;
+          progress = true;
+          continue;
+        }
+        bool frame_done = R.it >= max_iters;
+        if (!frame_done && R.checks >= 2) {  // the older of the part's two outstanding reads
+          const int prev = R.checks & 1;
+          const cudaError_t q = cudaEventQuery(wf_events[3 * R.idx + prev]);
+          if (q == cudaErrorNotReady) continue;  // the part still has two pairs queued: serve the others
+          if (q != cudaSuccess)
+            return fail(SNELLY_EDEVICE, std::string("wavefront progress wait failed: ") + cudaGetErrorString(q));
+          R.left = poll_host[2 * R.idx + prev];
+          frame_done = R.left == 0;
+        }
         progress = true;
-        continue;
+        if (frame_done) {
+          R.started = false;
+          if (++R.frame >= R.total) --active;
+          continue;
+        }
+        if ((rc = pair(R)) || (rc = pair(R))) return rc;
+        const int ps = R.checks & 1;
+        if (cudaMemcpyAsync(poll_host + 2 * R.idx + ps, j.wfb[R.k].cnt + WF_LEFT, sizeof(int), cudaMemcpyDeviceToHost,
+                            R.st) != cudaSuccess ||
+            cudaEventRecord(wf_events[3 * R.idx + ps], R.st) != cudaSuccess)
+          return fail(SNELLY_EDEVICE, "wavefront progress read failed");
+        ++R.checks;
       }
-      bool frame_done = R.it >= max_iters;
-      if (!frame_done && R.checks >= 2) {  // the older of the part's two outstanding reads
-        const int prev = R.checks & 1;
-        const cudaError_t q = cudaEventQuery(poll_done[prev][k]);
-        if (q == cudaErrorNotReady) continue;  // the part still has two pairs queued: serve the others
-        if (q != cudaSuccess) return fail(SNELLY_EDEVICE, std::string("wavefront progress wait failed: ") + cudaGetErrorString(q));
-        R.left = poll_host[prev * SNELLY_WF_MAX_PARTS + k];
-        frame_done = R.left == 0;
-      }
-      progress = true;
-      if (frame_done) {
-        R.started = false;
-        if (++R.frame >= frames) --active;
-        continue;
-      }
-      if ((rc = pair(k)) || (rc = pair(k))) return rc;
-      const int slot = R.checks & 1;
-      if (cudaMemcpyAsync(poll_host + slot * SNELLY_WF_MAX_PARTS + k, j.wfb[k].cnt + WF_LEFT, sizeof(int),
-                          cudaMemcpyDeviceToHost, wf_streams[k]) != cudaSuccess ||
-          cudaEventRecord(poll_done[slot][k], wf_streams[k]) != cudaSuccess)
-        return fail(SNELLY_EDEVICE, "wavefront progress read failed");
-      ++R.checks;
+      if (!progress) std::this_thread::yield();  // every part has work queued
     }
-    if (!progress) std::this_thread::yield();  // every part has work queued
-  }
-  // later work on the context stream (resolve, readback) waits for every part
-  for (int k = 1; k < parts; ++k) {
-    RT_TRY(cudaEventRecord(wf_join[k], wf_streams[k]));
-    RT_TRY(cudaStreamWaitEvent(stream, wf_join[k], 0));
+    // later work on the context stream (resolve, readback, the next wave) waits for every part
+    for (auto& R : runs) {
+      if (R.st == stream) continue;
+      RT_TRY(cudaEventRecord(wf_events[3 * R.idx + 2], R.st));
+      RT_TRY(cudaStreamWaitEvent(stream, wf_events[3 * R.idx + 2], 0));
+    }
   }
   return SNELLY_OK;
 }
 
-// The integrator choice of SNELLY_KERNEL_AUTO: per (scene module, image-size class) the first job
-// times one warm-up and two frames of each integrator on its own buffers, keeps the faster and
-// caches the decision; the job's state is seeded again afterwards by the caller. The size class is
-// the power of two nearest the pixel count (tail effects make the choice size-dependent).
+// Frames of one job with the given integrator on its own buffers, timed with events on the
+// context stream: one warm-up frame, then enough frames for about 5 ms (2 to 16); the per-frame
+// time. The job's state is seeded again afterwards by the caller.
+int Context::time_frames(Job& j, int kernel, float* ms_per_frame) {
+  void* tables = j.tables.ptr;
+  void* bstart = (char*)j.tables.ptr + 128;
+  int njobs = 1;
+  void* gparams = j.gparams.ptr;
+  void* margs[] = {&tables, &bstart, &njobs, &gparams};
+  auto frames = [&](int n) -> int {
+    if (kernel == SNELLY_KERNEL_WAVEFRONT) return enqueue_wavefront_frames(j, n);
+    for (int f = 0; f < n; ++f)
+      if (int rc = launch(j.module->f_frame_mega, j.blocks, SNELLY_BLOCK, margs)) return rc;
+    return SNELLY_OK;
+  };
+  cudaEvent_t e[3] = {nullptr, nullptr, nullptr};
+  for (auto& ev : e)
+    if (cudaEventCreate(&ev) != cudaSuccess) {
+      for (auto& x : e)
+        if (x) cudaEventDestroy(x);
+      return fail(SNELLY_EDEVICE, "autotune event creation failed");
+    }
+  int rc = SNELLY_OK;
+  float warm = 0.0f, ms = 0.0f;
+  int n = 2;
+  if (!(rc = (cudaEventRecord(e[0], stream) == cudaSuccess ? frames(1) : SNELLY_EDEVICE))) {
+    cudaEventRecord(e[1], stream);
+    if (cudaEventSynchronize(e[1]) != cudaSuccess) rc = fail(SNELLY_EDEVICE, "autotune timing failed");
+    else cudaEventElapsedTime(&warm, e[0], e[1]);
+  }
+  if (!rc) {
+    n = std::max(2, std::min(16, (int)std::ceil(5.0f / std::max(warm, 1e-3f))));
+    rc = frames(n);
+  }
+  if (!rc) {
+    cudaEventRecord(e[2], stream);
+    if (cudaEventSynchronize(e[2]) != cudaSuccess) rc = fail(SNELLY_EDEVICE, "autotune timing failed");
+    else cudaEventElapsedTime(&ms, e[1], e[2]);
+  }
+  for (auto& x : e) cudaEventDestroy(x);
+  *ms_per_frame = ms / n;
+  return rc;
+}
+
+// The integrator choice of SNELLY_KERNEL_AUTO and the wavefront's launch configuration, per
+// (scene module, image-size class): the first such job times, on its own buffers, the wavefront
+// with each value of one configuration field in turn (the best so far for the others; one pass
+// over pixel ranges, per-material shading, drain steps, refill chunk, claim size, refill threshold
+// and block shape; fields fixed by the environment are not varied), then the path-per-thread
+// kernel, keeps the fastest and caches the decision; the job's state is seeded again afterwards
+// by the caller. The size class is the power of two nearest the pixel count (tail effects make
+// the choice size-dependent).
 int Context::autotune(Job& j) {
   const long long npix = (long long)j.desc.width * j.desc.height;
   int cls = 0;
@@ -202,7 +351,7 @@ int Context::autotune(Job& j) {
   if (npix - (1ll << cls) > (1ll << (cls + 1)) - npix) ++cls;
   const std::string key = j.module->key + "/" + std::to_string(cls);
   auto it = tuned.find(key);
-  int best;
+  Tuned best{SNELLY_KERNEL_WAVEFRONT, j.wfc};  // the context's defaults, pixel ranges as allocated
   if (it != tuned.end()) {
     best = it->second;
   } else {
@@ -211,33 +360,59 @@ int Context::autotune(Job& j) {
     void* tables = j.tables.ptr;
     void* bstart = (char*)j.tables.ptr + 128;
     int njobs = 1;
-    void* gparams = j.gparams.ptr;
     void* sargs[] = {&tables, &bstart, &njobs};
-    void* margs[] = {&tables, &bstart, &njobs, &gparams};
     if ((rc = launch(j.module->f_seed, j.blocks, SNELLY_BLOCK, sargs))) return rc;
-    cudaEvent_t e0 = nullptr, e1 = nullptr;
-    if (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess) {
-      if (e0) cudaEventDestroy(e0);
-      return fail(SNELLY_EDEVICE, "autotune event creation failed");
-    }
-    float ms[2] = {0.0f, 0.0f};
-    for (int k = 0; k < 2 && !rc; ++k) {
-      for (int f = 0; f < 3 && !rc; ++f) {
-        if (f == 1) cudaEventRecord(e0, stream);
-        rc = k == 0 ? launch(j.module->f_frame_mega, j.blocks, SNELLY_BLOCK, margs) : enqueue_wavefront_frames(j, 1);
+    auto try_cfg = [&](const WfConfig& cfg, float* ms) -> int {
+      if (cfg.parts != j.wfc.parts) {  // another split into pixel ranges: new buffers
+        if (cudaStreamSynchronize(stream) != cudaSuccess) return fail(SNELLY_EDEVICE, "autotune sync failed");
+        release_wavefront(j);
+        j.wfc = cfg;
+        if (int r = alloc_wavefront(j)) return r;
       }
-      cudaEventRecord(e1, stream);
-      if (!rc && cudaEventSynchronize(e1) != cudaSuccess) rc = fail(SNELLY_EDEVICE, "autotune timing failed");
-      if (!rc) cudaEventElapsedTime(&ms[k], e0, e1);
+      j.wfc = cfg;
+      return time_frames(j, SNELLY_KERNEL_WAVEFRONT, ms);
+    };
+    float best_ms = 0.0f;
+    if ((rc = try_cfg(best.cfg, &best_ms))) return rc;
+    struct Field {
+      int WfConfig::*f;
+      std::vector<int> values;
+    } fields[] = {{&WfConfig::parts, {1, 2, 3, 4}},  {&WfConfig::shade_split, {0, 1}}, {&WfConfig::drain, {16, 32, 64}},
+                  {&WfConfig::chunk, {4, 8, 16}},   {&WfConfig::grab, {16, 32, 64}},  {&WfConfig::refill, {2, 4, 8}},
+                  {&WfConfig::block, {64, 128}}};
+    for (unsigned k = 0; k < sizeof fields / sizeof fields[0]; ++k) {
+      if (wf_fixed & (1u << k)) continue;
+      for (int v : fields[k].values) {
+        WfConfig cfg = best.cfg;
+        if (cfg.*(fields[k].f) == v) continue;
+        cfg.*(fields[k].f) = v;
+        if (k == 0 && v > 1 && npix < (long long)v * 65536) continue;  // too small for that many ranges
+        float ms = 0.0f;
+        if ((rc = try_cfg(cfg, &ms))) return rc;
+        if (ms < best_ms) {
+          best_ms = ms;
+          best.cfg = cfg;
+        }
+      }
     }
-    cudaEventDestroy(e0);
-    cudaEventDestroy(e1);
-    if (rc) return rc;
-    best = ms[1] < ms[0] ? SNELLY_KERNEL_WAVEFRONT : SNELLY_KERNEL_MEGA;
+    float mega_ms = 0.0f;
+    if ((rc = time_frames(j, SNELLY_KERNEL_MEGA, &mega_ms))) return rc;
+    best.kernel = mega_ms < best_ms ? SNELLY_KERNEL_MEGA : SNELLY_KERNEL_WAVEFRONT;
     tuned[key] = best;
   }
-  j.kernel_mode = best;
-  if (best == SNELLY_KERNEL_MEGA) release_wavefront(j);
+  j.kernel_mode = best.kernel;
+  if (best.kernel == SNELLY_KERNEL_MEGA) {
+    if (cudaStreamSynchronize(stream) != cudaSuccess) return fail(SNELLY_EDEVICE, "autotune sync failed");
+    release_wavefront(j);
+    return SNELLY_OK;
+  }
+  if (best.cfg.parts != j.wfc.parts) {
+    if (cudaStreamSynchronize(stream) != cudaSuccess) return fail(SNELLY_EDEVICE, "autotune sync failed");
+    release_wavefront(j);
+    j.wfc = best.cfg;
+    return alloc_wavefront(j);
+  }
+  j.wfc = best.cfg;
   return SNELLY_OK;
 }
 

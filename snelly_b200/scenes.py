@@ -266,6 +266,100 @@ float SDF_SURFACE(vec3 X)
         return 1.0e-4
 
 
+class PyroclasticSubsurface(VolumetricSubsurface):
+    """C2 complete: the subsurface Mandelbox together with a pyroclastic cloud between it and the
+    camera, a sphere of radius 1 at `centre` displaced by 5-octave fBm value noise of amplitude
+    0.3 (lattice hash offset by `seed`), scattering coefficient 2 and absorption 0.1 per unit
+    length, Henyey-Greenstein g = 0.5. The cloud is a heterogeneous medium given through the
+    VOLUME_EXTINCTION / VOLUME_EXTINCTION_MAX hooks, which the reference declares but never calls:
+    this build's extension renders it (delta tracking), the reference's shader would not."""
+
+    def __init__(self, width=None, height=None, seed=3, centre=(-4.8, 3.4, -3.9)):
+        super().__init__(width, height)
+        self.seed = seed
+        self.centre = centre
+
+    def init(self, snelly):
+        super().init(snelly)
+        v = snelly.getMaterials().loadVolume()
+        cx, cy, cz = self.centre
+        v.atmosphereMinX, v.atmosphereMaxX = cx - 1.5, cx + 1.5
+        v.atmosphereMinY, v.atmosphereMaxY = cy - 1.5, cy + 1.5
+        v.atmosphereMinZ, v.atmosphereMaxZ = cz - 1.5, cz + 1.5
+        v.lof10_mfp = 0.0
+        v.scatteringColor = [2.0, 2.0, 2.0]
+        v.absorptionColor = [0.1, 0.1, 0.1]
+        v.anisotropy = 0.5
+
+    def shader(self):
+        return super().shader() + """
+uniform vec3 cloudCentre;
+uniform float cloudSeed;
+
+// pseudo-random value in [0, 1) at an integer lattice point
+float cloudLattice(vec3 q)
+{
+    q = fract(q * vec3(0.1183, 0.1517, 0.1297) + vec3(cloudSeed * 0.0713));
+    q += dot(q, q.yzx + 23.17);
+    return fract((q.x + q.y) * q.z * 95.43);
+}
+
+// trilinear value noise with smoothstep weights, in [0, 1]
+float cloudNoise(vec3 p)
+{
+    vec3 i = floor(p);
+    vec3 f = p - i;
+    f = f * f * (3.0 - 2.0 * f);
+    float n000 = cloudLattice(i);
+    float n100 = cloudLattice(i + vec3(1.0, 0.0, 0.0));
+    float n010 = cloudLattice(i + vec3(0.0, 1.0, 0.0));
+    float n110 = cloudLattice(i + vec3(1.0, 1.0, 0.0));
+    float n001 = cloudLattice(i + vec3(0.0, 0.0, 1.0));
+    float n101 = cloudLattice(i + vec3(1.0, 0.0, 1.0));
+    float n011 = cloudLattice(i + vec3(0.0, 1.0, 1.0));
+    float n111 = cloudLattice(i + vec3(1.0, 1.0, 1.0));
+    float x00 = mix(n000, n100, f.x);
+    float x10 = mix(n010, n110, f.x);
+    float x01 = mix(n001, n101, f.x);
+    float x11 = mix(n011, n111, f.x);
+    return mix(mix(x00, x10, f.y), mix(x01, x11, f.y), f.z);
+}
+
+// 5-octave fBm in [-1, 1]
+float cloudFbm(vec3 p)
+{
+    float sum = 0.0;
+    float amp = 0.5;
+    float norm = 0.0;
+    for (int o = 0; o < 5; ++o)
+    {
+        sum += amp * (2.0 * cloudNoise(p) - 1.0);
+        norm += amp;
+        p *= 2.03;
+        amp *= 0.5;
+    }
+    return sum / norm;
+}
+
+float VOLUME_EXTINCTION(float extinction_ui, vec3 X)
+{
+    vec3 q = X - cloudCentre;
+    float r = 1.0 + 0.3 * cloudFbm(2.5 * q);
+    return length(q) < r ? extinction_ui : 0.0;
+}
+
+float VOLUME_EXTINCTION_MAX(float extinction_ui)
+{
+    return extinction_ui;
+}
+"""
+
+    def syncShader(self, snelly, shader):
+        super().syncShader(snelly, shader)
+        shader.uniform3F("cloudCentre", *self.centre)
+        shader.uniformF("cloudSeed", float(self.seed))
+
+
 class AtmosphereLights:
     """Coverage scene: homogeneous atmosphere with multiple scattering, fake fog, sphere light,
     sun and sky over a metal sphere, a glass box with absorption and a diffuse ground (RGB mode,
@@ -695,4 +789,4 @@ float SDF_SURFACE(vec3 X)
 
 SCENES = {"c0": PlainSphere, "c1": DispersiveFractal, "c2": VolumetricSubsurface, "atmosphere": AtmosphereLights,
           "hooks": HooksAndMaps, "mesh": MeshLike, "envmap": EnvMapLit, "turntable": Turntable,
-          "lowsun": LowSunNoSky}
+          "lowsun": LowSunNoSky, "c2_cloud": PyroclasticSubsurface}

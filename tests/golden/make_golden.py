@@ -15,6 +15,13 @@ Run with $SNELLY_REFERENCE naming a checkout of the reference:
   simplepathtracer-fragment-shader.glsl) on the same scenes: running means and RNG lanes.
 * tm_golden.npz: the reference's tonemapper program on path-traced and synthetic XYZ texels for
   three display settings.
+* bench_c1.npz: the benchmark's own workload (1920x1080 dispersive Menger sponge, gold sphere,
+  ground; seed 2) through the reference's path tracer: 20,000 fixed random pixels x 2 frames with
+  the seeds the GPU uses for the same pixels (running means and final RNG lanes).
+* stat_<case>.npz: the reference's path tracer at matched spp with independent seeds, for
+  statistical comparison: a 256x256 crop of the 1080p benchmark frame at 64 spp (16 batches of 4
+  frames), and the C0 image at its own 256x256 and 16 spp (16 batches of 1 frame); per-pixel mean
+  and variance of the batch-mean luminance, and every batch's image-mean luminance.
 * cie_csv.npy: the CIE XYZ table recomputed from scripts/color/lin2012xyz2e_fine_7sf.csv as
   scripts/color/cie.py does (linear interpolation to 1024 samples over 390..750 nm, both ends
   included), to pin the table in snelly_b200/data/materials.json.
@@ -107,6 +114,89 @@ def make_ptsimple(name):
     print(f"ps_{name}: {h.width}x{h.height}, {PS_FRAMES} frames, mean XYZ {mean[:, :3].mean(0)}")
 
 
+BENCH_C1_PIXELS, BENCH_C1_FRAMES, BENCH_C1_SEED = 20000, 2, 2
+
+
+def make_bench_c1():
+    """bench_c1.npz: matched seeds on the benchmark's own 1080p frame (see the module docstring)."""
+    h = HostSnelly(scenes.DispersiveFractal())
+    ref, p, tables, keep = build_ref.ref_for(h, name="bench_c1")
+    n = h.width * h.height
+    pix = np.sort(np.random.RandomState(20).choice(n, BENCH_C1_PIXELS, replace=False)).astype(np.int32)
+    rng0 = oracle.seed_pixels(BENCH_C1_SEED, pix)
+    sh = h.scene_shader()
+    mean, rng = ref.render(p, sh.calls, tables, h.width, h.height, pix, BENCH_C1_FRAMES, rng0, scene_textures=sh.textures)
+    np.savez_compressed(os.path.join(HERE, "bench_c1.npz"), width=h.width, height=h.height, frames=BENCH_C1_FRAMES,
+                        seed=BENCH_C1_SEED, pixels=pix, mean=mean, rng=rng)
+    print(f"bench_c1: {len(pix)} pixels of {h.width}x{h.height}, {BENCH_C1_FRAMES} frames, mean XYZ {mean[:, :3].mean(0)}")
+
+
+# (scene factory, crop (x0, y0, w, h) or None for the whole image, batches, frames per batch)
+STAT_CASES = {
+    "c1_crop": (lambda: scenes.DispersiveFractal(), (832, 412, 256, 256), 16, 4),
+    "c0": (lambda: scenes.PlainSphere(), None, 16, 1),
+}
+STAT_SEED0 = 1000
+
+
+def stat_pixels(h, crop):
+    if crop is None:
+        return np.arange(h.width * h.height, dtype=np.int32)
+    x0, y0, w, hh = crop
+    ys, xs = np.mgrid[y0:y0 + hh, x0:x0 + w]
+    return (ys * h.width + xs).reshape(-1).astype(np.int32)
+
+
+def stat_batches(name, seed0):
+    """Per-batch mean luminance (batches, pixels) of the reference's path tracer for STAT_CASES[name]."""
+    factory, crop, batches, frames = STAT_CASES[name]
+    h = HostSnelly(factory())
+    ref, p, tables, keep = build_ref.ref_for(h, name="bench_c1" if name == "c1_crop" else None)
+    pix = stat_pixels(h, crop)
+    sh = h.scene_shader()
+    ys = np.empty((batches, len(pix)), np.float64)
+    for b in range(batches):
+        rng0 = oracle.seed_pixels(seed0 + b, pix)
+        mean, _ = ref.render(p, sh.calls, tables, h.width, h.height, pix, frames, rng0, scene_textures=sh.textures)
+        ys[b] = mean[:, 1]
+    return ys
+
+
+def make_stat(name):
+    factory, crop, batches, frames = STAT_CASES[name]
+    ys = stat_batches(name, STAT_SEED0)
+    np.savez_compressed(os.path.join(HERE, f"stat_{name}.npz"), crop=np.asarray(crop or (0, 0, 0, 0), np.int32),
+                        batches=batches, frames=frames, seed0=STAT_SEED0, y_mean=ys.mean(0).astype(np.float32),
+                        y_var=ys.var(0, ddof=1).astype(np.float32), img_means=ys.mean(1))
+    print(f"stat_{name}: {ys.shape[1]} pixels, {batches} x {frames} frames, image mean Y {ys.mean():.6f}")
+
+
+FULL_BATCHES, FULL_FRAMES, FULL_SEED0, FULL_TILE = 14, 16, 7000, 30
+
+
+def make_full_c1():
+    """full_c1.npz: the reference's path tracer over the whole 1080p benchmark frame at
+    FULL_BATCHES x FULL_FRAMES spp (independent seeds per batch): each batch's image-mean XYZ and
+    its mean XYZ over FULL_TILE x FULL_TILE pixel tiles. The image mean luminance is known to about
+    0.1% from this, which the 0.5% bar needs (a 256x256 crop at 64 spp leaves a 1% standard
+    error: the sun's caustics through the sponge make the estimator heavy-tailed)."""
+    h = HostSnelly(scenes.DispersiveFractal())
+    ref, p, tables, keep = build_ref.ref_for(h, name="bench_c1")
+    W, H = h.width, h.height
+    pix = np.arange(W * H, dtype=np.int32)
+    sh = h.scene_shader()
+    img, tiles = [], []
+    for b in range(FULL_BATCHES):
+        rng0 = oracle.seed_pixels(FULL_SEED0 + b, pix)
+        mean, _ = ref.render(p, sh.calls, tables, W, H, pix, FULL_FRAMES, rng0, scene_textures=sh.textures)
+        m = mean[:, :3].astype(np.float64).reshape(H, W, 3)
+        img.append(m.mean((0, 1)))
+        tiles.append(m.reshape(H // FULL_TILE, FULL_TILE, W // FULL_TILE, FULL_TILE, 3).mean((1, 3)))
+        print(f"full_c1 batch {b}: image mean XYZ {img[-1]}", flush=True)
+    np.savez_compressed(os.path.join(HERE, "full_c1.npz"), batches=FULL_BATCHES, frames=FULL_FRAMES, seed0=FULL_SEED0,
+                        tile=FULL_TILE, img_xyz=np.asarray(img), tile_xyz=np.asarray(tiles, np.float32))
+
+
 TM_PARAMS = [  # exposure, invGamma (= 1/gamma as the host uploads it), contrast, saturation, hueShift
     (0.0, 1.0 / 2.2, 1.0, 1.0, 0.0),   # the Renderer defaults (js/renderer.js:118-122)
     (1.5, 1.0 / 1.8, 1.3, 0.8, 0.25),
@@ -157,5 +247,12 @@ if __name__ == "__main__":
     for n in FH_CASES:
         if not only or "ps" in only:
             make_ptsimple(n)
+    if not only or "bench" in only:
+        make_bench_c1()
+    for n in STAT_CASES:
+        if not only or "stat" in only:
+            make_stat(n)
+    if "full" in only:  # about 460 M path samples: tens of minutes on a few host cores
+        make_full_c1()
     if not only or "tm" in only:
         make_tonemap()

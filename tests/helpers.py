@@ -82,3 +82,18 @@ def gpu_render(ctx, scene, frames, seed=1, math_mode=None, kernel_mode=None, fp6
 
 def host(name):
     return HostSnelly(CASES[name]())
+
+
+def welch_p(a_mean, a_var, na, b_mean, b_var, nb):
+    """Two-sided p-values of Welch's two-sample t statistic per element (Welch-Satterthwaite
+    degrees of freedom), for means and unbiased variances of na and nb samples; NaN where both
+    variances are zero."""
+    from scipy import stats
+    va, vb = a_var / na, b_var / nb
+    se2 = va + vb
+    with np.errstate(divide="ignore", invalid="ignore"):
+        t = np.abs(a_mean - b_mean) / np.sqrt(se2)
+        dof = se2 ** 2 / (va ** 2 / (na - 1) + vb ** 2 / (nb - 1))
+    p = 2.0 * stats.t.sf(t, dof)
+    p[se2 <= 0] = np.nan
+    return p

@@ -45,3 +45,38 @@ def test_batches_larger_than_one_launch(gpu_ctx):
     for k, (s, fr, w, h) in enumerate(jobs):
         ref = gpu_render(gpu_ctx, scenes.PlainSphere(w, h), fr, seed=100 + k)[1]
         np.testing.assert_array_equal(s.readback(), ref)
+
+
+def test_wavefront_jobs_in_a_batch(gpu_ctx):
+    """Wavefront jobs in a batch run concurrently, each in its own constant-memory slot and pixel
+    ranges: 36 of one scene module (more than the 32 slots: two waves), path-per-thread jobs of
+    the same module (whose launch lane hands the slots over), other modules, and one image large
+    enough for three concurrent pixel ranges. Every image equals the job rendered alone, bit for
+    bit."""
+    from snelly_b200 import _native as N
+    rs = np.random.RandomState(3)
+    spec = []
+    for k in range(36):
+        spec.append((scenes.PlainSphere, int(rs.randint(24, 120)), int(rs.randint(24, 120)), int(rs.randint(1, 4)),
+                     N.KERNEL_WAVEFRONT))
+    for k in range(4):
+        spec.append((scenes.PlainSphere, int(rs.randint(24, 80)), int(rs.randint(24, 80)), 2, N.KERNEL_MEGA))
+    spec += [(scenes.DispersiveFractal, 96, 54, 3, N.KERNEL_WAVEFRONT), (scenes.AtmosphereLights, 64, 48, 2, N.KERNEL_WAVEFRONT),
+             (scenes.DispersiveFractal, 512, 400, 2, N.KERNEL_WAVEFRONT)]
+    jobs = []
+    for k, (cls, w, h, fr, km) in enumerate(spec):
+        s = api.Snelly(cls(w, h), context=gpu_ctx)
+        s.seed = 500 + k
+        s.pathtracer.kernelMode = km
+        s.render(0)
+        assert gpu_ctx.job_kernel(s.job_id()) == km
+        jobs.append((s, fr))
+    gpu_ctx.advance_batch({s.job_id(): fr for s, fr in jobs})
+    got = [s.readback().copy() for s, fr in jobs]
+    for s, fr in jobs:
+        gpu_ctx.destroy_job(s.job_id())
+    for k, (cls, w, h, fr, km) in enumerate(spec):
+        ref = gpu_render(gpu_ctx, cls(w, h), fr, seed=500 + k, kernel_mode=km)
+        assert (got[k][..., 3] == fr).all(), k
+        np.testing.assert_array_equal(got[k], ref[1], err_msg=f"job {k}")
+        gpu_ctx.destroy_job(ref[0].job_id())

@@ -1,0 +1,105 @@
+"""The heterogeneous-medium extension on the GPU (C2's pyroclastic cloud): a scene that defines
+VOLUME_EXTINCTION gets delta tracking through the medium; the reference's path tracer never calls
+that hook, so parity is against this build's own CPU restatement (oracle/pt_oracle_integrator.inc,
+HAS_HETERO_VOLUME): parity unpinned to the reference. Also the FP32 Kahan accumulation against the
+FP64 accumulation on C2 at 4096 spp. Tolerances are written in each test."""
+import numpy as np
+import pytest
+
+from helpers import gpu_render, oracle_render, welch_p
+from snelly_b200 import _native as N
+from snelly_b200 import scenes
+from snelly_b200.testing import HostSnelly
+
+pytestmark = pytest.mark.gpu
+
+
+def _close(a, b, rtol):
+    return np.abs(a - b).max(-1) <= rtol * np.maximum(1.0, np.abs(b).max(-1))
+
+
+@pytest.mark.parametrize("kernel", [N.KERNEL_MEGA, N.KERNEL_WAVEFRONT])
+def test_cloud_strict_matches_oracle_per_pixel(gpu_ctx, kernel):
+    """IEEE-strict module vs the oracle with matched seeds, 40x40, 2 frames: the medium's delta
+    tracking consumes the path's random numbers in the same order on both sides, and the shadow
+    rays' ratio tracking hashes its numbers from the ray. Bar: >= 90% of pixels within 1e-4 (the
+    Mandelbox's subsurface walks amplify last-ulp transcendental differences, as in the C2 surface
+    tests), image mean XYZ within 2%."""
+    frames = 2
+    s, img = gpu_render(gpu_ctx, scenes.PyroclasticSubsurface(40, 40), frames, seed=21, math_mode=N.MATH_STRICT,
+                        kernel_mode=kernel)
+    h = HostSnelly(scenes.PyroclasticSubsurface(40, 40), seed=21)
+    xyz, mean, rng = oracle_render(h, np.arange(40 * 40), frames)
+    got = img.reshape(-1, 4)
+    assert (got[:, 3] == frames).all()
+    ok = _close(got[:, :3], xyz / frames, 1e-4)
+    rel = np.abs(got[:, :3].mean(0) - (xyz / frames).mean(0)) / np.abs((xyz / frames).mean(0))
+    assert ok.mean() >= 0.90, ok.mean()
+    assert rel.max() <= 0.02, rel
+    gpu_ctx.destroy_job(s.job_id())
+
+
+def test_cloud_wavefront_equals_path_per_thread(gpu_ctx):
+    """The wavefront resolves a surface vertex's shadow rays one stage later than the
+    path-per-thread kernel; the medium's transmittance along them draws its numbers from the ray,
+    not from the path, so both give the same image under strict math (>= 97% of pixels within
+    1e-5; the rest differ in the summation order of the deferred estimate)."""
+    a = gpu_render(gpu_ctx, scenes.PyroclasticSubsurface(48, 48), 3, seed=5, math_mode=N.MATH_STRICT,
+                   kernel_mode=N.KERNEL_MEGA)[1].reshape(-1, 4)
+    b = gpu_render(gpu_ctx, scenes.PyroclasticSubsurface(48, 48), 3, seed=5, math_mode=N.MATH_STRICT,
+                   kernel_mode=N.KERNEL_WAVEFRONT)[1].reshape(-1, 4)
+    assert (a[:, 3] == b[:, 3]).all()
+    assert _close(b[:, :3], a[:, :3], 1e-5).mean() >= 0.97
+
+
+def test_cloud_statistics_against_oracle(gpu_ctx):
+    """Production build (fast math, autotuned integrator) and the oracle with independent seeds,
+    48x48, 16 batches of 4 frames each side; Welch's t statistic per pixel as a two-sided p-value.
+    Bars: image mean luminance within 4 standard errors; at most 0.8% of pixels with p < 0.0027
+    (0.27% expected) and 0.05% with p < 5.7e-7."""
+    B, F, W = 16, 4, 48
+    g, o = [], []
+    for b in range(B):
+        s, img = gpu_render(gpu_ctx, scenes.PyroclasticSubsurface(W, W), F, seed=3000 + b)
+        g.append(img[..., 1].reshape(-1).astype(np.float64))
+        gpu_ctx.destroy_job(s.job_id())
+        h = HostSnelly(scenes.PyroclasticSubsurface(W, W), seed=7000 + b)
+        xyz, _, _ = oracle_render(h, np.arange(W * W), F)
+        o.append(xyz[:, 1] / F)
+    g, o = np.array(g), np.array(o)
+    p = welch_p(g.mean(0), g.var(0, ddof=1), B, o.mean(0), o.var(0, ddof=1), B)
+    p = p[np.isfinite(p)]
+    gm, om = g.mean(1), o.mean(1)
+    se_img = np.sqrt(gm.var(ddof=1) / B + om.var(ddof=1) / B)
+    msg = (f"image mean gpu {gm.mean():.6f} oracle {om.mean():.6f} (SE {se_img:.2e}); "
+           f"pixels with p < 0.0027 / 5.7e-7 {(p < 0.0027).mean():.4f}/{(p < 5.7e-7).mean():.5f}")
+    print(msg)
+    assert abs(gm.mean() - om.mean()) <= 4 * se_img, msg
+    assert (p < 0.0027).mean() <= 0.008, msg
+    assert (p < 5.7e-7).mean() <= 0.0005, msg
+
+
+def test_cloud_changes_the_image(gpu_ctx):
+    """The medium is there: 64 spp of C2 with and without the cloud differ in the region it
+    covers (mean luminance over the image differs by more than 5%)."""
+    a = gpu_render(gpu_ctx, scenes.VolumetricSubsurface(96, 96), 64, seed=9)[1][..., 1].mean()
+    b = gpu_render(gpu_ctx, scenes.PyroclasticSubsurface(96, 96), 64, seed=9)[1][..., 1].mean()
+    assert abs(a - b) / a > 0.05, (a, b)
+
+
+def test_kahan_fp32_against_fp64_on_c2_4096spp(gpu_ctx):
+    """C2 with its cloud, 96x96 at 4096 spp: the FP32 Kahan-compensated sums against the FP64
+    accumulation of the same per-frame contributions. Bars (the statement of the accumulation
+    error): maximum relative error per pixel and channel below 1e-6, median below 1e-7."""
+    s, img = gpu_render(gpu_ctx, scenes.PyroclasticSubsurface(96, 96), 4096, seed=4, fp64=True)
+    rng, acc, comp, acc64 = s.readback_state()
+    assert (acc64[:, 3] == 4096).all() and (acc[:, 3] == 4096).all()
+    k = acc[:, :3].astype(np.float64) - comp[:, :3].astype(np.float64)
+    ref = acc64[:, :3]
+    nz = np.abs(ref) > 0
+    rel = np.abs(k - ref)[nz] / np.abs(ref)[nz]
+    naive = np.abs(acc[:, :3].astype(np.float64) - ref)[nz] / np.abs(ref)[nz]
+    print(f"Kahan FP32 vs FP64 at 4096 spp: max {rel.max():.3e}, median {np.median(rel):.3e}; "
+          f"without the compensation: max {naive.max():.3e}, median {np.median(naive):.3e}")
+    assert rel.max() < 1e-6 and np.median(rel) < 1e-7
+    gpu_ctx.destroy_job(s.job_id())
