@@ -132,10 +132,11 @@ def flops_per_path(host):
 
 
 def cpu_sampler(host, prefer_reference=True):
-    """A callable running `n` random pixels x 1 frame of the workload on every host core, its kind
-    ("reference": the reference's shader built for the CPU; "port": the oracle), and a callable
-    giving the threads the last run used. With the prebuilt reference library nothing of the
-    package's own native code is loaded: pixels are seeded by the numpy restatement."""
+    """A callable running `n` random pixels x `frames` frames of the workload on every host core
+    (returns seconds), its kind ("reference": the reference's shader built for the CPU; "port":
+    the oracle), and a callable giving the threads the last run used. With the prebuilt reference
+    library nothing of the package's own native code is loaded: pixels are seeded by the numpy
+    restatement."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle
     W, H = host.width, host.height
@@ -151,11 +152,11 @@ def cpu_sampler(host, prefer_reference=True):
         rlib, p, tables, keep = ref
         calls = host.scene_uniforms()
 
-        def run(n):
+        def run(n, frames=1):
             pix = np.sort(rs.choice(W * H, n, replace=False))
             rng0 = oracle.seed_pixels(host.seed, pix)
             t = time.perf_counter()
-            rlib.render(p, calls, tables, W, H, pix, 1, rng0, threads=0)
+            rlib.render(p, calls, tables, W, H, pix, frames, rng0, threads=0)
             return time.perf_counter() - t
         return run, "reference", rlib.last_team, (keep,)
     lib = oracle.OracleLib(host.sceneObj.shader(), host.scene_opts())
@@ -163,24 +164,26 @@ def cpu_sampler(host, prefer_reference=True):
     sh = host.scene_shader()
     ub = oracle.pack_uniforms(lib.cpp, sh.calls, sh.textures)
 
-    def run(n):
+    def run(n, frames=1):
         pix = np.sort(rs.choice(W * H, n, replace=False))
         rng0 = oracle.seed_pixels(host.seed, pix)
         t = time.perf_counter()
-        lib.render(p, ub, W, H, pix, 1, rng0, threads=0)
+        lib.render(p, ub, W, H, pix, frames, rng0, threads=0)
         return time.perf_counter() - t
     return run, "port", lib.last_team, (keep,)
 
 
-def cpu_baseline(host, budget_s):
+def cpu_baseline(host, budget_s, frames=64):
+    """The workload at its full spp (`frames` frames per pixel) on a random pixel sample sized to
+    about `budget_s` seconds, every host core."""
     run, kind, team, keep = cpu_sampler(host)
-    t = run(2000)  # calibration
+    t = run(2000)  # calibration, 1 frame each
     rate = 2000 / max(t, 1e-6)
-    n = int(min(host.width * host.height, max(2000, rate * budget_s)))
-    dt = run(n)
+    n = int(min(host.width * host.height, max(64, rate * budget_s / frames)))
+    dt = run(n, frames)
     cores = team()
-    return {"value": n / dt, "unit": "path samples/s", "cores": cores, "kind": kind,
-            "sample": f"{n} random pixels of the {host.width}x{host.height} workload, 1 frame each "
+    return {"value": n * frames / dt, "unit": "path samples/s", "cores": cores, "kind": kind,
+            "sample": f"{n} random pixels of the {host.width}x{host.height} workload, {frames} frames (its full spp) each "
                       f"({dt:.1f} s on {cores} host threads of {os.cpu_count()})"}
 
 
@@ -214,15 +217,17 @@ def reference_arm(args, rank):
     from snelly_b200.testing import HostSnelly
     host = HostSnelly(workload_scene(args))
     run, kind, team, keep = cpu_sampler(host)
+    frames = max(1, args.spp_per_step)
     t = run(1000)
-    per_step = int(min(host.width * host.height, max(1000, (1000 / max(t, 1e-6)) * args.cpu_seconds / max(1, args.steps))))
+    rate = 1000 / max(t, 1e-6)  # path samples/s
+    per_step = int(min(host.width * host.height, max(16, rate * args.cpu_seconds / max(1, args.steps) / frames)))
     for _ in range(args.warmup):
-        run(min(per_step, 2000))
-    times = [run(per_step) for _ in range(args.steps)]
-    value = per_step * args.steps / sum(times)
+        run(min(per_step, 64), frames)
+    times = [run(per_step, frames) for _ in range(args.steps)]
+    value = per_step * frames * args.steps / sum(times)
     cores = team()
-    sample = (f"{per_step} random pixels x 1 frame per step of the {host.width}x{host.height} workload "
-              f"(a bounded sample of its {args.spp_per_step}-frame step; {cores} host threads of {os.cpu_count()})")
+    sample = (f"{per_step} random pixels x {frames} frames (the step's full spp) per step of the {host.width}x{host.height} "
+              f"workload (a bounded pixel sample of the step; {cores} host threads of {os.cpu_count()})")
     native = [l.split()[-1] for l in open("/proc/self/maps") if "libsnelly" in l] if os.path.exists("/proc/self/maps") else []
     out = {"impl": "reference", "metric": METRIC, "value": value, "unit": "path samples/s", "n_gpus": args.gpus,
            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * sum(times) / args.steps,

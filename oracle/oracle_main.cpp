@@ -106,7 +106,7 @@ int oracle_render(const SnellyParams* P, const void* uniforms, int width, int he
 #pragma omp single nowait
     g_last_team = omp_get_num_threads();
 #endif
-#pragma omp for schedule(dynamic, 16)
+#pragma omp for schedule(dynamic, 1)
   for (int k = 0; k < n; ++k) {
     int idx = pixels[k];
     int x = idx % width, y = idx / width;
@@ -152,7 +152,7 @@ int oracle_firsthit(const SnellyParams* P, const void* uniforms, int mode, int w
 #pragma omp single nowait
     g_last_team = omp_get_num_threads();
 #endif
-#pragma omp for schedule(dynamic, 16)
+#pragma omp for schedule(dynamic, 1)
   for (int k = 0; k < n; ++k) {
     int idx = pixels[k];
     int x = idx % width, y = idx / width;

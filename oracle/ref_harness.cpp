@@ -71,7 +71,7 @@ extern "C" int ref_pick(const void* block, size_t block_bytes, size_t off_mouse,
 #endif
     std::vector<unsigned char> local(block_bytes + 16);
     unsigned char* lb = local.data();
-#pragma omp for schedule(dynamic, 16)
+#pragma omp for schedule(dynamic, 1)
     for (int k = 0; k < n; ++k) {
       std::memcpy(lb, block, block_bytes);
       int idx = pixels[k], x = idx % width, y = idx / width;
@@ -107,7 +107,7 @@ extern "C" int ref_render(const void* block, size_t block_bytes, size_t off_radi
     unsigned char* lb = local.data();
     float rad[4], st[4];
     glsl::sampler2D radS{rad, 1, 1, 4, 0, 0, 0}, rngS{st, 1, 1, 4, 0, 0, 0};
-#pragma omp for schedule(dynamic, 16)
+#pragma omp for schedule(dynamic, 1)
     for (int k = 0; k < n; ++k) {
       std::memcpy(lb, block, block_bytes);
       std::memcpy(lb + off_radiance, &radS, sizeof radS);

@@ -8,7 +8,7 @@
 #define SNELLY_MEGA_MIN_BLOCKS 5
 #endif
 #ifndef SNELLY_SHADE_MIN_BLOCKS
-#define SNELLY_SHADE_MIN_BLOCKS 4
+#define SNELLY_SHADE_MIN_BLOCKS 5
 #endif
 
 // Render modes (the values of SNELLY_MODE_* in snelly.h).

@@ -657,7 +657,7 @@ extern "C" __global__ void __launch_bounds__(SNELLY_BLOCK, SNELLY_SHADE_MIN_BLOC
 // registers and no material dispatch): misses and finishing paths, surface, metal, dielectric.
 // The host runs them back to back in place of snelly_wf_shade when the autotuner prefers it.
 #ifndef SNELLY_SHADE_SEG_MIN_BLOCKS
-#define SNELLY_SHADE_SEG_MIN_BLOCKS 4
+#define SNELLY_SHADE_SEG_MIN_BLOCKS 5
 #endif
 extern "C" __global__ void __launch_bounds__(SNELLY_BLOCK, SNELLY_SHADE_SEG_MIN_BLOCKS) snelly_wf_shade_miss(
     const JobRec* __restrict__ jobs, const SnellyParams* __restrict__ gparams, WfBuffers B, int it) {

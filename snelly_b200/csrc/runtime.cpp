@@ -360,6 +360,14 @@ int Context::compile_module(const std::string& src, int math_mode, std::shared_p
     else
       cudaGetLastError();
   }
+  if (m->f_wf_shade) {  // one resident wave of the shade stage's grid-stride loop
+    int nb = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, (const void*)m->f_wf_shade, SNELLY_BLOCK, 0) == cudaSuccess &&
+        nb > 0)
+      m->shade_blocks_per_sm = nb;
+    else
+      cudaGetLastError();
+  }
   size_t sz = 0;
   if (m->f_wf_generate) {  // the path-record size the wavefront kernels were compiled for
     int* rp = nullptr;

@@ -61,6 +61,7 @@ struct Module {
   cudaKernel_t f_firsthit = nullptr, f_ptsimple = nullptr;
   int extend_blocks_per_sm = 8;  // resident 128-thread blocks of the persistent extend stage (occupancy query)
   int extend_blocks_per_sm64 = 16;  // the same for 64-thread blocks
+  int shade_blocks_per_sm = 4;      // resident 128-thread blocks of the shade stage (occupancy query)
   char* c_params = nullptr;  // device addresses of the constant banks
   char* c_uniforms = nullptr;
   size_t c_uniforms_bytes = 0, slot_uniform_bytes = 0;

@@ -210,7 +210,7 @@ int Context::enqueue_wavefront(const std::vector<Job*>& js, const std::vector<in
       // find nothing to do: at most 3 rays (continuation, sky and sun shadows) per unfinished path.
       const long long left = R.left;
       const long long extend_blocks = (long long)sm_count * (bs < 128 ? m.extend_blocks_per_sm64 : m.extend_blocks_per_sm);
-      const long long shade_blocks = (long long)sm_count * 4 * (128 / bs);
+      const long long shade_blocks = (long long)sm_count * m.shade_blocks_per_sm * (128 / bs);
       const int eb = (int)std::max<long long>(sm_count, std::min(extend_blocks, (3 * left + bs - 1) / bs));
       const int sb = (int)std::max<long long>(sm_count, std::min(shade_blocks, (left + bs - 1) / bs));
       const bool split = cf.shade_split && m.f_wf_shade_seg[0];

@@ -89,6 +89,67 @@ class LowSunNoSky(PlainSphere):
         pass
 
 
+class DispersiveSphere:
+    """A rough dielectric sphere of radius 1 on a diffuse ground plane y = -1 under a 2-degree
+    sun and a sky, dispersive, maxBounces 6: the scene of the IOR-model parity cases. `dielectric`
+    names one of the reference's registered dielectrics (js/materials.js:1125-1147); `abbe`, when
+    given, sets the Abbe number (and `ior` the refractive index at the d line) of the Abbe model."""
+
+    width, height = 48, 48
+
+    def __init__(self, width=None, height=None, dielectric="Rutile", abbe=None, ior=None):
+        if width:
+            self.width = width
+        if height:
+            self.height = height
+        self.dielectric, self.abbe, self.ior = dielectric, abbe, ior
+
+    def init(self, snelly):
+        r = snelly.getRenderer()
+        r.width, r.height = self.width, self.height
+        r.dispersive = True
+        r.interactive = False
+        r.maxBounces = 6
+        r.maxMarchSteps = 256
+        r.skyPower = math.log10(0.6)
+        r.sunPower = math.log10(12.0)
+        r.sunAngularSize = 2.0
+        r.sunLatitude = 40.0
+        r.sunLongitude = 200.0
+        cam = snelly.getCamera()
+        cam.fov = 40.0
+        cam.position.set(0.4, 1.2, 4.2)
+        cam.aperture = -math.inf
+        snelly.getControls().target.set(0.0, -0.2, 0.0)
+        m = snelly.getMaterials()
+        d = m.loadDielectric(self.dielectric)
+        if self.abbe is not None:
+            d.abbe = self.abbe
+        if self.ior is not None:
+            d.iorVal = self.ior
+        d.roughness = 0.03
+        s = m.loadSurface()
+        s.diffuseAlbedo = [0.7, 0.7, 0.7]
+        s.specAlbedo = [0.0, 0.0, 0.0]
+        s.roughness = 0.4
+
+    def shader(self):
+        return """
+float SDF_DIELECTRIC(vec3 X)
+{
+    return length(X) - 1.0;
+}
+
+float SDF_SURFACE(vec3 X)
+{
+    return X.y + 1.0;
+}
+"""
+
+    def getMinLengthScale(self):
+        return 1.0e-4
+
+
 def c1_camera(seed=2):
     """Camera pose of C1 drawn from `seed`: a point at distance U(4.5, 6) from the look-at point
     (0.6, 0, 0), azimuth U(60, 120) degrees about +y from the +x axis (so the sponge and the gold

@@ -3,10 +3,13 @@
 Requests (a scene, a resolution, a target of spp or of relative noise on the mean luminance)
 arrive over time. The server admits waiting requests in arrival order while its HBM budget
 allows, keeps every admitted job's per-pixel state resident on the device, and on each tick
-advances every active job by one progressive frame in batched launches (snelly_advance_batch:
-jobs of one scene module share launches, different modules overlap on separate streams). A job
-leaves when it reaches its target; its image is read back and its memory returned to the budget,
-so requests that arrive while others render join as soon as memory frees up.
+advances every active job in one batched call (snelly_advance_batch: the autotuner's wavefront
+jobs run concurrently as pixel ranges on their own streams, the others share path-per-thread
+launches per scene module, modules on separate streams): a fixed-spp job by up to
+`frames_per_tick` frames, a noise-target job by one frame (its stopping rule reads the image
+statistics after every frame). A job leaves when it reaches its target; its image is read back
+and its memory returned to the budget, so requests that arrive while others render join as soon
+as memory frees up.
 
 Each pixel owns its RNG stream and its accumulation order, so a job's image does not depend on
 what it was batched with (tests/test_gpu_batch.py checks this bit for bit).
@@ -23,10 +26,11 @@ from dataclasses import dataclass, field
 
 import numpy as np
 
-from . import _native as N
 from . import api, scenes
 
-JOB_BYTES_PER_PIXEL = 64 + 16  # rng, Kahan sums + compensations, resolved image (+ margin)
+# per pixel: rng, Kahan sums + compensations, resolved image (80 B), and the wavefront's path
+# record, parked-ray state and queues when the autotuner gives the job the wavefront (<= 420 B)
+JOB_BYTES_PER_PIXEL = 80 + 420
 
 
 @dataclass
@@ -57,24 +61,27 @@ class Result:
 
 
 class Server:
-    def __init__(self, ctx, hbm_budget_bytes, keep_images=False):
+    def __init__(self, ctx, hbm_budget_bytes, keep_images=False, frames_per_tick=4):
         self.ctx = ctx
         self.budget = hbm_budget_bytes
         self.keep_images = keep_images
+        self.frames_per_tick = frames_per_tick
 
     @staticmethod
     def job_bytes(req):
         return req.scene.width * req.scene.height * JOB_BYTES_PER_PIXEL
 
     def warm(self, requests):
-        """Compile every distinct scene module before the clock starts (a server knows its scenes)."""
+        """Compile every distinct scene module and run the autotuner for every (module, image-size
+        class) before the clock starts (a server knows its scenes and sizes)."""
         seen = set()
         for r in requests:
             s = api.Snelly(r.scene, context=self.ctx)
-            key = (r.scene.shader(), bytes(s.scene_opts()))
+            key = (r.scene.shader(), bytes(s.scene_opts()), int(round(math.log2(r.scene.width * r.scene.height))))
             if key not in seen:
                 seen.add(key)
-                s.compileShaders()
+                s.render(0)
+                self.ctx.destroy_job(s.job_id())
 
     def run(self, requests, clock=time.perf_counter):
         pending = sorted(requests, key=lambda r: r.arrival)
@@ -90,8 +97,7 @@ class Server:
                 req = waiting.pop(0)
                 s = api.Snelly(req.scene, context=self.ctx)
                 s.seed = req.seed
-                s.pathtracer.kernelMode = N.KERNEL_MEGA  # batched ticks run the path-per-thread kernel
-                s.render(0)  # allocate + seed
+                s.render(0)  # allocate + seed (the integrator the autotuner chose for this module and size)
                 used += self.job_bytes(req)
                 active[s.job_id()] = {"req": req, "snelly": s, "spp": 0, "admitted": clock() - t0, "means": []}
             if not active:
@@ -100,14 +106,18 @@ class Server:
                 if pending:
                     time.sleep(max(0.0, min(0.01, pending[0].arrival - (clock() - t0))))
                 continue
-            self.ctx.advance_batch({jid: 1 for jid in active})
+            step = {}
+            for jid, a in active.items():
+                req = a["req"]
+                step[jid] = 1 if req.noise_target > 0 else max(1, min(self.frames_per_tick, req.target_spp - a["spp"]))
+            self.ctx.advance_batch(step)
             self.ctx.sync()
             finished = []
             for jid, a in active.items():
-                a["spp"] += 1
+                a["spp"] += step[jid]
                 req = a["req"]
                 s = a["snelly"]
-                samples += s.width * s.height
+                samples += s.width * s.height * step[jid]
                 noise = float("nan")
                 if req.noise_target > 0:
                     st = self.ctx.image_stats(jid)

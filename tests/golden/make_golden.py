@@ -52,6 +52,8 @@ CASES = {
     "hooks": (lambda: scenes.HooksAndMaps(48, 48), 3),
     "mesh": (lambda: scenes.MeshLike(48, 48, res=64), 3),
     "envmap": (lambda: scenes.EnvMapLit(48, 48), 3),
+    "abbe": (lambda: scenes.DispersiveSphere(40, 40, "Abbe dielectric", abbe=32.0, ior=1.62), 3),
+    "polyanskiy": (lambda: scenes.DispersiveSphere(40, 40, "Rutile"), 3),
 }
 SEED = 1
 

@@ -18,6 +18,8 @@ CASES = {
     "hooks": lambda: scenes.HooksAndMaps(48, 48),
     "mesh": lambda: scenes.MeshLike(48, 48, res=64),
     "envmap": lambda: scenes.EnvMapLit(48, 48),
+    "abbe": lambda: scenes.DispersiveSphere(40, 40, "Abbe dielectric", abbe=32.0, ior=1.62),
+    "polyanskiy": lambda: scenes.DispersiveSphere(40, 40, "Rutile"),
 }
 
 
