@@ -728,10 +728,13 @@ SD_FN unsigned hv_mix(unsigned x) {
   x ^= x >> 16;
   return x;
 }
+// The seed of a shadow ray's stream: its origin and direction with the 10 lowest mantissa bits
+// dropped (about 1e-4 relative), so that builds whose arithmetic differs in the last bits (the
+// CPU oracle's transcendentals) draw the same numbers for the same ray.
 SD_FN unsigned hv_seed(const vec3& p, const vec3& d) {
   unsigned h = 0x2545f491u;
   const float v[6] = {p.x, p.y, p.z, d.x, d.y, d.z};
-  for (int k = 0; k < 6; ++k) h = hv_mix(h ^ (unsigned)__float_as_int(v[k]));
+  for (int k = 0; k < 6; ++k) h = hv_mix(h ^ ((unsigned)__float_as_int(v[k]) & 0xfffffc00u));
   return h;
 }
 SD_FN float hv_uniform(unsigned& h) {  // in [0, 1), 24 bits

@@ -77,6 +77,7 @@ struct WfConfig {
   int grab = 32;        // work items a warp claims from the work head at a time
   int refill = 4;       // idle lanes of a warp that trigger a refill
   int block = 128;      // threads per block of the extend and shade launches (64 or 128)
+  int park_left = 0;    // stop parking once at most park_left / 1024 of the paths are unfinished
 };
 
 struct Scene {
@@ -148,8 +149,8 @@ struct Context {
   };
   std::map<std::string, Tuned> tuned;  // autotuner decisions per (module, image-size class)
   // Wavefront defaults; a field set from the environment (SNELLY_WF_SPLIT, SNELLY_WF_DRAIN,
-  // SNELLY_WF_SHADE_SPLIT, SNELLY_WF_CHUNK, SNELLY_WF_GRAB, SNELLY_WF_REFILL, SNELLY_WF_BLOCK) is
-  // also kept fixed by the autotuner.
+  // SNELLY_WF_SHADE_SPLIT, SNELLY_WF_CHUNK, SNELLY_WF_GRAB, SNELLY_WF_REFILL, SNELLY_WF_BLOCK,
+  // SNELLY_WF_PARK_LEFT) is also kept fixed by the autotuner.
   WfConfig wf_default;
   unsigned wf_fixed = 0;             // bit per WfConfig field, in declaration order
   int wf_park_iters = -1;            // iterations that may park rays; -1: 3 x (max_bounces + 2) (SNELLY_WF_PARK_ITERS)
@@ -178,7 +179,7 @@ struct Context {
   void release_wavefront(Job& j);
   int enqueue_wavefront_frames(Job& j, int frames);
   int enqueue_wavefront(const std::vector<Job*>& js, const std::vector<int>& frames,
-                        const std::map<Module*, cudaEvent_t>& after);
+                        const std::map<Module*, cudaEvent_t>& after, bool slot0_ready = false);
   int autotune(Job& j);
   int time_frames(Job& j, int kernel, float* ms_per_frame);
 };

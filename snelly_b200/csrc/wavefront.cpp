@@ -72,15 +72,16 @@ void Context::release_wavefront(Job& j) {
 int Context::enqueue_wavefront_frames(Job& j, int frames) {
   std::vector<Job*> js{&j};
   std::vector<int> fs{frames};
-  return enqueue_wavefront(js, fs, {});
+  return enqueue_wavefront(js, fs, {}, true);
 }
 
 // The wavefront frames of several jobs at once. Every job's pixel ranges ("parts") get their own
 // stream; a job's parameters and scene uniforms go to its own constant-memory slot, uploaded on
 // its first part's stream once the work it follows is done (`after`: an event per module, for
 // slots that another launch sequence of that module used). Up to SNELLY_MAX_BATCH jobs of one
-// module run concurrently; more wait for the next wave. A single job runs its first part on the
-// context stream, in slot 0 (its parameters are already uploaded there by enqueue_frames).
+// module run concurrently; more wait for the next wave. With `slot0_ready` (one job whose
+// parameters its caller has already uploaded into slot 0 on the context stream, enqueue_frames),
+// the job runs its first part on the context stream in slot 0 and nothing is uploaded.
 //
 // Per frame and part: generate, then iterations of (extend, shade [, subsurface walk]). The first
 // `budgeted` iterations park the slowest rays when their work runs out; after them every
@@ -93,7 +94,7 @@ int Context::enqueue_wavefront_frames(Job& j, int frames) {
 // the stragglers of theirs; the host serves whichever part's read has landed and never waits on
 // one part while another could be fed.
 int Context::enqueue_wavefront(const std::vector<Job*>& js, const std::vector<int>& frames,
-                               const std::map<Module*, cudaEvent_t>& after) {
+                               const std::map<Module*, cudaEvent_t>& after, bool slot0_ready) {
   for (size_t q = 0; q < js.size(); ++q) {
     Job& j = *js[q];
     Module& m = *j.module;
@@ -101,7 +102,8 @@ int Context::enqueue_wavefront(const std::vector<Job*>& js, const std::vector<in
         m.wf_rec_f4 != j.wfb[0].rec_f4)
       return fail(SNELLY_EINVAL, "wavefront integrator not available for this job");
   }
-  const bool single = js.size() == 1;
+  if (slot0_ready && js.size() != 1) return fail(SNELLY_EINVAL, "slot 0 holds one job's parameters");
+  const bool single = slot0_ready;
   // waves: at most SNELLY_MAX_BATCH concurrent jobs per module (one constant-memory slot each)
   std::vector<int> wave(js.size(), 0), slot(js.size(), 0);
   {
@@ -202,7 +204,10 @@ int Context::enqueue_wavefront(const std::vector<Job*>& js, const std::vector<in
       const int budgeted = wf_park_iters >= 0 ? std::min(wf_park_iters, 8 * nominal) : 3 * nominal;
       int it = R.it;
       const WfConfig& cf = j.wfc;
-      int drain = it < budgeted ? cf.drain : 0;
+      // rays are parked in the first `budgeted` iterations while more than park_left / 1024 of
+      // the part's paths are unfinished (per the latest read): a few stragglers are then marched
+      // to the end in one launch instead of a few dozen steps per iteration
+      int drain = (it < budgeted && R.left * 1024 > (long long)cf.park_left * B.paths) ? cf.drain : 0;
       int chunk = cf.chunk, grab = cf.grab, refill = cf.refill;
       const int bs = cf.block;
       // Both stages take their work from device-side counters whatever their grid. Once a read has
@@ -339,8 +344,9 @@ int Context::time_frames(Job& j, int kernel, float* ms_per_frame) {
 // The integrator choice of SNELLY_KERNEL_AUTO and the wavefront's launch configuration, per
 // (scene module, image-size class): the first such job times, on its own buffers, the wavefront
 // with each value of one configuration field in turn (the best so far for the others; one pass
-// over pixel ranges, per-material shading, drain steps, refill chunk, claim size, refill threshold
-// and block shape; fields fixed by the environment are not varied), then the path-per-thread
+// over pixel ranges, per-material shading, drain steps, refill chunk, claim size, refill threshold,
+// block shape and the unfinished-path fraction below which parking stops; fields fixed by the
+// environment are not varied), then the path-per-thread
 // kernel, keeps the fastest and caches the decision; the job's state is seeded again afterwards
 // by the caller. The size class is the power of two nearest the pixel count (tail effects make
 // the choice size-dependent).
@@ -379,7 +385,7 @@ int Context::autotune(Job& j) {
       std::vector<int> values;
     } fields[] = {{&WfConfig::parts, {1, 2, 3, 4}},  {&WfConfig::shade_split, {0, 1}}, {&WfConfig::drain, {16, 32, 64}},
                   {&WfConfig::chunk, {4, 8, 16}},   {&WfConfig::grab, {16, 32, 64}},  {&WfConfig::refill, {2, 4, 8}},
-                  {&WfConfig::block, {64, 128}}};
+                  {&WfConfig::block, {64, 128}},    {&WfConfig::park_left, {0, 8, 32, 128}}};
     for (unsigned k = 0; k < sizeof fields / sizeof fields[0]; ++k) {
       if (wf_fixed & (1u << k)) continue;
       for (int v : fields[k].values) {

@@ -173,7 +173,7 @@ def make_stat(name):
     print(f"stat_{name}: {ys.shape[1]} pixels, {batches} x {frames} frames, image mean Y {ys.mean():.6f}")
 
 
-FULL_BATCHES, FULL_FRAMES, FULL_SEED0, FULL_TILE = 14, 16, 7000, 30
+FULL_BATCHES, FULL_FRAMES, FULL_SEED0, FULL_TILE = 10, 16, 7000, 30
 
 
 def make_full_c1():

@@ -80,3 +80,29 @@ def test_wavefront_jobs_in_a_batch(gpu_ctx):
         assert (got[k][..., 3] == fr).all(), k
         np.testing.assert_array_equal(got[k], ref[1], err_msg=f"job {k}")
         gpu_ctx.destroy_job(ref[0].job_id())
+
+
+def test_single_wavefront_job_in_a_batch(gpu_ctx):
+    """A batch whose only wavefront job shares the call with path-per-thread jobs (what a serving
+    tick often is): the wavefront job's parameters go to its own slot like any batch job's, and its
+    image equals the job rendered alone, bit for bit, over two calls."""
+    from snelly_b200 import _native as N
+    spec = [(scenes.DispersiveFractal, 80, 45, N.KERNEL_WAVEFRONT, 31), (scenes.PlainSphere, 40, 40, N.KERNEL_MEGA, 32),
+            (scenes.HooksAndMaps, 32, 32, N.KERNEL_MEGA, 33)]
+    jobs = []
+    for cls, w, h, km, sd in spec:
+        s = api.Snelly(cls(w, h), context=gpu_ctx)
+        s.seed = sd
+        s.pathtracer.kernelMode = km
+        s.render(0)
+        jobs.append(s)
+    # another job's parameters in slot 0 of the fractal's module, as a solo render leaves them
+    other = gpu_render(gpu_ctx, scenes.DispersiveFractal(64, 64), 1, seed=99, kernel_mode=N.KERNEL_WAVEFRONT)[0]
+    for _ in range(2):
+        gpu_ctx.advance_batch({s.job_id(): 2 for s in jobs})
+    for (cls, w, h, km, sd), s in zip(spec, jobs):
+        ref = gpu_render(gpu_ctx, cls(w, h), 4, seed=sd, kernel_mode=km)
+        np.testing.assert_array_equal(s.readback(), ref[1])
+        gpu_ctx.destroy_job(ref[0].job_id())
+        gpu_ctx.destroy_job(s.job_id())
+    gpu_ctx.destroy_job(other.job_id())

@@ -104,8 +104,8 @@ def test_bench_config_statistics_matched_spp(gpu_ctx, case):
 
 def test_bench_config_image_mean_high_spp(gpu_ctx):
     """The benchmark frame's mean luminance within 0.5% of the reference's: the whole 1080p frame
-    at 256 spp on the GPU (16 jobs of 16 frames, independent seeds) against the reference at 224 spp
-    (14 batches of 16 frames), about 0.1% standard error on each side. Also every 30x30-pixel tile's
+    at 256 spp on the GPU (16 jobs of 16 frames, independent seeds) against the reference at 160 spp
+    (10 batches of 16 frames), about 0.02% standard error on each side. Also every 30x30-pixel tile's
     mean luminance: at most 1% of tiles beyond 4 standard errors of the difference."""
     g = dict(np.load(os.path.join(GOLDEN, "full_c1.npz")))
     W, H, t = 1920, 1080, int(g["tile"])
