@@ -606,27 +606,30 @@ __device__ __noinline__ Hit march_ray(int job, vec3 start, vec3 dir, float maxDi
   for (int n = 0; n < MAX_MARCH_STEPS; ++n) {
     vec3 p = start + t * dir;
     sdf = 1.0e20f;
-#ifdef HAS_SURFACE
-    {
-      float d = fabsf(sc.SDF_SURFACE(p));
-      if (d < minMarch) { h.mat = MAT_SURFA; h.p = start + t * dir; h.hit = true; return h; }
-      sdf = fminf(sdf, d);
-    }
+    // every SDF, then the hit: the first of surface, metal, dielectric below the threshold (the
+    // reference returns at the first, PT:906-912; the others' values are not used then)
+    int m = MAT_INVAL;
+#ifdef HAS_DIELECTRIC
+    const float d3 = fabsf(sc.SDF_DIELECTRIC(p));
+    m = d3 < minMarch ? MAT_DIELE : m;
+    sdf = fminf(sdf, d3);
 #endif
 #ifdef HAS_METAL
-    {
-      float d = fabsf(sc.SDF_METAL(p));
-      if (d < minMarch) { h.mat = MAT_METAL; h.p = start + t * dir; h.hit = true; return h; }
-      sdf = fminf(sdf, d);
-    }
+    const float d2 = fabsf(sc.SDF_METAL(p));
+    m = d2 < minMarch ? MAT_METAL : m;
+    sdf = fminf(sdf, d2);
 #endif
-#ifdef HAS_DIELECTRIC
-    {
-      float d = fabsf(sc.SDF_DIELECTRIC(p));
-      if (d < minMarch) { h.mat = MAT_DIELE; h.p = start + t * dir; h.hit = true; return h; }
-      sdf = fminf(sdf, d);
-    }
+#ifdef HAS_SURFACE
+    const float d1 = fabsf(sc.SDF_SURFACE(p));
+    m = d1 < minMarch ? MAT_SURFA : m;
+    sdf = fminf(sdf, d1);
 #endif
+    if (m != MAT_INVAL) {
+      h.mat = m;
+      h.p = start + t * dir;
+      h.hit = true;
+      return h;
+    }
     t += sgn * sdf;
     if (fabsf(t) >= maxDist) return h;
   }

@@ -421,27 +421,26 @@ extern "C" __global__ void __launch_bounds__(SNELLY_BLOCK) snelly_wf_extend(WfBu
       const vec3 p = first ? o : o + t * d;
       float sdf = 1.0e20f;
       int m = MAT_INVAL;
-#ifdef HAS_SURFACE
-      {
-        float dd = fabsf(sc.SDF_SURFACE(p));
-        if (!first && dd < minMarch) m = MAT_SURFA;
-        sdf = fminf(sdf, dd);
-      }
+      // Every SDF, unconditionally, and the hit named by selects: the first of surface, metal,
+      // dielectric below the threshold, as the reference's early returns decide (PT:906-912). No
+      // branch around an SDF, so the warp does not split where one lane's ray hits; the extra
+      // evaluations on a hit step change nothing (the march ends there).
+#ifdef HAS_DIELECTRIC
+      const float d3 = fabsf(sc.SDF_DIELECTRIC(p));
+      m = d3 < minMarch ? MAT_DIELE : m;
+      sdf = fminf(sdf, d3);
 #endif
 #ifdef HAS_METAL
-      if (m == MAT_INVAL) {
-        float dd = fabsf(sc.SDF_METAL(p));
-        if (!first && dd < minMarch) m = MAT_METAL;
-        sdf = fminf(sdf, dd);
-      }
+      const float d2 = fabsf(sc.SDF_METAL(p));
+      m = d2 < minMarch ? MAT_METAL : m;
+      sdf = fminf(sdf, d2);
 #endif
-#ifdef HAS_DIELECTRIC
-      if (m == MAT_INVAL) {
-        float dd = fabsf(sc.SDF_DIELECTRIC(p));
-        if (!first && dd < minMarch) m = MAT_DIELE;
-        sdf = fminf(sdf, dd);
-      }
+#ifdef HAS_SURFACE
+      const float d1 = fabsf(sc.SDF_SURFACE(p));
+      m = d1 < minMarch ? MAT_SURFA : m;
+      sdf = fminf(sdf, d1);
 #endif
+      if (first) m = MAT_INVAL;  // the origin is never a hit (its distance only fixes the sign)
       if (first) {  // the distance at the origin fixes the marching sign and the first step
         first = false;
         sgn = glsl::sign(sdf);

@@ -8,7 +8,7 @@ import pytest
 
 from helpers import gpu_render, oracle_render, welch_p
 from snelly_b200 import _native as N
-from snelly_b200 import scenes
+from snelly_b200 import api, scenes
 from snelly_b200.testing import HostSnelly
 
 pytestmark = pytest.mark.gpu
@@ -91,7 +91,11 @@ def test_kahan_fp32_against_fp64_on_c2_4096spp(gpu_ctx):
     """C2 with its cloud, 96x96 at 4096 spp: the FP32 Kahan-compensated sums against the FP64
     accumulation of the same per-frame contributions. Bars (the statement of the accumulation
     error): maximum relative error per pixel and channel below 1e-6, median below 1e-7."""
-    s, img = gpu_render(gpu_ctx, scenes.PyroclasticSubsurface(96, 96), 4096, seed=4, fp64=True)
+    s = api.Snelly(scenes.PyroclasticSubsurface(96, 96), context=gpu_ctx)
+    s.seed = 4
+    s.fp64 = True
+    s.pathtracer.maxSpp = 1 << 30  # the renderer's default stops progressive rendering at 1024 spp
+    s.render(4096)
     rng, acc, comp, acc64 = s.readback_state()
     assert (acc64[:, 3] == 4096).all() and (acc[:, 3] == 4096).all()
     k = acc[:, :3].astype(np.float64) - comp[:, :3].astype(np.float64)
