@@ -201,7 +201,7 @@ int snelly_readback_state(snelly_ctx* ctx, uint64_t job_id, uint32_t* rng, float
 /* The integrator a job's frames run: SNELLY_KERNEL_MEGA or SNELLY_KERNEL_WAVEFRONT (a scene
  * created with SNELLY_KERNEL_AUTO gets the autotuner's choice for its module and image size, once
  * per size class: the wavefront's launch configuration by one pass of coordinate descent, each
- * candidate timed over a warm-up frame and about 5 ms of frames, then the path-per-thread
+ * candidate timed over a warm-up frame and about 12 ms of frames, then the path-per-thread
  * kernel). No counterpart in the reference, which has one fragment program. */
 int snelly_job_kernel(snelly_ctx* ctx, uint64_t job_id, int* kernel_mode);
 /* A wavefront job's launch configuration, SNELLY_WF_CONFIG_FIELDS ints: concurrent pixel ranges,

@@ -77,7 +77,7 @@ struct WfConfig {
   int grab = 32;        // work items a warp claims from the work head at a time
   int refill = 4;       // idle lanes of a warp that trigger a refill
   int block = 128;      // threads per block of the extend and shade launches (64 or 128)
-  int park_left = 0;    // stop parking once at most park_left / 1024 of the paths are unfinished
+  int park_left = 32;   // stop parking once at most park_left / 1024 of the paths are unfinished
 };
 
 struct Scene {

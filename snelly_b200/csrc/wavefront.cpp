@@ -78,8 +78,8 @@ int Context::enqueue_wavefront_frames(Job& j, int frames) {
 // The wavefront frames of several jobs at once. Every job's pixel ranges ("parts") get their own
 // stream; a job's parameters and scene uniforms go to its own constant-memory slot, uploaded on
 // its first part's stream once the work it follows is done (`after`: an event per module, for
-// slots that another launch sequence of that module used). Up to SNELLY_MAX_BATCH jobs of one
-// module run concurrently; more wait for the next wave. With `slot0_ready` (one job whose
+// slots that another launch sequence of that module used). Up to SNELLY_MAX_BATCH jobs run
+// concurrently; more wait for the next wave. With `slot0_ready` (one job whose
 // parameters its caller has already uploaded into slot 0 on the context stream, enqueue_frames),
 // the job runs its first part on the context stream in slot 0 and nothing is uploaded.
 //
@@ -104,14 +104,14 @@ int Context::enqueue_wavefront(const std::vector<Job*>& js, const std::vector<in
   }
   if (slot0_ready && js.size() != 1) return fail(SNELLY_EINVAL, "slot 0 holds one job's parameters");
   const bool single = slot0_ready;
-  // waves: at most SNELLY_MAX_BATCH concurrent jobs per module (one constant-memory slot each)
+  // waves of at most SNELLY_MAX_BATCH concurrent jobs (so at most that many jobs' ranges and
+  // streams at a time, and one constant-memory slot per job of a module)
   std::vector<int> wave(js.size(), 0), slot(js.size(), 0);
   {
-    std::map<Module*, int> seen;
+    std::map<std::pair<int, Module*>, int> seen;
     for (size_t q = 0; q < js.size(); ++q) {
-      int n = seen[js[q]->module]++;
-      wave[q] = n / SNELLY_MAX_BATCH;
-      slot[q] = n % SNELLY_MAX_BATCH;
+      wave[q] = (int)(q / SNELLY_MAX_BATCH);
+      slot[q] = seen[{wave[q], js[q]->module}]++;
     }
   }
   const int nwaves = js.empty() ? 0 : *std::max_element(wave.begin(), wave.end()) + 1;
@@ -298,7 +298,7 @@ int Context::enqueue_wavefront(const std::vector<Job*>& js, const std::vector<in
 }
 
 // Frames of one job with the given integrator on its own buffers, timed with events on the
-// context stream: one warm-up frame, then enough frames for about 5 ms (2 to 16); the per-frame
+// context stream: one warm-up frame, then enough frames for about 12 ms (2 to 16); the per-frame
 // time. The job's state is seeded again afterwards by the caller.
 int Context::time_frames(Job& j, int kernel, float* ms_per_frame) {
   void* tables = j.tables.ptr;
@@ -328,7 +328,7 @@ int Context::time_frames(Job& j, int kernel, float* ms_per_frame) {
     else cudaEventElapsedTime(&warm, e[0], e[1]);
   }
   if (!rc) {
-    n = std::max(2, std::min(16, (int)std::ceil(5.0f / std::max(warm, 1e-3f))));
+    n = std::max(2, std::min(16, (int)std::ceil(12.0f / std::max(warm, 1e-3f))));
     rc = frames(n);
   }
   if (!rc) {
