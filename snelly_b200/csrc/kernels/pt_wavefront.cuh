@@ -239,6 +239,16 @@ SD_FN void dec_hit(float w, bool& hit, int& mat) {
   mat = (v >> 1) - 1;
 }
 
+// Entry of every wavefront kernel. With programmatic dependent launch (the host's launch attribute)
+// the kernel may start while the previous kernel of its stream is still running: it first waits
+// for that grid to complete and its writes to be visible (griddepcontrol.wait, a no-op without
+// the attribute), then lets the next kernel of the stream begin launching, so its launch and block
+// set-up overlap this one's work.
+SD_FN void wf_kernel_entry() {
+  asm volatile("griddepcontrol.wait;" ::: "memory");
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+
 // Final contribution of a path: XYZ added to the pixel's Kahan sums, RNG written back.
 SD_FN void finish_path(const JobRec& J, const WfBuffers& B, int path, const Rad& L, const vec3& xyzw, const Rng& g) {
   long long i = (long long)B.pixel_begin + path;
@@ -274,6 +284,7 @@ extern "C" __global__ void __launch_bounds__(SNELLY_BLOCK) snelly_wf_generate(co
                                                                            const SnellyParams* __restrict__ gparams,
                                                                            WfBuffers B) {
   using namespace sdev;
+  wf_kernel_entry();
   const JobRec& J = jobs[0];
   int path = blockIdx.x * blockDim.x + threadIdx.x;
   if (B.rec_f4 != snelly_wf_rec_f4) {  // buffers laid out for another record size: trace nothing
@@ -331,6 +342,7 @@ extern "C" __global__ void __launch_bounds__(SNELLY_BLOCK) snelly_wf_generate(co
 extern "C" __global__ void __launch_bounds__(SNELLY_BLOCK) snelly_wf_extend(WfBuffers B, int it, int drain, int chunk,
                                                                                   int grab, int refill) {
   using namespace sdev;
+  wf_kernel_entry();
   const SnellyParams& P = c_params[B.slot];
   Scene sc(uniforms_of(B.slot));
   sc.INIT();
@@ -616,6 +628,7 @@ SD_FN void shade_push(const WfBuffers& B, int* cnt, int nxt, int path, bool push
 template <int MAT>
 SD_FN void shade_segments(const JobRec* jobs, const SnellyParams* gparams, const WfBuffers& B, int it, int seg_lo,
                           int seg_hi) {
+  wf_kernel_entry();
   const JobRec& J = jobs[0];
   int* cnt = B.cnt;
   const int cur = it & 1, nxt = cur ^ 1;
@@ -689,6 +702,7 @@ extern "C" __global__ void __launch_bounds__(SNELLY_BLOCK, SNELLY_SHADE_SEG_MIN_
 extern "C" __global__ void __launch_bounds__(SNELLY_BLOCK, SNELLY_SHADE_MIN_BLOCKS) snelly_wf_sss(
     const JobRec* __restrict__ jobs, const SnellyParams* __restrict__ gparams, WfBuffers B, int it) {
   using namespace sdev;
+  wf_kernel_entry();
   const JobRec& J = jobs[0];
   const SnellyParams& P = c_params[B.slot];
   int* cnt = B.cnt;

@@ -686,6 +686,7 @@ int snelly_init(snelly_ctx** out, int device, size_t budget) {
   if (!file_exists(c->kernel_dir + "/pt_kernels.cu"))
     return fail(SNELLY_EINVAL, "kernel sources not found under " + c->kernel_dir);
   if (const char* pi = getenv("SNELLY_WF_PARK_ITERS")) c->wf_park_iters = atoi(pi);
+  if (const char* pd = getenv("SNELLY_WF_PDL")) c->wf_pdl = atoi(pd) ? 1 : 0;
   {  // wavefront defaults from the environment; those given are not tuned
     WfConfig& d = c->wf_default;
     struct {

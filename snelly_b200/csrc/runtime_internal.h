@@ -154,6 +154,7 @@ struct Context {
   WfConfig wf_default;
   unsigned wf_fixed = 0;             // bit per WfConfig field, in declaration order
   int wf_park_iters = -1;            // iterations that may park rays; -1: 3 x (max_bounces + 2) (SNELLY_WF_PARK_ITERS)
+  int wf_pdl = 0;                    // programmatic dependent launch of the wavefront kernels (SNELLY_WF_PDL)
   int* poll_host = nullptr;          // pinned words the wavefront's paths-left reads land in (2 per part)
   size_t poll_cap = 0;
   std::vector<cudaStream_t> wf_pool;  // one stream per concurrently running wavefront part

@@ -189,8 +189,20 @@ int Context::enqueue_wavefront(const std::vector<Job*>& js, const std::vector<in
           if (R.j == &j && R.k > 0) RT_TRY(cudaStreamWaitEvent(R.st, up, 0));
       }
     }
+    // Programmatic dependent launch (wf_pdl): a kernel may begin launching while the previous
+    // kernel of its stream runs; it waits for that grid on entry (wf_kernel_entry).
+    cudaLaunchAttribute pdl_attr[1];
+    pdl_attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    pdl_attr[0].val.programmaticStreamSerializationAllowed = 1;
     auto launch_on = [&](PartRun& R, cudaKernel_t f, int blocks, int threads, void** args) -> int {
-      RT_TRY(cudaLaunchKernel((const void*)f, dim3((unsigned)blocks), dim3((unsigned)threads), args, 0, R.st));
+      cudaLaunchConfig_t lc = {};
+      lc.gridDim = dim3((unsigned)blocks);
+      lc.blockDim = dim3((unsigned)threads);
+      lc.dynamicSmemBytes = 0;
+      lc.stream = R.st;
+      lc.attrs = pdl_attr;
+      lc.numAttrs = wf_pdl ? 1 : 0;
+      RT_TRY(cudaLaunchKernelExC(&lc, (const void*)f, args));
       launches++;
       return SNELLY_OK;
     };
