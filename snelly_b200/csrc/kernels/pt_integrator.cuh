@@ -172,32 +172,54 @@ SD_FN float scatter_prob(const Ctx& c, const Rad& Tr) {
 }
 
 #ifdef HAS_SURFACE
-// Subsurface random walk inside SDF_SURFACE (PT:1464-1518). Returns true at an exit point.
-SD_FN bool sss_walk(const Ctx& c, const vec3& pW, const Frame& f, Rng& g, const Rad& ssAlb, Rad& walkThr, vec3& pExit) {
-  const SnellyParams& P = c.P;
-  vec3 pw = pW - 3.0f * P.minLengthScale * f.n;
+// Subsurface random walk inside SDF_SURFACE (PT:1464-1518), as a start and single steps so that a
+// persistent walker can interleave many walks: the walk's position, direction, throughput and
+// step count.
+struct WalkState {
+  vec3 pw, dw;
+  Rad thr;
+  int n;
+};
+SD_FN void sss_walk_begin(const Ctx& c, const vec3& pW, const Frame& f, Rng& g, WalkState& w) {
+  w.pw = pW - 3.0f * c.P.minLengthScale * f.n;
   float pdf;
   vec3 dl = sample_cosine(g, pdf);
-  vec3 dw = -to_world(dl, f);
-  walkThr = Rad(1.0f);
-  for (int n = 0; n < 2048; ++n) {
-    if (n > P.maxSSSSteps) break;
-    float step = -logf(rand01(g)) * P.subsurfaceMFP * P.lengthScale;
-    Hit h = march_ray(c.job, pw, dw, step);
-    if (h.hit) {
-      pExit = h.p;
-      return true;
-    }
-    if (n > 4) {
-      float cont = glsl::clamp(10.0f * maxc(walkThr), 0.0f, 1.0f);
-      if (rand01(g) < 1.0f - cont) break;
-      walkThr /= cont;
-    }
-    dw = sample_hg(dw, P.subsurfaceAnisotropy, g);
-    pw += step * dw;
-    walkThr *= ssAlb;
+  w.dw = -to_world(dl, f);
+  w.thr = Rad(1.0f);
+  w.n = 0;
+}
+enum { WALK_ON = 0, WALK_EXIT = 1, WALK_END = 2 };
+// One step of the walk: WALK_EXIT with the exit point, WALK_END when the walk stops inside
+// (roulette or the step limit), else WALK_ON.
+SD_FN int sss_walk_step(const Ctx& c, Rng& g, const Rad& ssAlb, WalkState& w, vec3& pExit) {
+  const SnellyParams& P = c.P;
+  if (w.n >= 2048 || w.n > P.maxSSSSteps) return WALK_END;
+  float step = -logf(rand01(g)) * P.subsurfaceMFP * P.lengthScale;
+  Hit h = march_ray(c.job, w.pw, w.dw, step);
+  if (h.hit) {
+    pExit = h.p;
+    return WALK_EXIT;
   }
-  return false;
+  if (w.n > 4) {
+    float cont = glsl::clamp(10.0f * maxc(w.thr), 0.0f, 1.0f);
+    if (rand01(g) < 1.0f - cont) return WALK_END;
+    w.thr /= cont;
+  }
+  w.dw = sample_hg(w.dw, P.subsurfaceAnisotropy, g);
+  w.pw += step * w.dw;
+  w.thr *= ssAlb;
+  ++w.n;
+  return WALK_ON;
+}
+// The whole walk: true at an exit point.
+SD_FN bool sss_walk(const Ctx& c, const vec3& pW, const Frame& f, Rng& g, const Rad& ssAlb, Rad& walkThr, vec3& pExit) {
+  WalkState w;
+  sss_walk_begin(c, pW, f, g, w);
+  int r;
+  while ((r = sss_walk_step(c, g, ssAlb, w, pExit)) == WALK_ON) {
+  }
+  walkThr = w.thr;
+  return r == WALK_EXIT;
 }
 
 // Direct light at a subsurface exit point through a Lambertian lobe (PT:1521-1593).
@@ -403,13 +425,9 @@ struct SssEntry {
 #ifdef HAS_SURFACE
 // The rest of a vertex that chose the subsurface walk (PT:1866-1918): the walk to an exit point,
 // the exit's direct light and the Lambertian continuation direction.
-SD_FN int sss_step(const Ctx& c, PathState& s, const SssEntry& e, Rng& g) {
+// The vertex after a walk that reached an exit point (PT:1884-1918).
+SD_FN int sss_exit(const Ctx& c, PathState& s, float probSSS, const Rad& walkThr, const vec3& pExit, Rng& g) {
   const SnellyParams& P = c.P;
-  Rad walkThr = Rad(0.0f);
-  vec3 pExit(0.0f);
-  Frame fw = e.fr;
-  fw.n = e.ngW;  // geometric normal for the entry (the tangents stay those of the shading frame)
-  if (!sss_walk(c, s.pW, fw, g, e.ssAlb, walkThr, pExit)) return VERTEX_DONE;
   s.pW = pExit;
   vec3 nW = sdf_normal(c.job, pExit, MAT_SURFA);
   Frame fe = make_frame(nW);
@@ -428,10 +446,25 @@ SD_FN int sss_step(const Ctx& c, PathState& s, const SssEntry& e, Rng& g) {
 #endif
   Rad lobe = glsl::mix(Rad(1.0f), dAlbExit, P.subsurfaceDiffuseWeight) / kPi;
   Rad fop = glsl::min(Rad(P.radianceClamp), lobe / fmaxf(kPdfEps, bsdfPdf));
-  s.thr *= fop * fabsf(glsl::dot(woW, nW)) / fmaxf(kPdfEps, e.probSSS);
+  s.thr *= fop * fabsf(glsl::dot(woW, nW)) / fmaxf(kPdfEps, probSSS);
   s.pW += nW * glsl::sign(glsl::dot(s.rayDir, nW)) * 3.0f * P.minLengthScale;
   if (maxc(s.thr) < kThroughputEps) return VERTEX_DONE;
   return VERTEX_CONTINUE;
+}
+
+// The entry's frame for the walk: the geometric normal, with the shading frame's tangents.
+SD_FN Frame sss_walk_frame(const SssEntry& e) {
+  Frame fw = e.fr;
+  fw.n = e.ngW;
+  return fw;
+}
+
+// The rest of a vertex that chose the subsurface walk (PT:1866-1918): the walk, then the exit.
+SD_FN int sss_step(const Ctx& c, PathState& s, const SssEntry& e, Rng& g) {
+  Rad walkThr = Rad(0.0f);
+  vec3 pExit(0.0f);
+  if (!sss_walk(c, s.pW, sss_walk_frame(e), g, e.ssAlb, walkThr, pExit)) return VERTEX_DONE;
+  return sss_exit(c, s, e.probSSS, walkThr, pExit, g);
 }
 #endif
 

@@ -45,7 +45,9 @@ typedef struct JobRec {
 #define WF_LEFT 6   // paths of the frame not finished yet
 #define WF_Q 8      // shade-queue segment counts [2][4]
 #define WF_SSS 16   // subsurface-walk queue count (filled by the shade stage, read by the walk stage)
-#define WF_HEAD 17  // extend work heads, one per iteration
+#define WF_WHEAD 17 // the persistent walker's work head over that queue
+#define WF_XQ 18    // walks that ended (exit queue count, read by the walk-exit stage)
+#define WF_HEAD 19  // extend work heads, one per iteration
 #define WF_MAX_ITERS 300
 #define WF_COUNTERS (WF_HEAD + WF_MAX_ITERS)
 typedef struct WfBuffers {
@@ -59,6 +61,7 @@ typedef struct WfBuffers {
   int* qshade[2];   // shade queues [2] (ping-pong by iteration parity), 4 segments of `paths`
                     // entries each: finish/miss, surface, metal, dielectric
   int* qsss;        // paths whose surface vertex chose the subsurface walk (one iteration's)
+  int* qexit;       // paths whose walk the persistent walker finished (one iteration's)
   int* cnt;         // counters (WF_*)
   int paths;
   int pixel_begin;

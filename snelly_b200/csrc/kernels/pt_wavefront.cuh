@@ -352,6 +352,8 @@ extern "C" __global__ void __launch_bounds__(SNELLY_BLOCK) snelly_wf_extend(WfBu
     cnt[WF_A + nxt] = 0;
     cnt[WF_S + nxt] = 0;
     cnt[WF_SSS] = 0;
+    cnt[WF_WHEAD] = 0;
+    cnt[WF_XQ] = 0;
     for (int k = 0; k < 4; ++k) cnt[WF_Q + 4 * nxt + k] = 0;
   }
   const int nA = cnt[WF_A + cur], nS = cnt[WF_S + cur], nC = cnt[WF_C + cur];
@@ -724,6 +726,138 @@ extern "C" __global__ void __launch_bounds__(SNELLY_BLOCK, SNELLY_SHADE_MIN_BLOC
       const vec3 xyzw = wavelength_at(c, st.w);
       const SssEntry e = load_sss(r);
       int rv = sss_step(c, st.s, e, st.g);
+      ++st.vertex;
+      finished = rv == VERTEX_DONE || st.vertex > max_bounces(P) || maxc(st.s.thr) < kThroughputEps;
+      if (finished) {
+        finish_path(J, B, path, st.s.L, xyzw, st.g);
+      } else {
+        st.s.inDiele ? (st.flags |= WF_INDIELE) : (st.flags &= ~WF_INDIELE);
+        store_state(r, st);
+        B.pend[path] = 1;
+        push_active = true;
+      }
+    }
+    shade_push(B, cnt, nxt, path, push_active, 0, false, false, finished);
+  }
+}
+#endif
+
+#ifdef HAS_SURFACE
+// ---- persistent subsurface walker (the alternative to snelly_wf_sss) ------------------------------
+// After a walk the record holds, in place of the entry's bitangent, the exit point and the walk's
+// outcome (R_S2: xyz, w = WALK_EXIT or WALK_END as int bits), and the walk's throughput in place of
+// the subsurface albedo (R_S1.w in dispersive mode, R_S4 in RGB mode).
+//
+// Each lane runs one walk a step at a time (sss_walk_step: one march, the roulette, one phase
+// sample) and, when it ends, takes the next walk of the iteration's walk queue: a warp claims
+// `grab` queue entries per atomic and refills once `refill` lanes are idle, so it stays full
+// however uneven the walks' lengths are. Every path draws its random numbers in the same order as
+// sss_step, so images are the same as with snelly_wf_sss. A finished walk goes to the exit queue.
+extern "C" __global__ void __launch_bounds__(SNELLY_BLOCK) snelly_wf_walk(const JobRec* __restrict__ jobs,
+                                                                       const SnellyParams* __restrict__ gparams,
+                                                                       WfBuffers B, int it, int grab, int refill) {
+  using namespace sdev;
+  wf_kernel_entry();
+  (void)jobs;
+  (void)it;
+  const SnellyParams& P = c_params[B.slot];
+  Scene sc(uniforms_of(B.slot));
+  sc.INIT();
+  const Ctx c{P, gparams, sc, B.slot, 0.0f, vec3(0.0f), Frame()};
+  int* cnt = B.cnt;
+  const int total = cnt[WF_SSS];
+  bool has = false;
+  int path = 0;
+  WalkState w;
+  w.pw = vec3(0.0f);
+  w.dw = vec3(0.0f);
+  w.thr = Rad(0.0f);
+  w.n = 0;
+  Rng g;
+  g.s[0] = g.s[1] = g.s[2] = g.s[3] = 1u;
+  Rad ssAlb = Rad(0.0f);
+  int wbase = 0, wlim = 0;  // the warp's claimed range of queue entries (warp-uniform)
+  bool wdone = false;
+  for (;;) {
+    const bool want = !has;
+    const unsigned need = __ballot_sync(WF_FULL, want);
+    const unsigned busy = __ballot_sync(WF_FULL, has);
+    if (!wdone && need && (__popc(need) >= refill || !busy)) {
+      if (wbase >= wlim) {
+        int nb = 0;
+        if ((threadIdx.x & 31) == 0) nb = atomicAdd(cnt + WF_WHEAD, grab);
+        nb = __shfl_sync(WF_FULL, nb, 0);
+        wbase = nb;
+        wlim = min(nb + grab, total);
+        wdone = nb >= total;
+      }
+      const int q = wbase + __popc(need & lanemask_lt());
+      wbase = min(wbase + __popc(need), wlim);
+      if (want && q < wlim) {  // start this lane's next walk (PT:1466-1470)
+        path = B.qsss[q];
+        const float4* r = rec_of(B.rec, path);
+        const uint4 rq = *reinterpret_cast<const uint4*>(r + R_RNG);
+        g.s[0] = rq.x; g.s[1] = rq.y; g.s[2] = rq.z; g.s[3] = rq.w;
+        const SssEntry e = load_sss(r);
+        ssAlb = e.ssAlb;
+        sss_walk_begin(c, ld3(r[R_POS]), sss_walk_frame(e), g, w);
+        has = true;
+      }
+    }
+    int res = WALK_ON;
+    vec3 pExit(0.0f);
+    if (has) res = sss_walk_step(c, g, ssAlb, w, pExit);
+    const bool ended = has && res != WALK_ON;
+    if (ended) {
+      float4* r = rec_of(B.rec, path);
+      *reinterpret_cast<uint4*>(r + R_RNG) = make_uint4(g.s[0], g.s[1], g.s[2], g.s[3]);
+      r[R_S2] = st3(pExit, __int_as_float(res));
+#ifdef DISPERSION_ENABLED
+      r[R_S1].w = w.thr;
+#else
+      r[R_S4] = st3(w.thr);
+#endif
+    }
+    const int slot = warp_append(cnt + WF_XQ, ended);
+    if (slot >= 0) B.qexit[slot] = path;
+    if (ended) has = false;
+    if (wdone && !__any_sync(WF_FULL, has)) break;
+  }
+}
+
+// The vertices whose walk the persistent walker finished: the exit's normal, direct light and
+// continuation (sss_exit), or the end of the path when the walk stopped inside.
+extern "C" __global__ void __launch_bounds__(SNELLY_BLOCK, SNELLY_SHADE_MIN_BLOCKS) snelly_wf_walk_exit(
+    const JobRec* __restrict__ jobs, const SnellyParams* __restrict__ gparams, WfBuffers B, int it) {
+  using namespace sdev;
+  wf_kernel_entry();
+  const JobRec& J = jobs[0];
+  const SnellyParams& P = c_params[B.slot];
+  int* cnt = B.cnt;
+  const int nxt = (it & 1) ^ 1;
+  const int total = cnt[WF_XQ];
+  Scene sc(uniforms_of(B.slot));
+  sc.INIT();
+  const int stride = gridDim.x * blockDim.x;
+  for (int base = blockIdx.x * blockDim.x; base < total; base += stride) {
+    const int q = base + threadIdx.x;
+    int path = 0;
+    bool push_active = false, finished = false;
+    if (q < total) {
+      path = B.qexit[q];
+      float4* r = rec_of(B.rec, path);
+      WfState st;
+      load_state(r, st);
+      Ctx c{P, gparams, sc, B.slot, 0.0f, vec3(0.0f), make_frame(v3(P.sunDir))};
+      const vec3 xyzw = wavelength_at(c, st.w);
+      const float4 ex = r[R_S2];
+      const float probSSS = r[R_S0].w;
+#ifdef DISPERSION_ENABLED
+      const Rad wthr = r[R_S1].w;
+#else
+      const Rad wthr = ld3(r[R_S4]);
+#endif
+      const int rv = __float_as_int(ex.w) == WALK_EXIT ? sss_exit(c, st.s, probSSS, wthr, ld3(ex), st.g) : VERTEX_DONE;
       ++st.vertex;
       finished = rv == VERTEX_DONE || st.vertex > max_bounces(P) || maxc(st.s.thr) < kThroughputEps;
       if (finished) {

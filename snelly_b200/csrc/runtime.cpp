@@ -337,6 +337,8 @@ int Context::compile_module(const std::string& src, int math_mode, std::shared_p
              {"snelly_wf_shade_metal", &m->f_wf_shade_seg[2], false},
              {"snelly_wf_shade_dielectric", &m->f_wf_shade_seg[3], false},
              {"snelly_wf_sss", &m->f_wf_sss, false},
+             {"snelly_wf_walk", &m->f_wf_walk, false},
+             {"snelly_wf_walk_exit", &m->f_wf_walk_exit, false},
              {"snelly_firsthit", &m->f_firsthit, false},
              {"snelly_ptsimple", &m->f_ptsimple, false}};
   for (auto& f : fns) {
@@ -357,6 +359,13 @@ int Context::compile_module(const std::string& src, int math_mode, std::shared_p
     nb = 0;
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, (const void*)m->f_wf_extend, 64, 0) == cudaSuccess && nb > 0)
       m->extend_blocks_per_sm64 = nb;
+    else
+      cudaGetLastError();
+  }
+  if (m->f_wf_walk) {  // the walker is persistent too: one resident wave
+    int nb = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, (const void*)m->f_wf_walk, SNELLY_BLOCK, 0) == cudaSuccess && nb > 0)
+      m->walk_blocks_per_sm = nb;
     else
       cudaGetLastError();
   }
@@ -697,7 +706,8 @@ int snelly_init(snelly_ctx** out, int device, size_t budget) {
                  {"SNELLY_WF_DRAIN", &d.drain, 0, 4096},  // 0: never park rays
                  {"SNELLY_WF_CHUNK", &d.chunk, 1, 64}, {"SNELLY_WF_GRAB", &d.grab, 1, 1024},
                  {"SNELLY_WF_REFILL", &d.refill, 1, 32}, {"SNELLY_WF_BLOCK", &d.block, 64, 128},
-                 {"SNELLY_WF_PARK_LEFT", &d.park_left, 0, 1024}};
+                 {"SNELLY_WF_PARK_LEFT", &d.park_left, 0, 1024}, {"SNELLY_WF_WALKER", &d.walker, 0, 1},
+                 {"SNELLY_WF_LANE_RAYS", &d.lane_rays, 1, 64}};
     for (unsigned k = 0; k < sizeof knobs / sizeof knobs[0]; ++k)
       if (const char* v = getenv(knobs[k].name)) {
         *knobs[k].field = std::max(knobs[k].lo, std::min(atoi(v), knobs[k].hi));
@@ -1175,8 +1185,8 @@ int snelly_job_wavefront_config(snelly_ctx* ctx, uint64_t job_id, int* out) {
   auto it = c.jobs.find(job_id);
   if (it == c.jobs.end()) return fail(SNELLY_ENOTFOUND, "unknown job id");
   const WfConfig& w = it->second.wfc;
-  const int v[SNELLY_WF_CONFIG_FIELDS] = {it->second.wf_parts, w.shade_split, w.drain, w.chunk,
-                                          w.grab,  w.refill,      w.block, w.park_left};
+  const int v[SNELLY_WF_CONFIG_FIELDS] = {it->second.wf_parts, w.shade_split, w.drain,  w.chunk,    w.grab,
+                                          w.refill,              w.block,       w.park_left, w.walker, w.lane_rays};
   for (int k = 0; k < SNELLY_WF_CONFIG_FIELDS; ++k) out[k] = v[k];
   return SNELLY_OK;
 }

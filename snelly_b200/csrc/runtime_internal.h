@@ -54,6 +54,8 @@ struct Module {
   cudaLibrary_t lib = nullptr;
   cudaKernel_t f_seed = nullptr, f_frame_mega = nullptr, f_resolve = nullptr;
   cudaKernel_t f_wf_generate = nullptr, f_wf_extend = nullptr, f_wf_shade = nullptr, f_wf_sss = nullptr;
+  cudaKernel_t f_wf_walk = nullptr, f_wf_walk_exit = nullptr;  // the persistent subsurface walker
+  int walk_blocks_per_sm = 8;  // resident 128-thread blocks of the walker (occupancy query)
   // the shade stage split by queue segment: misses/finishing, surface, metal, dielectric (null
   // for a material the scene does not have)
   cudaKernel_t f_wf_shade_seg[4] = {nullptr, nullptr, nullptr, nullptr};
@@ -78,6 +80,8 @@ struct WfConfig {
   int refill = 4;       // idle lanes of a warp that trigger a refill
   int block = 128;      // threads per block of the extend and shade launches (64 or 128)
   int park_left = 32;   // stop parking once at most park_left / 1024 of the paths are unfinished
+  int walker = 0;       // subsurface walks by the persistent walker (1) or one thread per walk (0)
+  int lane_rays = 1;    // extend grid: one lane per lane_rays rays the iteration may hold
 };
 
 struct Scene {
@@ -150,7 +154,7 @@ struct Context {
   std::map<std::string, Tuned> tuned;  // autotuner decisions per (module, image-size class)
   // Wavefront defaults; a field set from the environment (SNELLY_WF_SPLIT, SNELLY_WF_DRAIN,
   // SNELLY_WF_SHADE_SPLIT, SNELLY_WF_CHUNK, SNELLY_WF_GRAB, SNELLY_WF_REFILL, SNELLY_WF_BLOCK,
-  // SNELLY_WF_PARK_LEFT) is also kept fixed by the autotuner.
+  // SNELLY_WF_PARK_LEFT, SNELLY_WF_WALKER, SNELLY_WF_LANE_RAYS) is also kept fixed by the autotuner.
   WfConfig wf_default;
   unsigned wf_fixed = 0;             // bit per WfConfig field, in declaration order
   int wf_park_iters = -1;            // iterations that may park rays; -1: 3 x (max_bounces + 2) (SNELLY_WF_PARK_ITERS)

@@ -21,10 +21,10 @@ int Context::alloc_wavefront(Job& j) {
   const int rec_f4 = j.module->wf_rec_f4;
   if (rec_f4 <= 0) return fail(SNELLY_EDEVICE, "module has no wavefront record layout");
   // per path: the record, parked-ray state (3 rays), shadow flags, pending count, int queues
-  // (2 active, 2 x 2 shadow, 2 x 3 parked, 2 x 4 shade, 1 subsurface walk); per part: counters
-  // and the 256-byte alignment of its 15 sub-buffers
-  size_t bytes = ((size_t)rec_f4 * 16 + 3 * 16 + 2 + 4 + (2 + 2 * 2 + 2 * 3 + 2 * 4 + 1) * 4) * P +
-                 (size_t)parts * (4 * WF_COUNTERS + 16 * 256);
+  // (2 active, 2 x 2 shadow, 2 x 3 parked, 2 x 4 shade, subsurface walk, walk exit); per part:
+  // counters and the 256-byte alignment of its 16 sub-buffers
+  size_t bytes = ((size_t)rec_f4 * 16 + 3 * 16 + 2 + 4 + (2 + 2 * 2 + 2 * 3 + 2 * 4 + 2) * 4) * P +
+                 (size_t)parts * (4 * WF_COUNTERS + 18 * 256);
   int rc = alloc(j.wf, bytes);
   if (rc) return rc;
   char* p = (char*)j.wf.ptr;
@@ -51,6 +51,7 @@ int Context::alloc_wavefront(Job& j) {
     B.qshade[0] = (int*)take(16 * Pk);
     B.qshade[1] = (int*)take(16 * Pk);
     B.qsss = (int*)take(4 * Pk);
+    B.qexit = (int*)take(4 * Pk);
     B.cnt = (int*)take(4 * WF_COUNTERS);
     B.shadow = (unsigned char*)take(2 * Pk);
     B.paths = (int)Pk;
@@ -228,7 +229,8 @@ int Context::enqueue_wavefront(const std::vector<Job*>& js, const std::vector<in
       const long long left = R.left;
       const long long extend_blocks = (long long)sm_count * (bs < 128 ? m.extend_blocks_per_sm64 : m.extend_blocks_per_sm);
       const long long shade_blocks = (long long)sm_count * m.shade_blocks_per_sm * (128 / bs);
-      const int eb = (int)std::max<long long>(sm_count, std::min(extend_blocks, (3 * left + bs - 1) / bs));
+      const long long lanes = (3 * left + cf.lane_rays - 1) / cf.lane_rays;
+      const int eb = (int)std::max<long long>(sm_count, std::min(extend_blocks, (lanes + bs - 1) / bs));
       const int sb = (int)std::max<long long>(sm_count, std::min(shade_blocks, (left + bs - 1) / bs));
       const bool split = cf.shade_split && m.f_wf_shade_seg[0];
       const bool walk = m.f_wf_sss && j.params.subsurfaceMFP > 0.0f;  // vertices may choose the walk
@@ -242,7 +244,14 @@ int Context::enqueue_wavefront(const std::vector<Job*>& js, const std::vector<in
       } else if ((r = launch_on(R, m.f_wf_shade, sb, bs, sargs))) {
         return r;
       }
-      if (walk && (r = launch_on(R, m.f_wf_sss, sb, bs, sargs))) return r;  // the subsurface walks it handed over
+      if (walk && cf.walker && m.f_wf_walk && m.f_wf_walk_exit) {  // the walks it handed over: walker, then exits
+        const int wb = sm_count * m.walk_blocks_per_sm;
+        void* wargs[] = {&jobs, &gparams, &B, &it, &grab, &refill};
+        if ((r = launch_on(R, m.f_wf_walk, wb, SNELLY_BLOCK, wargs))) return r;
+        if ((r = launch_on(R, m.f_wf_walk_exit, sb, bs, sargs))) return r;
+      } else if (walk && (r = launch_on(R, m.f_wf_sss, sb, bs, sargs))) {  // one thread per walk
+        return r;
+      }
       ++R.it;
       return SNELLY_OK;
     };
@@ -357,7 +366,9 @@ int Context::time_frames(Job& j, int kernel, float* ms_per_frame) {
 // (scene module, image-size class): the first such job times, on its own buffers, the wavefront
 // with each value of one configuration field in turn (the best so far for the others; one pass
 // over pixel ranges, per-material shading, drain steps, refill chunk, claim size, refill threshold,
-// block shape and the unfinished-path fraction below which parking stops; fields fixed by the
+// block shape, the unfinished-path fraction below which parking stops and, for jobs with subsurface
+// walks, the persistent walker against one thread per walk, and the extend grid's rays per lane;
+// fields fixed by the
 // environment are not varied), then the path-per-thread
 // kernel, keeps the fastest and caches the decision; the job's state is seeded again afterwards
 // by the caller. The size class is the power of two nearest the pixel count (tail effects make
@@ -397,9 +408,12 @@ int Context::autotune(Job& j) {
       std::vector<int> values;
     } fields[] = {{&WfConfig::parts, {1, 2, 3, 4}},  {&WfConfig::shade_split, {0, 1}}, {&WfConfig::drain, {16, 32, 64}},
                   {&WfConfig::chunk, {4, 8, 16}},   {&WfConfig::grab, {16, 32, 64}},  {&WfConfig::refill, {2, 4, 8}},
-                  {&WfConfig::block, {64, 128}},    {&WfConfig::park_left, {0, 8, 32, 128}}};
+                  {&WfConfig::block, {64, 128}},    {&WfConfig::park_left, {0, 8, 32, 128}},
+                  {&WfConfig::walker, {0, 1}},      {&WfConfig::lane_rays, {1, 2, 4}}};
+    const bool walks = j.module->f_wf_walk && j.params.subsurfaceMFP > 0.0f;
     for (unsigned k = 0; k < sizeof fields / sizeof fields[0]; ++k) {
       if (wf_fixed & (1u << k)) continue;
+      if (fields[k].f == &WfConfig::walker && !walks) continue;  // no subsurface walks to time
       for (int v : fields[k].values) {
         WfConfig cfg = best.cfg;
         if (cfg.*(fields[k].f) == v) continue;

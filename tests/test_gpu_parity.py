@@ -239,3 +239,29 @@ def test_wavefront_paths_without_shadow_rays_finish_once(gpu_ctx):
     assert (b[:, 3] == frames).all()
     ok = _close(b[:, :3], a[:, :3], 1e-5)
     assert ok.mean() >= 0.97, ok.mean()
+
+
+@pytest.mark.parametrize("name", ["c2", "c2_cloud"])
+def test_persistent_walker_does_not_change_results(name):
+    """Subsurface walks run by the persistent walker (each lane taking the next walk when its own
+    ends) or one thread per walk give the same image bit for bit: every path draws its random
+    numbers in the same order either way."""
+    import os
+    from snelly_b200 import api
+    imgs = []
+    for walker in ("0", "1"):
+        old = os.environ.pop("SNELLY_WF_WALKER", None)
+        os.environ["SNELLY_WF_WALKER"] = walker
+        try:
+            ctx = api.Context(0)
+        finally:
+            os.environ.pop("SNELLY_WF_WALKER", None)
+            if old is not None:
+                os.environ["SNELLY_WF_WALKER"] = old
+        scene = {"c2": scenes.VolumetricSubsurface, "c2_cloud": scenes.PyroclasticSubsurface}[name](64, 64)
+        s, img = gpu_render(ctx, scene, 3, seed=5, kernel_mode=N.KERNEL_WAVEFRONT)
+        assert ctx.job_wavefront_config(s.job_id())["walker"] == int(walker)
+        imgs.append(img.copy())
+        ctx.destroy_job(s.job_id())
+        ctx.close()
+    np.testing.assert_array_equal(imgs[0], imgs[1])
