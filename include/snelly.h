@@ -208,9 +208,10 @@ int snelly_job_kernel(snelly_ctx* ctx, uint64_t job_id, int* kernel_mode);
  * per-material shade launches (0/1), drain steps before parking, sphere-tracing steps between
  * refills, work items claimed per warp, idle lanes that trigger a refill, threads per block, the
  * fraction of unfinished paths (in 1/1024) below which rays are no longer parked, subsurface
- * walks by the persistent walker (1) or one thread per walk (0), and the rays an iteration may
- * hold per lane of the extend grid. */
-#define SNELLY_WF_CONFIG_FIELDS 10
+ * walks by the persistent walker (1) or one thread per walk (0), the rays an iteration may hold
+ * per lane of the extend grid, and whether the frames of one advance overlap (1: a path that
+ * finishes its pixel's sample starts the pixel's next one; 0: frame after frame). */
+#define SNELLY_WF_CONFIG_FIELDS 11
 int snelly_job_wavefront_config(snelly_ctx* ctx, uint64_t job_id, int* out);
 /* Start a job from saved state instead of seeding (resume). */
 int snelly_restore(snelly_ctx* ctx, uint64_t scene_id, const snelly_render_desc* desc, const uint32_t* rng,

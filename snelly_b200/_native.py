@@ -25,6 +25,19 @@ READ_WAIT, READ_POLL, READ_ASYNC = 1, 2, 4
 U_FLOAT, U_INT, U_BOOL, U_VEC2, U_VEC3, U_VEC4 = 0, 1, 2, 3, 4, 5
 U_IVEC2, U_IVEC3, U_IVEC4, U_MAT2, U_MAT3, U_MAT4, U_SAMPLER2D, U_SAMPLER3D = 6, 7, 8, 9, 10, 11, 12, 13
 IOR_MODELS = {"abbe": 0, "sellmeier": 1, "sellmeier2": 2, "polyanskiy": 3, "cauchy": 4}
+# snelly_job_wavefront_config's fields, in order (SNELLY_WF_CONFIG_FIELDS of them)
+WF_CONFIG_NAMES = ("parts", "shade_split", "drain", "chunk", "grab", "refill", "block", "park_left", "walker",
+                   "lane_rays", "overlap")
+
+
+def header_define(name):
+    """The integer value of a #define in include/snelly.h."""
+    text = open(os.path.join(ROOT, "include", "snelly.h")).read()
+    return int(re.search(r"#define %s (\d+)" % name, text).group(1))
+
+
+if header_define("SNELLY_WF_CONFIG_FIELDS") != len(WF_CONFIG_NAMES):
+    raise ImportError("WF_CONFIG_NAMES does not match SNELLY_WF_CONFIG_FIELDS of include/snelly.h")
 
 
 class SnellyError(RuntimeError):

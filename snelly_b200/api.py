@@ -1171,11 +1171,11 @@ class Context:
 
     def job_wavefront_config(self, jid):
         """A wavefront job's launch configuration as a dict (pixel ranges, per-material shade
-        launches, drain steps, refill chunk, claim size, refill threshold, block size)."""
-        out = (ctypes.c_int * 10)()
+        launches, drain steps, refill chunk, claim size, refill threshold, block size, parking
+        threshold, persistent walker, rays per extend lane, overlapping frames)."""
+        out = (ctypes.c_int * len(N.WF_CONFIG_NAMES))()
         N.check(self._lib.snelly_job_wavefront_config(self._h, jid, out))
-        return dict(zip(("parts", "shade_split", "drain", "chunk", "grab", "refill", "block", "park_left", "walker",
-                         "lane_rays"), out))
+        return dict(zip(N.WF_CONFIG_NAMES, out))
 
     def tonemap(self, jid, width, height, params, fmt=N.TONEMAP_RGBA8):
         """The job's mean image through the display transform: (H, W, 4) uint8 (RGBA8) or float32

@@ -42,14 +42,13 @@ typedef struct JobRec {
 #define WF_A 0      // active-path queue counts [2] (ping-pong by iteration parity)
 #define WF_S 2      // shadow-ray queue counts [2]
 #define WF_C 4      // parked-ray queue counts [2]
-#define WF_LEFT 6   // paths of the frame not finished yet
+#define WF_LEFT 6   // paths with samples of the launch sequence left to finish
 #define WF_Q 8      // shade-queue segment counts [2][4]
 #define WF_SSS 16   // subsurface-walk queue count (filled by the shade stage, read by the walk stage)
 #define WF_WHEAD 17 // the persistent walker's work head over that queue
 #define WF_XQ 18    // walks that ended (exit queue count, read by the walk-exit stage)
-#define WF_HEAD 19  // extend work heads, one per iteration
-#define WF_MAX_ITERS 300
-#define WF_COUNTERS (WF_HEAD + WF_MAX_ITERS)
+#define WF_HEAD 19  // extend work heads [2] (ping-pong by iteration parity)
+#define WF_COUNTERS (WF_HEAD + 2)
 typedef struct WfBuffers {
   float4* rec;      // path records, rec_f4 float4 slots per path
   float4* mt;       // march state of a parked ray (distance, sign, step count), by ray id
@@ -67,4 +66,6 @@ typedef struct WfBuffers {
   int pixel_begin;
   int rec_f4;       // float4 slots per path record (checked against the module's layout)
   int slot;         // the job's constant-memory parameter and uniform slot
+  int samples;      // samples per pixel one generate launch starts: a path that finishes its
+                    // pixel's sample starts the pixel's next one in place until this many are done
 } WfBuffers;

@@ -13,8 +13,12 @@
 //             shadow results, then run the vertex (vertex_step) with the sky/sun shadow rays
 //             deferred; continuing paths and new shadow rays go to the next iteration's queues,
 //             finished paths add their XYZ to the pixel's Kahan sums.
-// The host launches generate once and (extend, shade) until every path of the frame has finished
-// (a count the shade stage decrements); the queue counters ping-pong by iteration parity.
+// The host launches generate once and (extend, shade) until every path has finished (a count the
+// shade stage decrements); the queue counters ping-pong by iteration parity. One generate launch
+// may start several samples per pixel (B.samples): a path that finishes one sample of its pixel
+// starts the next in place, with the RNG state the finished one left, so the frames of a launch
+// sequence overlap (no stage waits for the last paths of a frame) and every pixel still draws
+// its random numbers and adds its samples in the same order as frame by frame.
 #pragma once
 #include "pt_integrator.cuh"
 #include "pt_launch.h"
@@ -24,6 +28,8 @@
 namespace sdev {
 
 enum { WF_INDIELE = 1, WF_FINISHING = 2, WF_NEE = 4, WF_NEE_SKY = 8, WF_NEE_SUN = 16 };
+// flags bits from here up: the index of the path's sample among those of its launch sequence
+#define WF_SAMPLE_SHIFT 8
 
 // ---- the path record ----------------------------------------------------------------------------
 // One path's state: WF_REC float4 slots, contiguous. Slots a stage reads together sit in the same
@@ -249,8 +255,10 @@ SD_FN void wf_kernel_entry() {
   asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
 }
 
-// Final contribution of a path: XYZ added to the pixel's Kahan sums, RNG written back.
-SD_FN void finish_path(const JobRec& J, const WfBuffers& B, int path, const Rad& L, const vec3& xyzw, const Rng& g) {
+// Final contribution of a path: XYZ added to the pixel's Kahan sums, and the RNG state written back
+// when it is the pixel's last sample of the launch sequence (save_rng).
+SD_FN void finish_path(const JobRec& J, const WfBuffers& B, int path, const Rad& L, const vec3& xyzw, const Rng& g,
+                       bool save_rng) {
   long long i = (long long)B.pixel_begin + path;
 #ifdef DISPERSION_ENABLED
   vec3 c = xyzw * (L / float(MAX_SAMPLES_PER_FRAME));
@@ -272,7 +280,37 @@ SD_FN void finish_path(const JobRec& J, const WfBuffers& B, int path, const Rad&
     J.acc64[4 * i + 2] += double(c.z);
     J.acc64[4 * i + 3] += 1.0;
   }
-  J.rng[i] = make_uint4(g.s[0], g.s[1], g.s[2], g.s[3]);
+  if (save_rng) J.rng[i] = make_uint4(g.s[0], g.s[1], g.s[2], g.s[3]);
+}
+
+// A camera sample of pixel i (PT:1934-1955): the wavelength, the filter jitter and the primary
+// ray, drawn from st.g in that order; the path starts over at vertex 0 as sample `sample`.
+SD_FN void start_sample(Ctx& c, const JobRec& J, long long i, WfState& st, int sample) {
+  const SnellyParams& P = c.P;
+  const int W = J.width;
+  const int x = int(i % W), y = int(i / W);
+  pick_wavelength(c, st.g, &st.w);
+  float jx = 0.5f * P.filterRadius * tent(rand01(st.g));
+  float jy = 0.5f * P.filterRadius * tent(rand01(st.g));
+  vec3 start, dir;
+  primary_ray_hook(c, vec2(float(x) + 0.5f, float(y) + 0.5f) + vec2(jx, jy), st.g, start, dir);
+  start_path(c, st.s, start, dir);
+  st.vertex = 0;
+  st.flags = (st.s.inDiele ? WF_INDIELE : 0) | (sample << WF_SAMPLE_SHIFT);
+}
+
+// A path whose sample just finished: the pixel's sample is added, and unless it was the pixel's
+// last of the launch sequence the next one starts in the same record, waiting for its camera ray
+// (returns true: the caller queues the path as active).
+SD_FN bool finish_sample(Ctx& c, const JobRec& J, const WfBuffers& B, int path, WfState& st, const vec3& xyzw) {
+  const int sample = (st.flags >> WF_SAMPLE_SHIFT) + 1;
+  const bool more = sample < B.samples;
+  finish_path(J, B, path, st.s.L, xyzw, st.g, !more);
+  if (!more) return false;
+  start_sample(c, J, (long long)B.pixel_begin + path, st, sample);
+  store_state(rec_of(B.rec, path), st);
+  B.pend[path] = 1;
+  return true;
 }
 
 }  // namespace sdev
@@ -305,18 +343,8 @@ extern "C" __global__ void __launch_bounds__(SNELLY_BLOCK) snelly_wf_generate(co
   st.g.s[0] = r4.x; st.g.s[1] = r4.y; st.g.s[2] = r4.z; st.g.s[3] = r4.w;
   Scene sc(uniforms_of(B.slot));
   sc.INIT();
-  Ctx c{P, gparams, sc, B.slot, 0.0f, vec3(0.0f), Frame()};
-  const int W = J.width;
-  const int x = int(i % W), y = int(i / W);
-  pick_wavelength(c, st.g, &st.w);
-  c.sun = make_frame(v3(P.sunDir));
-  float jx = 0.5f * P.filterRadius * tent(rand01(st.g));
-  float jy = 0.5f * P.filterRadius * tent(rand01(st.g));
-  vec3 start, dir;
-  primary_ray_hook(c, vec2(float(x) + 0.5f, float(y) + 0.5f) + vec2(jx, jy), st.g, start, dir);
-  start_path(c, st.s, start, dir);
-  st.vertex = 0;
-  st.flags = st.s.inDiele ? WF_INDIELE : 0;
+  Ctx c{P, gparams, sc, B.slot, 0.0f, vec3(0.0f), make_frame(v3(P.sunDir))};
+  start_sample(c, J, i, st, 0);
   store_state(rec_of(B.rec, path), st);
   B.pend[path] = 1;  // the camera ray
   B.qa[0][path] = path;
@@ -354,6 +382,7 @@ extern "C" __global__ void __launch_bounds__(SNELLY_BLOCK) snelly_wf_extend(WfBu
     cnt[WF_SSS] = 0;
     cnt[WF_WHEAD] = 0;
     cnt[WF_XQ] = 0;
+    cnt[WF_HEAD + nxt] = 0;
     for (int k = 0; k < 4; ++k) cnt[WF_Q + 4 * nxt + k] = 0;
   }
   const int nA = cnt[WF_A + cur], nS = cnt[WF_S + cur], nC = cnt[WF_C + cur];
@@ -385,7 +414,7 @@ extern "C" __global__ void __launch_bounds__(SNELLY_BLOCK) snelly_wf_extend(WfBu
     if (!wdone && need && (__popc(need) >= refill || !busy)) {
       if (wbase >= wlim) {
         int nb = 0;
-        if ((threadIdx.x & 31) == 0) nb = atomicAdd(cnt + WF_HEAD + it, grab);
+        if ((threadIdx.x & 31) == 0) nb = atomicAdd(cnt + WF_HEAD + cur, grab);
         nb = __shfl_sync(WF_FULL, nb, 0);
         wbase = nb;
         wlim = min(nb + grab, total);
@@ -592,7 +621,11 @@ SD_FN void shade_path(const JobRec& J, const SnellyParams* gparams, const WfBuff
   }
   st.s.inDiele ? (flags |= WF_INDIELE) : (flags &= ~WF_INDIELE);
   if (finished) {
-    finish_path(J, B, path, st.s.L, xyzw, st.g);
+    st.flags = flags;
+    if (finish_sample(c, J, B, path, st, xyzw)) {  // the pixel's next sample: its camera ray
+      finished = false;
+      push_active = true;
+    }
     return;
   }
   st.flags = flags;
@@ -729,7 +762,10 @@ extern "C" __global__ void __launch_bounds__(SNELLY_BLOCK, SNELLY_SHADE_MIN_BLOC
       ++st.vertex;
       finished = rv == VERTEX_DONE || st.vertex > max_bounces(P) || maxc(st.s.thr) < kThroughputEps;
       if (finished) {
-        finish_path(J, B, path, st.s.L, xyzw, st.g);
+        if (finish_sample(c, J, B, path, st, xyzw)) {
+          finished = false;
+          push_active = true;
+        }
       } else {
         st.s.inDiele ? (st.flags |= WF_INDIELE) : (st.flags &= ~WF_INDIELE);
         store_state(r, st);
@@ -861,7 +897,10 @@ extern "C" __global__ void __launch_bounds__(SNELLY_BLOCK, SNELLY_SHADE_MIN_BLOC
       ++st.vertex;
       finished = rv == VERTEX_DONE || st.vertex > max_bounces(P) || maxc(st.s.thr) < kThroughputEps;
       if (finished) {
-        finish_path(J, B, path, st.s.L, xyzw, st.g);
+        if (finish_sample(c, J, B, path, st, xyzw)) {
+          finished = false;
+          push_active = true;
+        }
       } else {
         st.s.inDiele ? (st.flags |= WF_INDIELE) : (st.flags &= ~WF_INDIELE);
         store_state(r, st);

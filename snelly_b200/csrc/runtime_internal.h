@@ -82,6 +82,8 @@ struct WfConfig {
   int park_left = 32;   // stop parking once at most park_left / 1024 of the paths are unfinished
   int walker = 0;       // subsurface walks by the persistent walker (1) or one thread per walk (0)
   int lane_rays = 1;    // extend grid: one lane per lane_rays rays the iteration may hold
+  int overlap = 1;      // the frames of one advance overlap (a path that finishes its pixel's sample
+                        // starts the pixel's next) rather than run one after another
 };
 
 struct Scene {

@@ -84,16 +84,19 @@ int Context::enqueue_wavefront_frames(Job& j, int frames) {
 // parameters its caller has already uploaded into slot 0 on the context stream, enqueue_frames),
 // the job runs its first part on the context stream in slot 0 and nothing is uploaded.
 //
-// Per frame and part: generate, then iterations of (extend, shade [, subsurface walk]). The first
-// `budgeted` iterations park the slowest rays when their work runs out; after them every
-// iteration advances every path by one vertex, so `nominal` more always finish the frame. Beyond
-// the nominal count, a part's iterations go in pairs, each followed by a read of its paths-left
-// count; a part gets its next pair once the read of the pair before last has landed, so its
-// stream always has a pair queued, and it moves on to its next frame once a read shows zero (an
-// extra pair then finds empty queues and returns at once). The parts are independent pixel
-// ranges, so a part that finishes a frame early starts its next one while the others still trace
-// the stragglers of theirs; the host serves whichever part's read has landed and never waits on
-// one part while another could be fed.
+// Per launch sequence and part: generate, then iterations of (extend, shade [, subsurface walk]).
+// With overlapping frames (wfc.overlap) one sequence runs all of the advance's frames: generate
+// starts every pixel's first sample and each finished sample starts the pixel's next in place
+// (B.samples), so no iteration waits for the last paths of a frame; otherwise each frame is a
+// sequence of its own. The first `budgeted` iterations park the slowest rays when their work runs
+// out; after them every iteration advances every path by one vertex, so `nominal` more per sample
+// always finish the sequence. Beyond the first `nominal`, a part's iterations go in pairs, each
+// followed by a read of its paths-left count; a part gets its next pair once the read of the pair
+// before last has landed, so its stream always has a pair queued, and it moves on to its next
+// sequence once a read shows zero (an extra pair then finds empty queues and returns at once).
+// The parts are independent pixel ranges, so a part that finishes early starts its next sequence
+// while the others still trace the stragglers of theirs; the host serves whichever part's read
+// has landed and never waits on one part while another could be fed.
 int Context::enqueue_wavefront(const std::vector<Job*>& js, const std::vector<int>& frames,
                                const std::map<Module*, cudaEvent_t>& after, bool slot0_ready) {
   for (size_t q = 0; q < js.size(); ++q) {
@@ -121,7 +124,8 @@ int Context::enqueue_wavefront(const std::vector<Job*>& js, const std::vector<in
     // the parts of this wave, each with a stream and two progress-read events
     struct PartRun {
       Job* j;
-      int k, total = 0, frame = 0, it = 0, checks = 0;
+      int k, total = 0, frame = 0, it = 0, checks = 0;  // total, frame: launch sequences
+      int samples = 1;  // samples per pixel of each sequence
       long long left = 0;  // paths of the frame not finished at the latest read (an upper bound afterwards)
       bool started = false;
       cudaStream_t st = nullptr;
@@ -134,7 +138,8 @@ int Context::enqueue_wavefront(const std::vector<Job*>& js, const std::vector<in
         PartRun R;
         R.j = js[q];
         R.k = k;
-        R.total = frames[q];
+        R.total = js[q]->wfc.overlap ? 1 : frames[q];
+        R.samples = js[q]->wfc.overlap ? frames[q] : 1;
         R.idx = (int)runs.size();
         runs.push_back(R);
       }
@@ -211,10 +216,11 @@ int Context::enqueue_wavefront(const std::vector<Job*>& js, const std::vector<in
       Job& j = *R.j;
       Module& m = *j.module;
       WfBuffers B = j.wfb[R.k];
+      B.samples = R.samples;
       void* jobs = j.tables.ptr;
       void* gparams = j.gparams.ptr;
       const int nominal = j.scene->opts.max_bounces + 2;
-      const int budgeted = wf_park_iters >= 0 ? std::min(wf_park_iters, 8 * nominal) : 3 * nominal;
+      const int budgeted = R.samples * (wf_park_iters >= 0 ? std::min(wf_park_iters, 8 * nominal) : 3 * nominal);
       int it = R.it;
       const WfConfig& cf = j.wfc;
       // rays are parked in the first `budgeted` iterations while more than park_left / 1024 of
@@ -263,11 +269,11 @@ int Context::enqueue_wavefront(const std::vector<Job*>& js, const std::vector<in
         if (R.frame >= R.total) continue;
         Job& j = *R.j;
         const int nominal = j.scene->opts.max_bounces + 2;
-        const int budgeted = wf_park_iters >= 0 ? std::min(wf_park_iters, 8 * nominal) : 3 * nominal;
-        const int max_iters = budgeted + nominal;
-        if (max_iters + 2 > WF_MAX_ITERS) return fail(SNELLY_EINVAL, "too many wavefront iterations for max_bounces");
-        if (!R.started) {  // the part's next frame: camera rays, then the unpolled iterations
+        const int budgeted = R.samples * (wf_park_iters >= 0 ? std::min(wf_park_iters, 8 * nominal) : 3 * nominal);
+        const int max_iters = budgeted + R.samples * nominal;
+        if (!R.started) {  // the part's next sequence: camera rays, then the unpolled iterations
           WfBuffers B = j.wfb[R.k];
+          B.samples = R.samples;
           void* jobs = j.tables.ptr;
           void* gparams = j.gparams.ptr;
           void* gargs[] = {&jobs, &gparams, &B};
@@ -367,7 +373,8 @@ int Context::time_frames(Job& j, int kernel, float* ms_per_frame) {
 // with each value of one configuration field in turn (the best so far for the others; one pass
 // over pixel ranges, per-material shading, drain steps, refill chunk, claim size, refill threshold,
 // block shape, the unfinished-path fraction below which parking stops and, for jobs with subsurface
-// walks, the persistent walker against one thread per walk, and the extend grid's rays per lane;
+// walks, the persistent walker against one thread per walk, the extend grid's rays per lane, and
+// overlapping frames against frame after frame;
 // fields fixed by the
 // environment are not varied), then the path-per-thread
 // kernel, keeps the fastest and caches the decision; the job's state is seeded again afterwards
@@ -409,7 +416,8 @@ int Context::autotune(Job& j) {
     } fields[] = {{&WfConfig::parts, {1, 2, 3, 4}},  {&WfConfig::shade_split, {0, 1}}, {&WfConfig::drain, {16, 32, 64}},
                   {&WfConfig::chunk, {4, 8, 16}},   {&WfConfig::grab, {16, 32, 64}},  {&WfConfig::refill, {2, 4, 8}},
                   {&WfConfig::block, {64, 128}},    {&WfConfig::park_left, {0, 8, 32, 128}},
-                  {&WfConfig::walker, {0, 1}},      {&WfConfig::lane_rays, {1, 2, 4}}};
+                  {&WfConfig::walker, {0, 1}},      {&WfConfig::lane_rays, {1, 2, 4}},
+                  {&WfConfig::overlap, {0, 1}}};
     const bool walks = j.module->f_wf_walk && j.params.subsurfaceMFP > 0.0f;
     for (unsigned k = 0; k < sizeof fields / sizeof fields[0]; ++k) {
       if (wf_fixed & (1u << k)) continue;
