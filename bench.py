@@ -177,9 +177,9 @@ def cpu_baseline(host, budget_s, frames=64):
     """The workload at its full spp (`frames` frames per pixel) on a random pixel sample sized to
     about `budget_s` seconds, every host core."""
     run, kind, team, keep = cpu_sampler(host)
-    t = run(2000)  # calibration, 1 frame each
+    t = run(2000, frames)  # calibration at the full spp (a 1-frame sample runs faster per sample)
     rate = 2000 / max(t, 1e-6)
-    n = int(min(host.width * host.height, max(64, rate * budget_s / frames)))
+    n = int(min(host.width * host.height, max(64, rate * budget_s)))
     dt = run(n, frames)
     cores = team()
     return {"value": n * frames / dt, "unit": "path samples/s", "cores": cores, "kind": kind,
@@ -218,9 +218,9 @@ def reference_arm(args, rank):
     host = HostSnelly(workload_scene(args))
     run, kind, team, keep = cpu_sampler(host)
     frames = max(1, args.spp_per_step)
-    t = run(1000)
-    rate = 1000 / max(t, 1e-6)  # path samples/s
-    per_step = int(min(host.width * host.height, max(16, rate * args.cpu_seconds / max(1, args.steps) / frames)))
+    t = run(1000, frames)  # calibration at the step's spp
+    rate = 1000 / max(t, 1e-6)  # pixels/s
+    per_step = int(min(host.width * host.height, max(16, rate * args.cpu_seconds / max(1, args.steps))))
     for _ in range(args.warmup):
         run(min(per_step, 64), frames)
     times = [run(per_step, frames) for _ in range(args.steps)]
