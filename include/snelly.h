@@ -200,8 +200,9 @@ int snelly_pick(snelly_ctx* ctx, uint64_t scene_id, const snelly_render_desc* de
 int snelly_readback_state(snelly_ctx* ctx, uint64_t job_id, uint32_t* rng, float* acc, float* comp, double* acc64);
 /* The integrator a job's frames run: SNELLY_KERNEL_MEGA or SNELLY_KERNEL_WAVEFRONT (a scene
  * created with SNELLY_KERNEL_AUTO gets the autotuner's choice for its module and image size, once
- * per size class: the wavefront's launch configuration by one pass of coordinate descent, each
- * candidate timed over a warm-up frame and about 12 ms of frames, then the path-per-thread
+ * per size class: the wavefront's launch configuration by coordinate descent (one pass over every
+ * field, a second over the pixel ranges and the extend grid's rays per lane), each
+ * candidate timed over a warm-up frame and about 40 ms of frames, then the path-per-thread
  * kernel). No counterpart in the reference, which has one fragment program. */
 int snelly_job_kernel(snelly_ctx* ctx, uint64_t job_id, int* kernel_mode);
 /* A wavefront job's launch configuration, SNELLY_WF_CONFIG_FIELDS ints: concurrent pixel ranges,
@@ -209,9 +210,10 @@ int snelly_job_kernel(snelly_ctx* ctx, uint64_t job_id, int* kernel_mode);
  * refills, work items claimed per warp, idle lanes that trigger a refill, threads per block, the
  * fraction of unfinished paths (in 1/1024) below which rays are no longer parked, subsurface
  * walks by the persistent walker (1) or one thread per walk (0), the rays an iteration may hold
- * per lane of the extend grid, and whether the frames of one advance overlap (1: a path that
- * finishes its pixel's sample starts the pixel's next one; 0: frame after frame). */
-#define SNELLY_WF_CONFIG_FIELDS 11
+ * per lane of the extend grid, whether the frames of one advance overlap (1: a path that
+ * finishes its pixel's sample starts the pixel's next one; 0: frame after frame), and the eighths
+ * of the shade stage's resident blocks its grid may fill. */
+#define SNELLY_WF_CONFIG_FIELDS 12
 int snelly_job_wavefront_config(snelly_ctx* ctx, uint64_t job_id, int* out);
 /* Start a job from saved state instead of seeding (resume). */
 int snelly_restore(snelly_ctx* ctx, uint64_t scene_id, const snelly_render_desc* desc, const uint32_t* rng,

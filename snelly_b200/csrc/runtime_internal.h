@@ -81,9 +81,12 @@ struct WfConfig {
   int block = 128;      // threads per block of the extend and shade launches (64 or 128)
   int park_left = 32;   // stop parking once at most park_left / 1024 of the paths are unfinished
   int walker = 0;       // subsurface walks by the persistent walker (1) or one thread per walk (0)
-  int lane_rays = 1;    // extend grid: one lane per lane_rays rays the iteration may hold
+  int lane_rays = 8;    // extend grid: one lane per lane_rays rays the iteration may hold (a
+                        // smaller grid lets the ranges' extend launches share the GPU)
   int overlap = 1;      // the frames of one advance overlap (a path that finishes its pixel's sample
                         // starts the pixel's next) rather than run one after another
+  int shade_share = 8;  // shade grid: at most shade_share / 8 of the stage's resident blocks, so that
+                        // other ranges' extend blocks fit beside a range's shade stage
 };
 
 struct Scene {

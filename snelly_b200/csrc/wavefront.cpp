@@ -234,7 +234,8 @@ int Context::enqueue_wavefront(const std::vector<Job*>& js, const std::vector<in
       // find nothing to do: at most 3 rays (continuation, sky and sun shadows) per unfinished path.
       const long long left = R.left;
       const long long extend_blocks = (long long)sm_count * (bs < 128 ? m.extend_blocks_per_sm64 : m.extend_blocks_per_sm);
-      const long long shade_blocks = (long long)sm_count * m.shade_blocks_per_sm * (128 / bs);
+      const long long shade_blocks =
+          std::max<long long>(1, (long long)sm_count * m.shade_blocks_per_sm * cf.shade_share / 8) * (128 / bs);
       const long long lanes = (3 * left + cf.lane_rays - 1) / cf.lane_rays;
       const int eb = (int)std::max<long long>(sm_count, std::min(extend_blocks, (lanes + bs - 1) / bs));
       const int sb = (int)std::max<long long>(sm_count, std::min(shade_blocks, (left + bs - 1) / bs));
@@ -325,8 +326,9 @@ int Context::enqueue_wavefront(const std::vector<Job*>& js, const std::vector<in
 }
 
 // Frames of one job with the given integrator on its own buffers, timed with events on the
-// context stream: one warm-up frame, then enough frames for about 12 ms (2 to 16); the per-frame
-// time. The job's state is seeded again afterwards by the caller.
+// context stream: one warm-up frame, then enough frames for about 40 ms (4 to 16) in one call, so
+// that overlapping frames are timed over a sequence of several; the per-frame time. The job's
+// state is seeded again afterwards by the caller.
 int Context::time_frames(Job& j, int kernel, float* ms_per_frame) {
   void* tables = j.tables.ptr;
   void* bstart = (char*)j.tables.ptr + 128;
@@ -355,7 +357,7 @@ int Context::time_frames(Job& j, int kernel, float* ms_per_frame) {
     else cudaEventElapsedTime(&warm, e[0], e[1]);
   }
   if (!rc) {
-    n = std::max(2, std::min(16, (int)std::ceil(12.0f / std::max(warm, 1e-3f))));
+    n = std::max(4, std::min(16, (int)std::ceil(40.0f / std::max(warm, 1e-3f))));
     rc = frames(n);
   }
   if (!rc) {
@@ -374,9 +376,9 @@ int Context::time_frames(Job& j, int kernel, float* ms_per_frame) {
 // over pixel ranges, per-material shading, drain steps, refill chunk, claim size, refill threshold,
 // block shape, the unfinished-path fraction below which parking stops and, for jobs with subsurface
 // walks, the persistent walker against one thread per walk, the extend grid's rays per lane, and
-// overlapping frames against frame after frame;
-// fields fixed by the
-// environment are not varied), then the path-per-thread
+// overlapping frames against frame after frame, and the share of the GPU a shade launch may fill;
+// then a second pass over the pixel ranges and the rays per lane; fields fixed by the environment
+// are not varied), then the path-per-thread
 // kernel, keeps the fastest and caches the decision; the job's state is seeded again afterwards
 // by the caller. The size class is the power of two nearest the pixel count (tail effects make
 // the choice size-dependent).
@@ -413,28 +415,38 @@ int Context::autotune(Job& j) {
     struct Field {
       int WfConfig::*f;
       std::vector<int> values;
-    } fields[] = {{&WfConfig::parts, {1, 2, 3, 4}},  {&WfConfig::shade_split, {0, 1}}, {&WfConfig::drain, {16, 32, 64}},
-                  {&WfConfig::chunk, {4, 8, 16}},   {&WfConfig::grab, {16, 32, 64}},  {&WfConfig::refill, {2, 4, 8}},
-                  {&WfConfig::block, {64, 128}},    {&WfConfig::park_left, {0, 8, 32, 128}},
-                  {&WfConfig::walker, {0, 1}},      {&WfConfig::lane_rays, {1, 2, 4}},
-                  {&WfConfig::overlap, {0, 1}}};
+    } fields[] = {{&WfConfig::parts, {1, 2, 3, 4, 6, 8}}, {&WfConfig::shade_split, {0, 1}},
+                  {&WfConfig::drain, {16, 32, 64}},       {&WfConfig::chunk, {4, 8, 16}},
+                  {&WfConfig::grab, {16, 32, 64}},        {&WfConfig::refill, {2, 4, 8}},
+                  {&WfConfig::block, {64, 128}},          {&WfConfig::park_left, {0, 8, 32, 128}},
+                  {&WfConfig::walker, {0, 1}},            {&WfConfig::lane_rays, {1, 2, 4, 8, 16}},
+                  {&WfConfig::overlap, {0, 1}},           {&WfConfig::shade_share, {3, 5, 8}}};
+    const unsigned nfields = sizeof fields / sizeof fields[0];
     const bool walks = j.module->f_wf_walk && j.params.subsurfaceMFP > 0.0f;
-    for (unsigned k = 0; k < sizeof fields / sizeof fields[0]; ++k) {
-      if (wf_fixed & (1u << k)) continue;
-      if (fields[k].f == &WfConfig::walker && !walks) continue;  // no subsurface walks to time
+    auto descend = [&](unsigned k) -> int {  // try every value of field k against the best so far
+      if (wf_fixed & (1u << k)) return SNELLY_OK;
+      if (fields[k].f == &WfConfig::walker && !walks) return SNELLY_OK;  // no subsurface walks to time
       for (int v : fields[k].values) {
         WfConfig cfg = best.cfg;
         if (cfg.*(fields[k].f) == v) continue;
         cfg.*(fields[k].f) = v;
-        if (k == 0 && v > 1 && npix < (long long)v * 65536) continue;  // too small for that many ranges
+        if (fields[k].f == &WfConfig::parts && v > 1 && npix < (long long)v * 65536)
+          continue;  // too small for that many ranges
         float ms = 0.0f;
-        if ((rc = try_cfg(cfg, &ms))) return rc;
+        if (int r = try_cfg(cfg, &ms)) return r;
         if (ms < best_ms) {
           best_ms = ms;
           best.cfg = cfg;
         }
       }
-    }
+      return SNELLY_OK;
+    };
+    for (unsigned k = 0; k < nfields; ++k)
+      if ((rc = descend(k))) return rc;
+    // the pixel ranges and the extend grid's rays per lane decide together how the ranges'
+    // launches share the GPU: a second pass over both
+    for (unsigned k = 0; k < nfields; ++k)
+      if ((fields[k].f == &WfConfig::parts || fields[k].f == &WfConfig::lane_rays) && (rc = descend(k))) return rc;
     float mega_ms = 0.0f;
     if ((rc = time_frames(j, SNELLY_KERNEL_MEGA, &mega_ms))) return rc;
     best.kernel = mega_ms < best_ms ? SNELLY_KERNEL_MEGA : SNELLY_KERNEL_WAVEFRONT;
