@@ -63,7 +63,9 @@ typedef struct WfBuffers {
   int* qexit;       // paths whose walk the persistent walker finished (one iteration's)
   int* cnt;         // counters (WF_*)
   int paths;
-  int pixel_begin;
+  int pixel_begin;  // contiguous range (pixel_group 0): its first pixel; interleaved: the range's index
+  int pixel_group;  // > 0: the image's groups of pixel_group pixels are dealt to the ranges in turn
+  int pixel_parts;  // ranges the groups are dealt to
   int rec_f4;       // float4 slots per path record (checked against the module's layout)
   int slot;         // the job's constant-memory parameter and uniform slot
   int samples;      // samples per pixel one generate launch starts: a path that finishes its

@@ -255,11 +255,20 @@ SD_FN void wf_kernel_entry() {
   asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
 }
 
+// The pixel a path of this range traces: the range's contiguous pixels from pixel_begin, or,
+// with interleaved ranges, the path's group among those dealt to range pixel_begin in turn
+// (group b of the image goes to range b mod pixel_parts).
+SD_FN long long pixel_of(const WfBuffers& B, int path) {
+  if (B.pixel_group <= 0) return (long long)B.pixel_begin + path;
+  const int g = path / B.pixel_group;
+  return ((long long)g * B.pixel_parts + B.pixel_begin) * B.pixel_group + (path - g * B.pixel_group);
+}
+
 // Final contribution of a path: XYZ added to the pixel's Kahan sums, and the RNG state written back
 // when it is the pixel's last sample of the launch sequence (save_rng).
 SD_FN void finish_path(const JobRec& J, const WfBuffers& B, int path, const Rad& L, const vec3& xyzw, const Rng& g,
                        bool save_rng) {
-  long long i = (long long)B.pixel_begin + path;
+  long long i = pixel_of(B, path);
 #ifdef DISPERSION_ENABLED
   vec3 c = xyzw * (L / float(MAX_SAMPLES_PER_FRAME));
 #else
@@ -307,7 +316,7 @@ SD_FN bool finish_sample(Ctx& c, const JobRec& J, const WfBuffers& B, int path, 
   const bool more = sample < B.samples;
   finish_path(J, B, path, st.s.L, xyzw, st.g, !more);
   if (!more) return false;
-  start_sample(c, J, (long long)B.pixel_begin + path, st, sample);
+  start_sample(c, J, pixel_of(B, path), st, sample);
   store_state(rec_of(B.rec, path), st);
   B.pend[path] = 1;
   return true;
@@ -336,7 +345,7 @@ extern "C" __global__ void __launch_bounds__(SNELLY_BLOCK) snelly_wf_generate(co
     B.cnt[WF_LEFT] = B.paths;
   }
   if (path >= B.paths) return;
-  long long i = (long long)B.pixel_begin + path;
+  long long i = pixel_of(B, path);
   const SnellyParams& P = c_params[B.slot];
   uint4 r4 = J.rng[i];
   WfState st;

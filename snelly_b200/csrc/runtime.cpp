@@ -708,7 +708,7 @@ int snelly_init(snelly_ctx** out, int device, size_t budget) {
                  {"SNELLY_WF_REFILL", &d.refill, 1, 32}, {"SNELLY_WF_BLOCK", &d.block, 64, 128},
                  {"SNELLY_WF_PARK_LEFT", &d.park_left, 0, 1024}, {"SNELLY_WF_WALKER", &d.walker, 0, 1},
                  {"SNELLY_WF_LANE_RAYS", &d.lane_rays, 1, 64}, {"SNELLY_WF_OVERLAP", &d.overlap, 0, 1},
-                 {"SNELLY_WF_SHADE_SHARE", &d.shade_share, 1, 8}};
+                 {"SNELLY_WF_SHADE_SHARE", &d.shade_share, 1, 8}, {"SNELLY_WF_INTERLEAVE", &d.interleave, 0, 1}};
     for (unsigned k = 0; k < sizeof knobs / sizeof knobs[0]; ++k)
       if (const char* v = getenv(knobs[k].name)) {
         *knobs[k].field = std::max(knobs[k].lo, std::min(atoi(v), knobs[k].hi));
@@ -1188,7 +1188,7 @@ int snelly_job_wavefront_config(snelly_ctx* ctx, uint64_t job_id, int* out) {
   const WfConfig& w = it->second.wfc;
   const int v[SNELLY_WF_CONFIG_FIELDS] = {it->second.wf_parts, w.shade_split, w.drain,  w.chunk,    w.grab,
                                           w.refill,              w.block,       w.park_left, w.walker, w.lane_rays,
-                                          w.overlap,             w.shade_share};
+                                          w.overlap,             w.shade_share, w.interleave};
   for (int k = 0; k < SNELLY_WF_CONFIG_FIELDS; ++k) out[k] = v[k];
   return SNELLY_OK;
 }

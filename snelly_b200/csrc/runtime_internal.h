@@ -87,6 +87,8 @@ struct WfConfig {
                         // starts the pixel's next) rather than run one after another
   int shade_share = 8;  // shade grid: at most shade_share / 8 of the stage's resident blocks, so that
                         // other ranges' extend blocks fit beside a range's shade stage
+  int interleave = 1;   // pixel ranges as the image's rows dealt to the ranges in turn (1), so that every
+                        // range holds a like share of the scene, or as contiguous runs of rows (0)
 };
 
 struct Scene {

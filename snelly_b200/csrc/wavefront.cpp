@@ -33,9 +33,19 @@ int Context::alloc_wavefront(Job& j) {
     p += (n + 255) / 256 * 256;
     return q;
   };
+  // interleaved ranges: the image's rows go to the ranges in turn (range k: rows k, k + parts, ...;
+  // only the last row can be short), so that every range holds a like share of the scene and the
+  // ranges finish their launch sequences together instead of the emptiest ones first
+  const size_t G = (j.wfc.interleave && parts > 1) ? (size_t)j.desc.width : 0;
+  const size_t ng = G ? (P + G - 1) / G : 0;
+  const bool dealt = G > 0 && ng >= (size_t)parts;
   size_t begin = 0;
   for (int k = 0; k < parts; ++k) {
-    const size_t Pk = P / parts + ((size_t)k < P % parts ? 1 : 0);
+    size_t Pk = P / parts + ((size_t)k < P % parts ? 1 : 0);
+    if (dealt) {
+      const size_t groups = (ng - k + parts - 1) / parts;
+      Pk = groups * G - ((ng - 1) % parts == (size_t)k ? ng * G - P : 0);
+    }
     const size_t f4 = 16 * Pk;
     WfBuffers& B = j.wfb[k];
     B.rec = (float4*)take((size_t)rec_f4 * f4);
@@ -55,9 +65,12 @@ int Context::alloc_wavefront(Job& j) {
     B.cnt = (int*)take(4 * WF_COUNTERS);
     B.shadow = (unsigned char*)take(2 * Pk);
     B.paths = (int)Pk;
-    B.pixel_begin = (int)begin;
+    B.pixel_begin = dealt ? k : (int)begin;
+    B.pixel_group = dealt ? (int)G : 0;
+    B.pixel_parts = parts;
     begin += Pk;
   }
+  if (begin != P) return fail(SNELLY_EDEVICE, "wavefront pixel ranges do not cover the image");
   j.wf_parts = parts;
   j.wfc.parts = parts;
   if ((size_t)(p - (char*)j.wf.ptr) > bytes) return fail(SNELLY_EDEVICE, "wavefront buffer layout overflow");
@@ -401,7 +414,7 @@ int Context::autotune(Job& j) {
     void* sargs[] = {&tables, &bstart, &njobs};
     if ((rc = launch(j.module->f_seed, j.blocks, SNELLY_BLOCK, sargs))) return rc;
     auto try_cfg = [&](const WfConfig& cfg, float* ms) -> int {
-      if (cfg.parts != j.wfc.parts) {  // another split into pixel ranges: new buffers
+      if (cfg.parts != j.wfc.parts || cfg.interleave != j.wfc.interleave) {  // another split into pixel ranges: new buffers
         if (cudaStreamSynchronize(stream) != cudaSuccess) return fail(SNELLY_EDEVICE, "autotune sync failed");
         release_wavefront(j);
         j.wfc = cfg;
@@ -420,7 +433,8 @@ int Context::autotune(Job& j) {
                   {&WfConfig::grab, {16, 32, 64}},        {&WfConfig::refill, {2, 4, 8}},
                   {&WfConfig::block, {64, 128}},          {&WfConfig::park_left, {0, 8, 32, 128}},
                   {&WfConfig::walker, {0, 1}},            {&WfConfig::lane_rays, {1, 2, 4, 8, 16}},
-                  {&WfConfig::overlap, {0, 1}},           {&WfConfig::shade_share, {3, 5, 8}}};
+                  {&WfConfig::overlap, {0, 1}},           {&WfConfig::shade_share, {3, 5, 8}},
+                  {&WfConfig::interleave, {0, 1}}};
     const unsigned nfields = sizeof fields / sizeof fields[0];
     const bool walks = j.module->f_wf_walk && j.params.subsurfaceMFP > 0.0f;
     auto descend = [&](unsigned k) -> int {  // try every value of field k against the best so far
@@ -443,10 +457,13 @@ int Context::autotune(Job& j) {
     };
     for (unsigned k = 0; k < nfields; ++k)
       if ((rc = descend(k))) return rc;
-    // the pixel ranges and the extend grid's rays per lane decide together how the ranges'
-    // launches share the GPU: a second pass over both
+    // the pixel ranges (their number and how they deal out the rows) and the extend grid's rays
+    // per lane decide together how the ranges' launches share the GPU: a second pass over them
     for (unsigned k = 0; k < nfields; ++k)
-      if ((fields[k].f == &WfConfig::parts || fields[k].f == &WfConfig::lane_rays) && (rc = descend(k))) return rc;
+      if ((fields[k].f == &WfConfig::parts || fields[k].f == &WfConfig::lane_rays ||
+           fields[k].f == &WfConfig::interleave) &&
+          (rc = descend(k)))
+        return rc;
     float mega_ms = 0.0f;
     if ((rc = time_frames(j, SNELLY_KERNEL_MEGA, &mega_ms))) return rc;
     best.kernel = mega_ms < best_ms ? SNELLY_KERNEL_MEGA : SNELLY_KERNEL_WAVEFRONT;
@@ -458,7 +475,7 @@ int Context::autotune(Job& j) {
     release_wavefront(j);
     return SNELLY_OK;
   }
-  if (best.cfg.parts != j.wfc.parts) {
+  if (best.cfg.parts != j.wfc.parts || best.cfg.interleave != j.wfc.interleave) {
     if (cudaStreamSynchronize(stream) != cudaSuccess) return fail(SNELLY_EDEVICE, "autotune sync failed");
     release_wavefront(j);
     j.wfc = best.cfg;
