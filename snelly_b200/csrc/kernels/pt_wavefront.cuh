@@ -367,7 +367,7 @@ extern "C" __global__ void __launch_bounds__(SNELLY_BLOCK) snelly_wf_generate(co
 // marching sign, PT:888-900) is such a step too, so refilled lanes march in step with the rest of
 // the warp. Idle lanes are refilled when at least `refill` of them are idle, or when none of the
 // warp is busy, from a range of `grab` items the warp claims from the global work head with one
-// atomic (all three chosen by the host's autotuner; 8, 32 and 4 by default). Once the work of the
+// atomic (all three chosen by the host's autotuner; 8, 32 and 8 by default). Once the work of the
 // iteration is exhausted, a warp marches at most `drain` more steps
 // (0: no limit) and then parks its unfinished rays (distance, sign, step count) for the next
 // iteration, so no launch waits for the few longest rays. The march of a ray is the same sequence

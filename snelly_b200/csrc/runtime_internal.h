@@ -72,16 +72,16 @@ struct Module {
 // Launch configuration of a wavefront job: chosen per (scene module, image-size class) by the
 // autotuner, or the context's defaults.
 struct WfConfig {
-  int parts = 3;        // concurrent pixel ranges (one per 65,536 pixels at most)
+  int parts = 8;        // concurrent pixel ranges (one per 65,536 pixels at most)
   int shade_split = 0;  // the shade stage as one launch per material segment
   int drain = 32;       // steps an extend warp marches once its work runs out before parking (0: never)
   int chunk = 8;        // sphere-tracing steps between refills of idle lanes
   int grab = 32;        // work items a warp claims from the work head at a time
-  int refill = 4;       // idle lanes of a warp that trigger a refill
+  int refill = 8;       // idle lanes of a warp that trigger a refill
   int block = 128;      // threads per block of the extend and shade launches (64 or 128)
-  int park_left = 32;   // stop parking once at most park_left / 1024 of the paths are unfinished
+  int park_left = 0;    // stop parking once at most park_left / 1024 of the paths are unfinished
   int walker = 0;       // subsurface walks by the persistent walker (1) or one thread per walk (0)
-  int lane_rays = 8;    // extend grid: one lane per lane_rays rays the iteration may hold (a
+  int lane_rays = 16;   // extend grid: one lane per lane_rays rays the iteration may hold (a
                         // smaller grid lets the ranges' extend launches share the GPU)
   int overlap = 1;      // the frames of one advance overlap (a path that finishes its pixel's sample
                         // starts the pixel's next) rather than run one after another
@@ -161,7 +161,8 @@ struct Context {
   std::map<std::string, Tuned> tuned;  // autotuner decisions per (module, image-size class)
   // Wavefront defaults; a field set from the environment (SNELLY_WF_SPLIT, SNELLY_WF_DRAIN,
   // SNELLY_WF_SHADE_SPLIT, SNELLY_WF_CHUNK, SNELLY_WF_GRAB, SNELLY_WF_REFILL, SNELLY_WF_BLOCK,
-  // SNELLY_WF_PARK_LEFT, SNELLY_WF_WALKER, SNELLY_WF_LANE_RAYS) is also kept fixed by the autotuner.
+  // SNELLY_WF_PARK_LEFT, SNELLY_WF_WALKER, SNELLY_WF_LANE_RAYS, SNELLY_WF_OVERLAP,
+  // SNELLY_WF_SHADE_SHARE, SNELLY_WF_INTERLEAVE) is also kept fixed by the autotuner.
   WfConfig wf_default;
   unsigned wf_fixed = 0;             // bit per WfConfig field, in declaration order
   int wf_park_iters = -1;            // iterations that may park rays; -1: 3 x (max_bounces + 2) (SNELLY_WF_PARK_ITERS)

@@ -394,7 +394,12 @@ int Context::time_frames(Job& j, int kernel, float* ms_per_frame) {
 // are not varied), then the path-per-thread
 // kernel, keeps the fastest and caches the decision; the job's state is seeded again afterwards
 // by the caller. The size class is the power of two nearest the pixel count (tail effects make
-// the choice size-dependent).
+// the choice size-dependent). A candidate must beat the best so far by 1.5% to replace it.
+// A candidate replaces the best configuration so far only when it is faster by more than the
+// timing noise of one short window (about 1-2%), so that noise does not walk the choice away
+// from the defaults (measured on the 1080p fractal workload) or from a better earlier value.
+static constexpr float kTuneMargin = 0.985f;
+
 int Context::autotune(Job& j) {
   const long long npix = (long long)j.desc.width * j.desc.height;
   int cls = 0;
@@ -448,7 +453,7 @@ int Context::autotune(Job& j) {
           continue;  // too small for that many ranges
         float ms = 0.0f;
         if (int r = try_cfg(cfg, &ms)) return r;
-        if (ms < best_ms) {
+        if (ms < best_ms * kTuneMargin) {
           best_ms = ms;
           best.cfg = cfg;
         }

@@ -1,6 +1,6 @@
 """Parity on the exact configuration the benchmark times: the 1920x1080 dispersive Menger sponge,
 gold sphere and ground (seed 2) through the production build (fast math), the integrator the
-autotuner picks (the wavefront) and the default split into three concurrent pixel ranges, against
+autotuner picks (the wavefront) and the concurrent pixel ranges it chooses, against
 the reference's own path tracer built for the CPU (golden fixtures, tests/golden/make_golden.py).
 C0 is checked at its own 256x256 and 16 spp. Tolerances are written in each test."""
 import os
