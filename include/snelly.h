@@ -212,9 +212,11 @@ int snelly_job_kernel(snelly_ctx* ctx, uint64_t job_id, int* kernel_mode);
  * walks by the persistent walker (1) or one thread per walk (0), the rays an iteration may hold
  * per lane of the extend grid, whether the frames of one advance overlap (1: a path that
  * finishes its pixel's sample starts the pixel's next one; 0: frame after frame), the eighths
- * of the shade stage's resident blocks its grid may fill, and whether the pixel ranges are the
- * image's rows dealt to the ranges in turn (1) or contiguous runs of rows (0). */
-#define SNELLY_WF_CONFIG_FIELDS 13
+ * of the shade stage's resident blocks its grid may fill, whether the pixel ranges are the
+ * image's rows dealt to the ranges in turn (1) or contiguous runs of rows (0), and whether
+ * vertices that collide in a heterogeneous medium scatter in a stage of their own (1) or inside
+ * the shade stage (0). */
+#define SNELLY_WF_CONFIG_FIELDS 14
 int snelly_job_wavefront_config(snelly_ctx* ctx, uint64_t job_id, int* out);
 /* Start a job from saved state instead of seeding (resume). */
 int snelly_restore(snelly_ctx* ctx, uint64_t scene_id, const snelly_render_desc* desc, const uint32_t* rng,

@@ -27,7 +27,7 @@ U_IVEC2, U_IVEC3, U_IVEC4, U_MAT2, U_MAT3, U_MAT4, U_SAMPLER2D, U_SAMPLER3D = 6,
 IOR_MODELS = {"abbe": 0, "sellmeier": 1, "sellmeier2": 2, "polyanskiy": 3, "cauchy": 4}
 # snelly_job_wavefront_config's fields, in order (SNELLY_WF_CONFIG_FIELDS of them)
 WF_CONFIG_NAMES = ("parts", "shade_split", "drain", "chunk", "grab", "refill", "block", "park_left", "walker",
-                   "lane_rays", "overlap", "shade_share", "interleave")
+                   "lane_rays", "overlap", "shade_share", "interleave", "volume_stage")
 
 
 def header_define(name):

@@ -1173,7 +1173,7 @@ class Context:
         """A wavefront job's launch configuration as a dict (pixel ranges, per-material shade
         launches, drain steps, refill chunk, claim size, refill threshold, block size, parking
         threshold, persistent walker, rays per extend lane, overlapping frames, shade grid share,
-        interleaved pixel ranges)."""
+        interleaved pixel ranges, the heterogeneous medium's own scatter stage)."""
         out = (ctypes.c_int * len(N.WF_CONFIG_NAMES))()
         N.check(self._lib.snelly_job_wavefront_config(self._h, jid, out))
         return dict(zip(N.WF_CONFIG_NAMES, out))

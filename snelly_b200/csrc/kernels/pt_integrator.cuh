@@ -412,7 +412,7 @@ SD_FN Rad resolve_deferred(const Ctx& c, const DeferredNee& nd, const bool occlu
   return nd.thr * glsl::min(Rad(c.P.radianceClamp), Ld);
 }
 
-enum { VERTEX_CONTINUE = 0, VERTEX_DONE = 1, VERTEX_SSS = 2 };
+enum { VERTEX_CONTINUE = 0, VERTEX_DONE = 1, VERTEX_SSS = 2, VERTEX_VOLUME = 3 };
 
 // A surface vertex that chose the subsurface walk: what the rest of the vertex needs.
 struct SssEntry {
@@ -537,16 +537,25 @@ SD_FN int hv_scatter(const Ctx& c, PathState& s, const vec3& ps, Rng& g) {
 // Everything of one loop iteration of the camera path after the ray has been traced (`h`).
 // With `nd` non-null the surface vertex's sky/sun next-event estimate is deferred into it; with
 // `sss` non-null a vertex that chooses the subsurface walk stops before it, fills `sss` and
-// returns VERTEX_SSS (the walk stage finishes it with sss_step).
+// returns VERTEX_SSS (the walk stage finishes it with sss_step); with `vol_ps` non-null a vertex
+// that collides in the heterogeneous medium stops there, stores the collision point in `vol_ps`
+// and returns VERTEX_VOLUME (the volume stage finishes it with hv_scatter).
 SD_FN int vertex_step(const Ctx& c, PathState& s, const Hit& h, int vertex, Rng& g, DeferredNee* nd,
-                      SssEntry* sss = nullptr) {
+                      SssEntry* sss = nullptr, vec3* vol_ps = nullptr) {
   const SnellyParams& P = c.P;
   (void)vertex;
+  (void)vol_ps;
 #ifdef HAS_HETERO_VOLUME
   {  // the medium before the hit (or the escape): a collision makes this a scattering vertex
     vec3 ps(0.0f);
     const float seg = h.hit ? glsl::length(h.p - s.pW) : P.maxLengthScale;
-    if (hv_collision(c, s.pW, s.rayDir, seg, g, ps)) return hv_scatter(c, s, ps, g);
+    if (hv_collision(c, s.pW, s.rayDir, seg, g, ps)) {
+      if (vol_ps) {
+        *vol_ps = ps;
+        return VERTEX_VOLUME;
+      }
+      return hv_scatter(c, s, ps, g);
+    }
   }
 #endif
   float rayLength = P.maxLengthScale;

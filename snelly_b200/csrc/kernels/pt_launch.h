@@ -48,7 +48,8 @@ typedef struct JobRec {
 #define WF_WHEAD 17 // the persistent walker's work head over that queue
 #define WF_XQ 18    // walks that ended (exit queue count, read by the walk-exit stage)
 #define WF_HEAD 19  // extend work heads [2] (ping-pong by iteration parity)
-#define WF_COUNTERS (WF_HEAD + 2)
+#define WF_VOL 21   // medium-scatter queue count (filled by the shade stage, read by the volume stage)
+#define WF_COUNTERS (WF_VOL + 1)
 typedef struct WfBuffers {
   float4* rec;      // path records, rec_f4 float4 slots per path
   float4* mt;       // march state of a parked ray (distance, sign, step count), by ray id
@@ -61,6 +62,7 @@ typedef struct WfBuffers {
                     // entries each: finish/miss, surface, metal, dielectric
   int* qsss;        // paths whose surface vertex chose the subsurface walk (one iteration's)
   int* qexit;       // paths whose walk the persistent walker finished (one iteration's)
+  int* qvol;        // paths whose vertex scatters in the heterogeneous medium (one iteration's)
   int* cnt;         // counters (WF_*)
   int paths;
   int pixel_begin;  // contiguous range (pixel_group 0): its first pixel; interleaved: the range's index
@@ -70,4 +72,5 @@ typedef struct WfBuffers {
   int slot;         // the job's constant-memory parameter and uniform slot
   int samples;      // samples per pixel one generate launch starts: a path that finishes its
                     // pixel's sample starts the pixel's next one in place until this many are done
+  int vol_stage;    // 1: the shade stage hands medium collisions to the volume stage (queue qvol)
 } WfBuffers;

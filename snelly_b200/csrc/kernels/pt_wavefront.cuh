@@ -391,6 +391,7 @@ extern "C" __global__ void __launch_bounds__(SNELLY_BLOCK) snelly_wf_extend(WfBu
     cnt[WF_SSS] = 0;
     cnt[WF_WHEAD] = 0;
     cnt[WF_XQ] = 0;
+    cnt[WF_VOL] = 0;
     cnt[WF_HEAD + nxt] = 0;
     for (int k = 0; k < 4; ++k) cnt[WF_Q + 4 * nxt + k] = 0;
   }
@@ -562,10 +563,13 @@ namespace sdev {
 // Shade one queued path of iteration `it`: resolve the previous vertex's deferred next-event
 // estimate with its shadow results, run the vertex (vertex_step) with the sky/sun shadow rays
 // deferred, and queue what the path waits for next. MAT is the material every path of the calling
-// kernel hit (MAT_INVAL: read it from the record). Returns true when the path finished.
+// kernel hit (MAT_INVAL: read it from the record). Returns true when the path finished. With
+// B.vol_stage, a vertex that collides in the heterogeneous medium stops at the collision point
+// (kept in the R_HIT slot) and joins the volume stage's queue (push_vol).
 template <int MAT>
 SD_FN void shade_path(const JobRec& J, const SnellyParams* gparams, const WfBuffers& B, Scene& sc, int path, int nxt,
-                      bool& push_active, int& push_shadow, bool& push_direct, bool& push_sss, bool& finished) {
+                      bool& push_active, int& push_shadow, bool& push_direct, bool& push_sss, bool& push_vol,
+                      bool& finished) {
   const SnellyParams& P = c_params[B.slot];
   float4* r = rec_of(B.rec, path);
   WfState st;
@@ -597,9 +601,14 @@ SD_FN void shade_path(const JobRec& J, const SnellyParams* gparams, const WfBuff
     }
     DeferredNee nd;
     nd.any = false;
+    vec3 vps(0.0f);  // a collision in the heterogeneous medium, handed to the volume stage
+    vec3* volp = nullptr;
+#ifdef HAS_HETERO_VOLUME
+    if (B.vol_stage) volp = &vps;
+#endif
 #ifdef HAS_SURFACE
     SssEntry se;
-    int rv = vertex_step(c, st.s, h, st.vertex, st.g, &nd, &se);
+    int rv = vertex_step(c, st.s, h, st.vertex, st.g, &nd, &se, volp);
     if (rv == VERTEX_SSS) {  // the walk stage finishes this vertex
       store_sss(r, se);
       st.flags = (flags & ~WF_INDIELE) | (st.s.inDiele ? WF_INDIELE : 0);
@@ -608,8 +617,15 @@ SD_FN void shade_path(const JobRec& J, const SnellyParams* gparams, const WfBuff
       return;
     }
 #else
-    int rv = vertex_step(c, st.s, h, st.vertex, st.g, &nd);
+    int rv = vertex_step(c, st.s, h, st.vertex, st.g, &nd, nullptr, volp);
 #endif
+    if (rv == VERTEX_VOLUME) {  // the volume stage finishes this vertex
+      r[R_HIT] = st3(vps, enc_hit(false, MAT_INVAL));
+      st.flags = (flags & ~WF_INDIELE) | (st.s.inDiele ? WF_INDIELE : 0);
+      store_state(r, st);
+      push_vol = true;
+      return;
+    }
     ++st.vertex;
     finished = rv == VERTEX_DONE || st.vertex > max_bounces(P) || maxc(st.s.thr) < kThroughputEps;
     continues = !finished;
@@ -651,7 +667,7 @@ SD_FN void shade_path(const JobRec& J, const SnellyParams* gparams, const WfBuff
 
 // Queue the outcome of a warp's shaded paths for the next iteration, and count finished paths.
 SD_FN void shade_push(const WfBuffers& B, int* cnt, int nxt, int path, bool push_active, int push_shadow,
-                      bool push_direct, bool push_sss, bool finished) {
+                      bool push_direct, bool push_sss, bool finished, bool push_vol = false) {
   int slot = warp_append(cnt + WF_A + nxt, push_active);
   if (slot >= 0) pp(B.qa, nxt)[slot] = path;
   for (int l = 0; l < 2; ++l) {
@@ -664,6 +680,12 @@ SD_FN void shade_push(const WfBuffers& B, int* cnt, int nxt, int path, bool push
   if (ds >= 0) pp(B.qshade, nxt)[ds] = path;
   int ws = warp_append(cnt + WF_SSS, push_sss);
   if (ws >= 0) B.qsss[ws] = path;
+#ifdef HAS_HETERO_VOLUME
+  int vs = warp_append(cnt + WF_VOL, push_vol);
+  if (vs >= 0) B.qvol[vs] = path;
+#else
+  (void)push_vol;
+#endif
   unsigned fin = __ballot_sync(WF_FULL, finished);
   if (fin && (int)(threadIdx.x & 31) == __ffs(fin) - 1) atomicSub(cnt + WF_LEFT, __popc(fin));
 }
@@ -689,15 +711,16 @@ SD_FN void shade_segments(const JobRec* jobs, const SnellyParams* gparams, const
   for (int base = blockIdx.x * blockDim.x; base < total; base += stride) {
     const int w = base + threadIdx.x;
     int path = 0;
-    bool push_active = false, push_direct = false, push_sss = false, finished = false;
+    bool push_active = false, push_direct = false, push_sss = false, push_vol = false, finished = false;
     int push_shadow = 0;  // bit 0: sky, bit 1: sun
     if (w < total) {
       const int seg = w < n0 ? 0 : (w < n0 + n1 ? 1 : (w < n0 + n1 + n2 ? 2 : 3));
       const int off = w - (seg == 0 ? 0 : (seg == 1 ? n0 : (seg == 2 ? n0 + n1 : n0 + n1 + n2)));
       path = pp(B.qshade, cur)[seg * B.paths + off];
-      shade_path<MAT>(J, gparams, B, sc, path, nxt, push_active, push_shadow, push_direct, push_sss, finished);
+      shade_path<MAT>(J, gparams, B, sc, path, nxt, push_active, push_shadow, push_direct, push_sss, push_vol,
+                      finished);
     }
-    shade_push(B, cnt, nxt, path, push_active, push_shadow, push_direct, push_sss, finished);
+    shade_push(B, cnt, nxt, path, push_active, push_shadow, push_direct, push_sss, finished, push_vol);
   }
 }
 
@@ -777,6 +800,58 @@ extern "C" __global__ void __launch_bounds__(SNELLY_BLOCK, SNELLY_SHADE_MIN_BLOC
         }
       } else {
         st.s.inDiele ? (st.flags |= WF_INDIELE) : (st.flags &= ~WF_INDIELE);
+        store_state(r, st);
+        B.pend[path] = 1;
+        push_active = true;
+      }
+    }
+    shade_push(B, cnt, nxt, path, push_active, 0, false, false, finished);
+  }
+}
+#endif
+
+#ifdef HAS_HETERO_VOLUME
+// The volume stage of iteration `it`: the vertices the shade stage stopped at a collision in the
+// heterogeneous medium scatter there (hv_scatter: the single-scattering albedo, next-event
+// estimates of sky, sun and sphere light through the phase function, with their shadow rays
+// traced inline through the SDFs and ratio-tracked through the medium, then a new direction from
+// the phase function). One thread per path over the volume queue, so a warp holds only medium
+// vertices and their shadow marches; the rest of the vertex (the bounce count, the throughput
+// cut, the pixel's next sample) is the shade stage's, in the same order.
+extern "C" __global__ void __launch_bounds__(SNELLY_BLOCK, SNELLY_SHADE_MIN_BLOCKS) snelly_wf_volume(
+    const JobRec* __restrict__ jobs, const SnellyParams* __restrict__ gparams, WfBuffers B, int it) {
+  using namespace sdev;
+  wf_kernel_entry();
+  const JobRec& J = jobs[0];
+  const SnellyParams& P = c_params[B.slot];
+  int* cnt = B.cnt;
+  const int nxt = (it & 1) ^ 1;
+  const int total = cnt[WF_VOL];
+  Scene sc(uniforms_of(B.slot));
+  sc.INIT();
+  const int stride = gridDim.x * blockDim.x;
+  for (int base = blockIdx.x * blockDim.x; base < total; base += stride) {
+    const int w = base + threadIdx.x;
+    int path = 0;
+    bool push_active = false, finished = false;
+    if (w < total) {
+      path = B.qvol[w];
+      float4* r = rec_of(B.rec, path);
+      WfState st;
+      load_state(r, st);
+      Ctx c{P, gparams, sc, B.slot, 0.0f, vec3(0.0f), make_frame(v3(P.sunDir))};
+      const vec3 xyzw = wavelength_at(c, st.w);
+      const vec3 ps = ld3(r[R_HIT]);
+      int rv = hv_scatter(c, st.s, ps, st.g);
+      ++st.vertex;
+      finished = rv == VERTEX_DONE || st.vertex > max_bounces(P) || maxc(st.s.thr) < kThroughputEps;
+      st.s.inDiele ? (st.flags |= WF_INDIELE) : (st.flags &= ~WF_INDIELE);
+      if (finished) {
+        if (finish_sample(c, J, B, path, st, xyzw)) {
+          finished = false;
+          push_active = true;
+        }
+      } else {
         store_state(r, st);
         B.pend[path] = 1;
         push_active = true;

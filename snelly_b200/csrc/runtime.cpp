@@ -339,6 +339,7 @@ int Context::compile_module(const std::string& src, int math_mode, std::shared_p
              {"snelly_wf_sss", &m->f_wf_sss, false},
              {"snelly_wf_walk", &m->f_wf_walk, false},
              {"snelly_wf_walk_exit", &m->f_wf_walk_exit, false},
+             {"snelly_wf_volume", &m->f_wf_volume, false},
              {"snelly_firsthit", &m->f_firsthit, false},
              {"snelly_ptsimple", &m->f_ptsimple, false}};
   for (auto& f : fns) {
@@ -708,7 +709,8 @@ int snelly_init(snelly_ctx** out, int device, size_t budget) {
                  {"SNELLY_WF_REFILL", &d.refill, 1, 32}, {"SNELLY_WF_BLOCK", &d.block, 64, 128},
                  {"SNELLY_WF_PARK_LEFT", &d.park_left, 0, 1024}, {"SNELLY_WF_WALKER", &d.walker, 0, 1},
                  {"SNELLY_WF_LANE_RAYS", &d.lane_rays, 1, 64}, {"SNELLY_WF_OVERLAP", &d.overlap, 0, 1},
-                 {"SNELLY_WF_SHADE_SHARE", &d.shade_share, 1, 8}, {"SNELLY_WF_INTERLEAVE", &d.interleave, 0, 1}};
+                 {"SNELLY_WF_SHADE_SHARE", &d.shade_share, 1, 8}, {"SNELLY_WF_INTERLEAVE", &d.interleave, 0, 1},
+                 {"SNELLY_WF_VOLUME", &d.vol_stage, 0, 1}};
     for (unsigned k = 0; k < sizeof knobs / sizeof knobs[0]; ++k)
       if (const char* v = getenv(knobs[k].name)) {
         *knobs[k].field = std::max(knobs[k].lo, std::min(atoi(v), knobs[k].hi));
@@ -1188,7 +1190,7 @@ int snelly_job_wavefront_config(snelly_ctx* ctx, uint64_t job_id, int* out) {
   const WfConfig& w = it->second.wfc;
   const int v[SNELLY_WF_CONFIG_FIELDS] = {it->second.wf_parts, w.shade_split, w.drain,  w.chunk,    w.grab,
                                           w.refill,              w.block,       w.park_left, w.walker, w.lane_rays,
-                                          w.overlap,             w.shade_share, w.interleave};
+                                          w.overlap,             w.shade_share, w.interleave, w.vol_stage};
   for (int k = 0; k < SNELLY_WF_CONFIG_FIELDS; ++k) out[k] = v[k];
   return SNELLY_OK;
 }

@@ -55,6 +55,7 @@ struct Module {
   cudaKernel_t f_seed = nullptr, f_frame_mega = nullptr, f_resolve = nullptr;
   cudaKernel_t f_wf_generate = nullptr, f_wf_extend = nullptr, f_wf_shade = nullptr, f_wf_sss = nullptr;
   cudaKernel_t f_wf_walk = nullptr, f_wf_walk_exit = nullptr;  // the persistent subsurface walker
+  cudaKernel_t f_wf_volume = nullptr;  // the heterogeneous medium's scatter stage (null without one)
   int walk_blocks_per_sm = 8;  // resident 128-thread blocks of the walker (occupancy query)
   // the shade stage split by queue segment: misses/finishing, surface, metal, dielectric (null
   // for a material the scene does not have)
@@ -89,6 +90,8 @@ struct WfConfig {
                         // other ranges' extend blocks fit beside a range's shade stage
   int interleave = 1;   // pixel ranges as the image's rows dealt to the ranges in turn (1), so that every
                         // range holds a like share of the scene, or as contiguous runs of rows (0)
+  int vol_stage = 1;    // vertices that collide in a heterogeneous medium scatter in a stage of their
+                        // own (1) rather than inside the shade stage (0)
 };
 
 struct Scene {
@@ -162,7 +165,7 @@ struct Context {
   // Wavefront defaults; a field set from the environment (SNELLY_WF_SPLIT, SNELLY_WF_DRAIN,
   // SNELLY_WF_SHADE_SPLIT, SNELLY_WF_CHUNK, SNELLY_WF_GRAB, SNELLY_WF_REFILL, SNELLY_WF_BLOCK,
   // SNELLY_WF_PARK_LEFT, SNELLY_WF_WALKER, SNELLY_WF_LANE_RAYS, SNELLY_WF_OVERLAP,
-  // SNELLY_WF_SHADE_SHARE, SNELLY_WF_INTERLEAVE) is also kept fixed by the autotuner.
+  // SNELLY_WF_SHADE_SHARE, SNELLY_WF_INTERLEAVE, SNELLY_WF_VOLUME) is also kept fixed by the autotuner.
   WfConfig wf_default;
   unsigned wf_fixed = 0;             // bit per WfConfig field, in declaration order
   int wf_park_iters = -1;            // iterations that may park rays; -1: 3 x (max_bounces + 2) (SNELLY_WF_PARK_ITERS)

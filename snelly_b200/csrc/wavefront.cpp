@@ -21,9 +21,9 @@ int Context::alloc_wavefront(Job& j) {
   const int rec_f4 = j.module->wf_rec_f4;
   if (rec_f4 <= 0) return fail(SNELLY_EDEVICE, "module has no wavefront record layout");
   // per path: the record, parked-ray state (3 rays), shadow flags, pending count, int queues
-  // (2 active, 2 x 2 shadow, 2 x 3 parked, 2 x 4 shade, subsurface walk, walk exit); per part:
-  // counters and the 256-byte alignment of its 16 sub-buffers
-  size_t bytes = ((size_t)rec_f4 * 16 + 3 * 16 + 2 + 4 + (2 + 2 * 2 + 2 * 3 + 2 * 4 + 2) * 4) * P +
+  // (2 active, 2 x 2 shadow, 2 x 3 parked, 2 x 4 shade, subsurface walk, walk exit, medium
+  // scatter); per part: counters and the 256-byte alignment of its 16 sub-buffers
+  size_t bytes = ((size_t)rec_f4 * 16 + 3 * 16 + 2 + 4 + (2 + 2 * 2 + 2 * 3 + 2 * 4 + 3) * 4) * P +
                  (size_t)parts * (4 * WF_COUNTERS + 18 * 256);
   int rc = alloc(j.wf, bytes);
   if (rc) return rc;
@@ -62,6 +62,7 @@ int Context::alloc_wavefront(Job& j) {
     B.qshade[1] = (int*)take(16 * Pk);
     B.qsss = (int*)take(4 * Pk);
     B.qexit = (int*)take(4 * Pk);
+    B.qvol = (int*)take(4 * Pk);
     B.cnt = (int*)take(4 * WF_COUNTERS);
     B.shadow = (unsigned char*)take(2 * Pk);
     B.paths = (int)Pk;
@@ -254,6 +255,8 @@ int Context::enqueue_wavefront(const std::vector<Job*>& js, const std::vector<in
       const int sb = (int)std::max<long long>(sm_count, std::min(shade_blocks, (left + bs - 1) / bs));
       const bool split = cf.shade_split && m.f_wf_shade_seg[0];
       const bool walk = m.f_wf_sss && j.params.subsurfaceMFP > 0.0f;  // vertices may choose the walk
+      const bool volume = m.f_wf_volume && cf.vol_stage;  // medium collisions go to the volume stage
+      B.vol_stage = volume ? 1 : 0;
       void* eargs[] = {&B, &it, &drain, &chunk, &grab, &refill};
       int r = launch_on(R, m.f_wf_extend, eb, bs, eargs);
       if (r) return r;
@@ -272,6 +275,7 @@ int Context::enqueue_wavefront(const std::vector<Job*>& js, const std::vector<in
       } else if (walk && (r = launch_on(R, m.f_wf_sss, sb, bs, sargs))) {  // one thread per walk
         return r;
       }
+      if (volume && (r = launch_on(R, m.f_wf_volume, sb, bs, sargs))) return r;  // the medium vertices
       ++R.it;
       return SNELLY_OK;
     };
@@ -439,12 +443,13 @@ int Context::autotune(Job& j) {
                   {&WfConfig::block, {64, 128}},          {&WfConfig::park_left, {0, 8, 32, 128}},
                   {&WfConfig::walker, {0, 1}},            {&WfConfig::lane_rays, {1, 2, 4, 8, 16}},
                   {&WfConfig::overlap, {0, 1}},           {&WfConfig::shade_share, {3, 5, 8}},
-                  {&WfConfig::interleave, {0, 1}}};
+                  {&WfConfig::interleave, {0, 1}},        {&WfConfig::vol_stage, {0, 1}}};
     const unsigned nfields = sizeof fields / sizeof fields[0];
     const bool walks = j.module->f_wf_walk && j.params.subsurfaceMFP > 0.0f;
     auto descend = [&](unsigned k) -> int {  // try every value of field k against the best so far
       if (wf_fixed & (1u << k)) return SNELLY_OK;
       if (fields[k].f == &WfConfig::walker && !walks) return SNELLY_OK;  // no subsurface walks to time
+      if (fields[k].f == &WfConfig::vol_stage && !j.module->f_wf_volume) return SNELLY_OK;  // no medium
       for (int v : fields[k].values) {
         WfConfig cfg = best.cfg;
         if (cfg.*(fields[k].f) == v) continue;

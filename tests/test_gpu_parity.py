@@ -273,6 +273,36 @@ def test_persistent_walker_does_not_change_results(name):
     np.testing.assert_array_equal(imgs[0], imgs[1])
 
 
+@pytest.mark.parametrize("math_mode", [None, N.MATH_STRICT])
+def test_volume_stage_does_not_change_results(math_mode):
+    """Vertices that collide in the heterogeneous medium (C2's cloud) scatter in a stage of their
+    own, one thread per medium vertex with its shadow marches, or inside the shade stage: the same
+    functions run in the same order on the path's random numbers, so the image is the same bit for
+    bit, in the production and the IEEE-strict builds. The stage's launches show that it ran."""
+    import os
+    from snelly_b200 import api
+    imgs, launches = [], []
+    for stage in ("0", "1"):
+        old = os.environ.pop("SNELLY_WF_VOLUME", None)
+        os.environ["SNELLY_WF_VOLUME"] = stage
+        try:
+            ctx = api.Context(0)
+        finally:
+            os.environ.pop("SNELLY_WF_VOLUME", None)
+            if old is not None:
+                os.environ["SNELLY_WF_VOLUME"] = old
+        before = ctx.launch_count()
+        s, img = gpu_render(ctx, scenes.PyroclasticSubsurface(64, 64), 3, seed=5, math_mode=math_mode,
+                            kernel_mode=N.KERNEL_WAVEFRONT)
+        launches.append(ctx.launch_count() - before)
+        assert ctx.job_wavefront_config(s.job_id())["volume_stage"] == int(stage)
+        imgs.append(img.copy())
+        ctx.destroy_job(s.job_id())
+        ctx.close()
+    assert launches[1] > launches[0], launches
+    np.testing.assert_array_equal(imgs[0], imgs[1])
+
+
 @pytest.mark.parametrize("name", ["c1", "c2", "c2_cloud", "lowsun", "hooks", "atmosphere"])
 def test_overlapping_frames_do_not_change_results(name):
     """The frames of one advance run overlapped (a path that finishes its pixel's sample starts the
