@@ -78,7 +78,38 @@ def prebuild_modules(hosts, math_modes=(0, 1), workers=None):
             o.kernel_mode = 0
             items[(glsl, bytes(o))] = True
     work = list(items)
+    prune_module_cache()
     with cf.ProcessPoolExecutor(max_workers=workers or min(8, os.cpu_count() or 1),
                                 mp_context=mp.get_context("spawn")) as ex:
         list(ex.map(_compile_one, work))
     return len(work)
+
+
+CACHE_DIR = os.path.join(HERE, "_build", "kcache")
+
+
+def module_key_sources():
+    """The files whose contents every module's cache key includes (the runtime's module_key): the
+    kernel directory, the GLSL compatibility header and its swizzle table, the parameter block."""
+    kdir = os.path.join(HERE, "csrc", "kernels")
+    files = [os.path.join(kdir, f) for f in os.listdir(kdir) if not f.startswith(".")]
+    files += [os.path.join(HERE, "csrc", "glslcompat.h"), os.path.join(HERE, "csrc", "glsl_swizzles.inc"),
+              os.path.join(ROOT, "include", "snelly_params.h")]
+    return files
+
+
+def prune_module_cache(cache_dir=CACHE_DIR, sources=None):
+    """Delete cached modules compiled before the latest edit of a file their keys include: such a
+    module's key covers the file's old contents, so no build asks for it again (unless the edit is
+    undone, when it is compiled once more). Without this the cache keeps a full set of modules per
+    kernel edit. Returns the number of files deleted."""
+    if not os.path.isdir(cache_dir):
+        return 0
+    newest = max(os.path.getmtime(f) for f in (sources if sources is not None else module_key_sources()))
+    deleted = 0
+    for f in os.listdir(cache_dir):
+        p = os.path.join(cache_dir, f)
+        if f.endswith(".cubin") and os.path.getmtime(p) < newest:
+            os.remove(p)
+            deleted += 1
+    return deleted

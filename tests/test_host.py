@@ -146,3 +146,25 @@ def test_sdf_asset_scene_binds_the_packed_grid(tmp_path):
     tex, linear = sh.textures["sdfTex"]
     assert tex.shape == (16, 16, 16, 1) and tex.dtype == np.float32 and linear
     assert sh.calls["gridMin"][1] == [-1.0, -1.0, -1.0] and sh.calls["gridSize"][1] == [2.0, 2.0, 2.0]
+
+
+def test_module_cache_prune_drops_modules_older_than_their_sources(tmp_path):
+    """A cached module compiled before the latest edit of a file its key includes can never be
+    asked for again and is deleted; one compiled after it is kept, and so are files that are not
+    modules."""
+    import os
+    from snelly_b200 import build as B
+    src = tmp_path / "kernel.cuh"
+    src.write_text("// source")
+    cache = tmp_path / "kcache"
+    cache.mkdir()
+    old, new, other = cache / "old.cubin", cache / "new.cubin", cache / "notes.txt"
+    for f in (old, new, other):
+        f.write_bytes(b"x")
+    t = os.path.getmtime(src)
+    os.utime(old, (t - 100, t - 100))
+    os.utime(other, (t - 100, t - 100))
+    os.utime(new, (t + 100, t + 100))
+    assert B.prune_module_cache(str(cache), [str(src)]) == 1
+    assert sorted(os.listdir(cache)) == ["new.cubin", "notes.txt"]
+    assert all(os.path.exists(f) for f in B.module_key_sources())
