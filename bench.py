@@ -191,7 +191,7 @@ def workload_config(args, width, height):
     """The workload's definition, printed identically by both arms."""
     return {"workload": WORKLOAD, "width": width, "height": height, "spp_per_step": max(1, args.spp_per_step),
             "image_spp": 64, "max_bounces": 8, "max_march_steps": 512, "dispersive": True,
-            "l2": "flushed between timed steps (256 MiB write); path state 0.7 GB > L2",
+            "l2": "flushed between timed steps (256 MiB write); path state 0.77 GB > L2",
             "parallelism": f"replicas x{args.gpus}"}
 
 
