@@ -243,6 +243,23 @@ def reference_arm(args, rank):
     print(json.dumps(out), flush=True)
 
 
+def rank_max(dist, x):
+    """The largest of every rank's x (each rank passes its own; dist None: one rank)."""
+    if dist is None:
+        return x
+    import torch
+    t = torch.tensor([x], dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replica_throughput(world, samples_per_step, steps, slowest_s):
+    """Replicas (one job per GPU, no collective on the data path): every rank renders
+    samples_per_step path samples per step, so the job renders world times that over the slowest
+    rank's time."""
+    return world * samples_per_step * steps / slowest_s
+
+
 def gpu_arm(args, rank, world, local_rank):
     import ctypes
 
@@ -262,11 +279,7 @@ def gpu_arm(args, rank, world, local_rank):
             dist.barrier()
 
     def allmax(x):
-        if dist is None:
-            return x
-        t = torch.tensor([x], dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+        return rank_max(dist, x)
 
     ctx = api.Context(local_rank)
     peak_tflops, _ = ctx.fp32_peak()
@@ -308,7 +321,7 @@ def gpu_arm(args, rank, world, local_rank):
     clk = clocks.stop()
     step_ms = [a.elapsed_time(b) for a, b in zip(starts, ends)]
     total_ms = allmax(sum(step_ms))
-    value = world * samples_per_step * args.steps / (total_ms / 1000.0)
+    value = replica_throughput(world, samples_per_step, args.steps, total_ms / 1000.0)
 
     # ---- end to end through the public API ----------------------------------------------------
     # each step's image is read into one of two page-locked host buffers while the next step renders
@@ -321,7 +334,7 @@ def gpu_arm(args, rank, world, local_rank):
         s.readback(out=pinned[k % 2], wait=False)
     ctx.sync()  # every step's image is on the host
     e2e_s = allmax(time.perf_counter() - t0)
-    e2e_value = world * samples_per_step * args.steps / e2e_s
+    e2e_value = replica_throughput(world, samples_per_step, args.steps, e2e_s)
     assert all(np.isfinite(p).all() for p in pinned)
 
     latency = None
