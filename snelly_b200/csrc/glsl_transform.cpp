@@ -365,6 +365,96 @@ bool uniform_type(const std::string& t, UTypeInfo* u) {
   return true;
 }
 
+// GLSL passes out / inout arguments by copy-in, copy-out, so an argument may be any l-value of the
+// parameter's type, a swizzle such as `p.xz` included; the C++ rewrite passes them by reference,
+// which takes only a variable of that exact type. For a function with out / inout parameters this
+// returns a template overload that takes the other arguments: it copies each such argument into a
+// temporary of the parameter's type, calls the function with the temporaries and assigns them
+// back. The overload is enabled only when some out / inout argument is not an l-value of the
+// parameter's own type (glsl::g_copy_in_out), so every call the reference form accepts still
+// resolves to the function itself. Returns "" for functions without out / inout parameters and
+// for forms it does not handle (array parameters or results).
+std::string copy_in_out_overload(const std::vector<Tok>& t, size_t b, size_t open) {
+  size_t close = match_close(t, open);
+  if (close >= t.size()) return "";
+  size_t nm = open;
+  while (nm > b && (t[nm - 1].k == T_WS || t[nm - 1].k == T_COMMENT)) --nm;
+  if (nm <= b || t[nm - 1].k != T_IDENT) return "";
+  const std::string fname = t[nm - 1].s;
+  std::string ret;
+  for (size_t q = b; q < nm - 1; ++q) {
+    if (t[q].k == T_PUNCT) return "";  // an array result or something else unexpected
+    if (t[q].k == T_IDENT && !dropped_qualifiers().count(t[q].s))
+      ret += (ret.empty() ? "" : " ") + (t[q].s == "float" ? std::string("gfloat") : t[q].s);
+  }
+  if (ret.empty()) return "";
+  struct Param {
+    std::string type;
+    bool byref = false;
+  };
+  std::vector<Param> ps;
+  std::vector<std::string> seg;
+  auto flush = [&]() -> bool {
+    if (seg.empty()) return true;
+    Param p;
+    size_t k = 0;
+    for (; k < seg.size(); ++k) {
+      const std::string& s = seg[k];
+      if (s == "out" || s == "inout") p.byref = true;
+      else if (s != "in" && s != "const" && !dropped_qualifiers().count(s)) break;
+    }
+    if (k >= seg.size()) return false;
+    p.type = seg[k] == "float" ? "gfloat" : seg[k];
+    if (k + 2 < seg.size() || (k + 1 < seg.size() && !is_ident_start(seg[k + 1][0]))) return false;  // arrays
+    if (p.type == "void" && seg.size() == 1) {
+      seg.clear();
+      return true;
+    }
+    ps.push_back(p);
+    seg.clear();
+    return true;
+  };
+  for (size_t q = open + 1; q < close; ++q) {
+    if (t[q].k == T_WS || t[q].k == T_COMMENT) continue;
+    if (t[q].k == T_PUNCT && t[q].s == ",") {
+      if (!flush()) return "";
+      continue;
+    }
+    if (t[q].k == T_PUNCT && t[q].s != "[" && t[q].s != "]") return "";
+    seg.push_back(t[q].s);
+  }
+  if (!flush()) return "";
+  bool any = false;
+  for (auto& p : ps) any = any || p.byref;
+  if (!any) return "";
+  const size_t n = ps.size();
+  auto A = [](size_t k) { return "A" + std::to_string(k) + "_g"; };
+  auto a = [](size_t k) { return "arg" + std::to_string(k) + "_g"; };
+  auto tmp = [](size_t k) { return "tmp" + std::to_string(k) + "_g"; };
+  std::ostringstream os;
+  os << "\n  template <";
+  for (size_t k = 0; k < n; ++k) os << "class " << A(k) << ", ";
+  os << "typename glsl::g_enable_if<glsl::g_copy_in_out<";
+  for (size_t k = 0; k < n; ++k)
+    os << (k ? ", " : "") << "glsl::g_param<" << A(k) << ", " << ps[k].type << ", " << (ps[k].byref ? 1 : 0) << ">";
+  os << ">::value>::type = 0>\n  " << ret << " " << fname << "(";
+  for (size_t k = 0; k < n; ++k) os << (k ? ", " : "") << A(k) << "&& " << a(k);
+  os << ") {";
+  for (size_t k = 0; k < n; ++k)
+    if (ps[k].byref) os << " " << ps[k].type << " " << tmp(k) << "(" << a(k) << ");";
+  std::ostringstream call;
+  call << fname << "(";
+  for (size_t k = 0; k < n; ++k) call << (k ? ", " : "") << (ps[k].byref ? tmp(k) : a(k));
+  call << ")";
+  const bool is_void = ret == "void";
+  os << (is_void ? " " : " auto ret_g = ") << call.str() << ";";
+  for (size_t k = 0; k < n; ++k)
+    if (ps[k].byref) os << " " << a(k) << " = " << tmp(k) << ";";
+  if (!is_void) os << " return ret_g;";
+  os << " }\n";
+  return os.str();
+}
+
 }  // namespace
 
 std::string glsl_rewrite_fragment(const std::string& src) {
@@ -486,6 +576,7 @@ bool glsl_transform(const std::string& src, const std::string& name, const std::
     }
     if (is_prototype) { i = e; continue; }
     body += rewrite_tokens(t, b, e);
+    if (is_function) body += copy_in_out_overload(t, b, first_paren);
     i = e;
   }
 

@@ -174,6 +174,10 @@ struct vec2 {
   GLSL_FN vec2(gfloat a, gfloat b) { x = a; y = b; }
   GLSL_FN explicit vec2(const vec3& v);
   GLSL_FN explicit vec2(const vec4& v);
+  // a constructor may take only the leading components of its last argument (GLSL ES 3.00 5.4.2)
+  GLSL_FN vec2(gfloat a, const vec2& v) { x = a; y = v.x; }
+  // float(v): the first component
+  GLSL_FN explicit operator gfloat() const { return d[0]; }
   GLSL_FN vec2& operator=(const vec2& o) { x = o.x; y = o.y; return *this; }
   GLSL_FN gfloat& operator[](int i) { return d[i]; }
   GLSL_FN const gfloat& operator[](int i) const { return d[i]; }
@@ -201,6 +205,11 @@ struct vec3 {
   GLSL_FN vec3(const vec2& v, gfloat c) { x = v.x; y = v.y; z = c; }
   GLSL_FN vec3(gfloat a, const vec2& v) { x = a; y = v.x; z = v.y; }
   GLSL_FN explicit vec3(const vec4& v);
+  GLSL_FN vec3(gfloat a, gfloat b, const vec2& v) { x = a; y = b; z = v.x; }
+  GLSL_FN vec3(gfloat a, gfloat b, const vec3& v) { x = a; y = b; z = v.x; }
+  GLSL_FN vec3(const vec2& u, const vec2& v) { x = u.x; y = u.y; z = v.x; }
+  GLSL_FN vec3(gfloat a, const vec3& v) { x = a; y = v.x; z = v.y; }
+  GLSL_FN explicit operator gfloat() const { return d[0]; }
   GLSL_FN vec3& operator=(const vec3& o) { x = o.x; y = o.y; z = o.z; return *this; }
   GLSL_FN gfloat& operator[](int i) { return d[i]; }
   GLSL_FN const gfloat& operator[](int i) const { return d[i]; }
@@ -232,6 +241,13 @@ struct vec4 {
   GLSL_FN vec4(const vec2& u, gfloat c, gfloat e) { x = u.x; y = u.y; z = c; w = e; }
   GLSL_FN vec4(gfloat c, gfloat e, const vec2& u) { x = c; y = e; z = u.x; w = u.y; }
   GLSL_FN vec4(gfloat c, const vec2& u, gfloat e) { x = c; y = u.x; z = u.y; w = e; }
+  GLSL_FN vec4(gfloat a_, gfloat b_, gfloat c_, const vec2& v) { x = a_; y = b_; z = c_; w = v.x; }
+  GLSL_FN vec4(gfloat a_, gfloat b_, gfloat c_, const vec3& v) { x = a_; y = b_; z = c_; w = v.x; }
+  GLSL_FN vec4(gfloat a_, gfloat b_, const vec3& v) { x = a_; y = b_; z = v.x; w = v.y; }
+  GLSL_FN vec4(const vec3& u, const vec2& v) { x = u.x; y = u.y; z = u.z; w = v.x; }
+  GLSL_FN vec4(const vec3& u, const vec3& v) { x = u.x; y = u.y; z = u.z; w = v.x; }
+  GLSL_FN vec4(const vec2& u, const vec3& v) { x = u.x; y = u.y; z = v.x; w = v.y; }
+  GLSL_FN explicit operator gfloat() const { return d[0]; }
   GLSL_FN vec4& operator=(const vec4& o) { x = o.x; y = o.y; z = o.z; w = o.w; return *this; }
   GLSL_FN gfloat& operator[](int i) { return d[i]; }
   GLSL_FN const gfloat& operator[](int i) const { return d[i]; }
@@ -339,6 +355,7 @@ struct ivec2 {
   GLSL_FN explicit ivec2(const vec2& v) : x(int(s_tofloat(v.x))), y(int(s_tofloat(v.y))) {}
   GLSL_FN int& operator[](int i) { return i == 0 ? x : y; }
   GLSL_FN int operator[](int i) const { return i == 0 ? x : y; }
+  GLSL_FN explicit operator vec2() const;
 };
 struct ivec3 {
   int x, y, z;
@@ -349,16 +366,71 @@ struct ivec3 {
       : x(int(s_tofloat(v.x))), y(int(s_tofloat(v.y))), z(int(s_tofloat(v.z))) {}
   GLSL_FN int& operator[](int i) { return i == 0 ? x : (i == 1 ? y : z); }
   GLSL_FN int operator[](int i) const { return i == 0 ? x : (i == 1 ? y : z); }
+  GLSL_FN explicit operator vec3() const;
 };
 struct ivec4 {
   int x, y, z, w;
   GLSL_FN ivec4() : x(0), y(0), z(0), w(0) {}
   GLSL_FN explicit ivec4(int a) : x(a), y(a), z(a), w(a) {}
   GLSL_FN ivec4(int a, int b, int c, int e) : x(a), y(b), z(c), w(e) {}
+  GLSL_FN explicit operator vec4() const;
 };
-struct bvec2 { bool x, y; };
-struct bvec3 { bool x, y, z; };
-struct bvec4 { bool x, y, z, w; };
+struct bvec2 {
+  bool x, y;
+  GLSL_FN explicit operator vec2() const;
+};
+struct bvec3 {
+  bool x, y, z;
+  GLSL_FN explicit operator vec3() const;
+};
+struct bvec4 {
+  bool x, y, z, w;
+  GLSL_FN explicit operator vec4() const;
+};
+// float vectors from integer and boolean ones: vec3(ivec3(i, j, k)), vec4(bvec4(...)) (0 or 1)
+GLSL_FN vec2 to_vec(const ivec2& v) { return vec2(gfloat(float(v.x)), gfloat(float(v.y))); }
+GLSL_FN vec3 to_vec(const ivec3& v) { return vec3(gfloat(float(v.x)), gfloat(float(v.y)), gfloat(float(v.z))); }
+GLSL_FN vec4 to_vec(const ivec4& v) {
+  return vec4(gfloat(float(v.x)), gfloat(float(v.y)), gfloat(float(v.z)), gfloat(float(v.w)));
+}
+GLSL_FN vec2 to_vec(const bvec2& v) { return to_vec(ivec2(v.x, v.y)); }
+GLSL_FN vec3 to_vec(const bvec3& v) { return to_vec(ivec3(v.x, v.y, v.z)); }
+GLSL_FN vec4 to_vec(const bvec4& v) { return to_vec(ivec4(v.x, v.y, v.z, v.w)); }
+GLSL_FN ivec2::operator vec2() const { return to_vec(*this); }
+GLSL_FN ivec3::operator vec3() const { return to_vec(*this); }
+GLSL_FN ivec4::operator vec4() const { return to_vec(*this); }
+GLSL_FN bvec2::operator vec2() const { return to_vec(*this); }
+GLSL_FN bvec3::operator vec3() const { return to_vec(*this); }
+GLSL_FN bvec4::operator vec4() const { return to_vec(*this); }
+// component-wise comparisons and their reductions (GLSL ES 3.00 8.7); `not` is `not_g` after the
+// translator's renaming of C++ keywords
+#define GLSL_REL(NAME, OP)                                                                           \
+  GLSL_FN bvec2 NAME(const vec2& a, const vec2& b) { return bvec2{a.x OP b.x, a.y OP b.y}; }        \
+  GLSL_FN bvec3 NAME(const vec3& a, const vec3& b) { return bvec3{a.x OP b.x, a.y OP b.y, a.z OP b.z}; } \
+  GLSL_FN bvec4 NAME(const vec4& a, const vec4& b) {                                                \
+    return bvec4{a.x OP b.x, a.y OP b.y, a.z OP b.z, a.w OP b.w};                                   \
+  }                                                                                                 \
+  GLSL_FN bvec2 NAME(const ivec2& a, const ivec2& b) { return bvec2{a.x OP b.x, a.y OP b.y}; }      \
+  GLSL_FN bvec3 NAME(const ivec3& a, const ivec3& b) { return bvec3{a.x OP b.x, a.y OP b.y, a.z OP b.z}; } \
+  GLSL_FN bvec4 NAME(const ivec4& a, const ivec4& b) {                                              \
+    return bvec4{a.x OP b.x, a.y OP b.y, a.z OP b.z, a.w OP b.w};                                   \
+  }
+GLSL_REL(lessThan, <)
+GLSL_REL(lessThanEqual, <=)
+GLSL_REL(greaterThan, >)
+GLSL_REL(greaterThanEqual, >=)
+GLSL_REL(equal, ==)
+GLSL_REL(notEqual, !=)
+#undef GLSL_REL
+GLSL_FN bool any(const bvec2& v) { return v.x || v.y; }
+GLSL_FN bool any(const bvec3& v) { return v.x || v.y || v.z; }
+GLSL_FN bool any(const bvec4& v) { return v.x || v.y || v.z || v.w; }
+GLSL_FN bool all(const bvec2& v) { return v.x && v.y; }
+GLSL_FN bool all(const bvec3& v) { return v.x && v.y && v.z; }
+GLSL_FN bool all(const bvec4& v) { return v.x && v.y && v.z && v.w; }
+GLSL_FN bvec2 not_g(const bvec2& v) { return bvec2{!v.x, !v.y}; }
+GLSL_FN bvec3 not_g(const bvec3& v) { return bvec3{!v.x, !v.y, !v.z}; }
+GLSL_FN bvec4 not_g(const bvec4& v) { return bvec4{!v.x, !v.y, !v.z, !v.w}; }
 
 // ---- matrices (column-major) --------------------------------------------------------------
 struct mat2 {
@@ -442,6 +514,23 @@ GLSL_FN mat4 operator+(const mat4& a, const mat4& b) {
 }
 GLSL_FN vec3& vec3::operator*=(const mat3& m) { return *this = (*this) * m; }
 GLSL_FN vec4& vec4::operator*=(const mat4& m) { return *this = (*this) * m; }
+// the remaining component-wise matrix operators and the compound assignments GLSL defines
+// (m *= n is m = m * n, the linear-algebra product)
+GLSL_FN mat2 operator/(const mat2& a, gfloat s) { return mat2(a.c[0] / s, a.c[1] / s); }
+GLSL_FN mat3 operator/(const mat3& a, gfloat s) { return mat3(a.c[0] / s, a.c[1] / s, a.c[2] / s); }
+GLSL_FN mat4 operator/(const mat4& a, gfloat s) { return mat4(a.c[0] / s, a.c[1] / s, a.c[2] / s, a.c[3] / s); }
+#define GLSL_MAT_OPS(M)                                                                   \
+  GLSL_FN M operator-(const M& a) { return a * gfloat(-1); }                              \
+  GLSL_FN M operator-(const M& a, const M& b) { return a + (-b); }                        \
+  GLSL_FN M& operator*=(M& a, gfloat s) { return a = a * s; }                             \
+  GLSL_FN M& operator/=(M& a, gfloat s) { return a = a / s; }                             \
+  GLSL_FN M& operator*=(M& a, const M& b) { return a = a * b; }                           \
+  GLSL_FN M& operator+=(M& a, const M& b) { return a = a + b; }                           \
+  GLSL_FN M& operator-=(M& a, const M& b) { return a = a - b; }
+GLSL_MAT_OPS(mat2)
+GLSL_MAT_OPS(mat3)
+GLSL_MAT_OPS(mat4)
+#undef GLSL_MAT_OPS
 GLSL_FN mat2 transpose(const mat2& m) { return mat2(m.c[0].x, m.c[1].x, m.c[0].y, m.c[1].y); }
 GLSL_FN mat3 transpose(const mat3& m) {
   return mat3(m.c[0].x, m.c[1].x, m.c[2].x, m.c[0].y, m.c[1].y, m.c[2].y, m.c[0].z, m.c[1].z, m.c[2].z);
@@ -471,6 +560,49 @@ GLSL_FN mat3 inverse(const mat3& m) {
   gfloat id = gfloat(1) / (a.x * r0.x + b.x * r0.y + e.x * r0.z);
   return mat3(r0 * id, r1 * id, r2 * id);
 }
+
+// ---- out / inout arguments ----------------------------------------------------------------
+// The translator gives each scene function with out / inout parameters a template overload
+// that passes those arguments by copy-in, copy-out, as GLSL does, so that a swizzle or a
+// component view can be passed (f(p.xz) writes back into p). These traits decide which calls it
+// takes: every argument must convert to its parameter's type, every out / inout argument must
+// also take the result back by assignment, and at least one out / inout argument must not be an
+// l-value of the parameter's own type (those calls go to the function itself).
+#ifdef GLSL_DEVICE
+#define GLSL_DECL __host__ __device__
+#else
+#define GLSL_DECL
+#endif
+template <class T> GLSL_DECL T&& g_declval() noexcept;  // unevaluated use only
+template <bool B> struct g_enable_if {};
+template <> struct g_enable_if<true> { typedef int type; };
+template <class A, class B> struct g_same { static constexpr bool value = false; };
+template <class A> struct g_same<A, A> { static constexpr bool value = true; };
+template <class T> struct g_sink { GLSL_DECL static char take(T); };  // unevaluated use only
+template <class A, class T, class = void> struct g_converts { static constexpr bool value = false; };
+template <class A, class T>
+struct g_converts<A, T, decltype(void(g_sink<T>::take(g_declval<A>())))> { static constexpr bool value = true; };
+template <class A, class T, class = void> struct g_assigns { static constexpr bool value = false; };
+template <class A, class T>
+struct g_assigns<A, T, decltype(void(g_declval<A>() = g_declval<const T&>()))> { static constexpr bool value = true; };
+template <class A, class T, int ByRef> struct g_param;
+template <class A, class T> struct g_param<A, T, 0> {
+  static constexpr bool ok = g_converts<A, T>::value;
+  static constexpr bool exact = true;
+};
+template <class A, class T> struct g_param<A, T, 1> {
+  static constexpr bool ok = g_converts<A, T>::value && g_assigns<A, T>::value;
+  static constexpr bool exact = g_same<A, T&>::value;
+};
+template <class... P> struct g_copy_in_out_all { static constexpr bool ok = true, exact = true; };
+template <class P, class... R> struct g_copy_in_out_all<P, R...> {
+  static constexpr bool ok = P::ok && g_copy_in_out_all<R...>::ok;
+  static constexpr bool exact = P::exact && g_copy_in_out_all<R...>::exact;
+};
+template <class... P> struct g_copy_in_out {
+  static constexpr bool value = g_copy_in_out_all<P...>::ok && !g_copy_in_out_all<P...>::exact;
+};
+#undef GLSL_DECL
 
 // ---- built-in functions -------------------------------------------------------------------
 #define GLSL_MAP1(NAME, IMPL)                                                                  \
