@@ -190,3 +190,22 @@ def test_reference_example_scenes_translate_and_compile():
             failed.append(rel)
     assert tried >= 50, tried
     assert not failed, failed
+
+
+@pytest.mark.reference
+@pytest.mark.parametrize("rel", ["fractals/IFS/mandalay_mod.html", "fractals/doyleSpirals.html"])
+def test_reference_example_scene_compiles_for_the_gpu(rel):
+    """Two example scenes that need the copy-in/copy-out overloads (swizzles passed to inout
+    parameters) and the vector relational functions, conversions and matrix operators, compiled
+    by NVRTC for sm_100a with the path tracer's kernels (no GPU needed)."""
+    import re
+
+    from conftest import REFERENCE
+    from snelly_b200 import scenes
+    from snelly_b200.testing import HostSnelly
+    text = open(os.path.join(REFERENCE, "exampleScenes", rel), encoding="utf-8", errors="replace").read()
+    m = re.search(r"prototype\.shader\s*=\s*function\s*\(\)\s*\{", text)
+    i = text.find("`", m.end())
+    glsl = re.sub(r"\$\{[^}]*\}", "1", text[i + 1:text.find("`", i + 1)])
+    nbytes, _ = N.compile_check(glsl, HostSnelly(scenes.PlainSphere(32, 32)).scene_opts())
+    assert nbytes > 0
