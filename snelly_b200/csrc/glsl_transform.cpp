@@ -380,7 +380,8 @@ std::string copy_in_out_overload(const std::vector<Tok>& t, size_t b, size_t ope
   size_t nm = open;
   while (nm > b && (t[nm - 1].k == T_WS || t[nm - 1].k == T_COMMENT)) --nm;
   if (nm <= b || t[nm - 1].k != T_IDENT) return "";
-  const std::string fname = t[nm - 1].s;
+  // the name the rewrite gave the function (C++-only keywords get the _g suffix)
+  const std::string fname = t[nm - 1].s + (cxx_only_keywords().count(t[nm - 1].s) ? "_g" : "");
   std::string ret;
   for (size_t q = b; q < nm - 1; ++q) {
     if (t[q].k == T_PUNCT) return "";  // an array result or something else unexpected
