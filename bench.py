@@ -162,7 +162,7 @@ def cpu_sampler(host, prefer_reference=True):
     lib = oracle.OracleLib(host.sceneObj.shader(), host.scene_opts())
     p, keep = oracle.host_params(host)
     sh = host.scene_shader()
-    ub = oracle.pack_uniforms(lib.cpp, sh.calls, sh.textures)
+    ub = oracle.pack_uniforms(lib.cpp, sh.calls, sh.textures, params=p)
 
     def run(n, frames=1):
         pix = np.sort(rs.choice(W * H, n, replace=False))

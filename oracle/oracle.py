@@ -132,6 +132,13 @@ def uniform_layout(cpp):
     return out, size
 
 
+def renderer_uniforms(cpp):
+    """Names of the renderer's own uniforms the translation added to the scene's block (the scene
+    reads them without declaring them); their values come from the job's parameters."""
+    body = re.search(r"struct SceneUniforms \{(.*?)\};", cpp, re.S).group(1)
+    return set(re.findall(r"\w+ (\w+);\s*// offset \d+, renderer uniform", body))
+
+
 def sampler_record(kind, array, linear=True):
     """The 32-byte sampler2D / sampler3D record of glslcompat.h for a texture array ((h, w, c) or
     (d, h, w, c) of float32 / float16 / uint8): {data pointer, w, h, [d,] channels, format,
@@ -145,10 +152,13 @@ def sampler_record(kind, array, linear=True):
     return struct.pack("<Q6i", array.ctypes.data, w, h, d, c, fmt, 1 if linear else 0)
 
 
-def pack_uniforms(cpp, calls, textures=None):
+def pack_uniforms(cpp, calls, textures=None, params=None):
     """Uniform block bytes for the recorded shader.uniform* calls ({name: (type, values)}) and
-    the bound textures ({name: (array, linear)}; the arrays must be contiguous and stay alive)."""
+    the bound textures ({name: (array, linear)}; the arrays must be contiguous and stay alive).
+    Renderer uniforms the scene reads without declaring take their values from `params` (the
+    job's SnellyParams), as snelly_render does."""
     layout, size = uniform_layout(cpp)
+    from_params = renderer_uniforms(cpp) if params is not None else set()
     buf = bytearray(size)
     for name, typ, off, alen in layout:
         if typ in ("sampler2D", "sampler3D"):
@@ -156,9 +166,13 @@ def pack_uniforms(cpp, calls, textures=None):
                 arr, linear = textures[name]
                 buf[off:off + 32] = sampler_record(typ, arr, linear)
             continue
-        if name not in calls:
+        if name in from_params:
+            v = getattr(params, name)
+            vals = list(v) if hasattr(v, "__len__") else [v]
+        elif name not in calls:
             continue
-        _, vals = calls[name]
+        else:
+            _, vals = calls[name]
         if typ in ("int",):
             buf[off:off + 4 * len(vals)] = np.asarray(vals, np.int32).tobytes()
         else:
@@ -344,7 +358,7 @@ def flops_per_path(snelly, pixels=2000, frames=2, seed=5):
     pix = np.sort(np.random.RandomState(seed).choice(n, min(pixels, n), replace=False))
     p, keep = host_params(snelly)
     sh = snelly.scene_shader()
-    ub = pack_uniforms(lib.cpp, sh.calls, sh.textures)
+    ub = pack_uniforms(lib.cpp, sh.calls, sh.textures, params=p)
     lib.counts()
     lib.render(p, ub, snelly.width, snelly.height, pix, frames, lib.seed(snelly.seed, pix), threads=1)
     f, sp = lib.counts()

@@ -15,13 +15,53 @@
 
 #include <algorithm>
 #include <cctype>
+#include <cstddef>
 #include <cstdlib>
+#include <cstring>
 #include <map>
 #include <set>
 #include <sstream>
 
+#include "snelly_params.h"
+
 namespace snelly {
 namespace {
+
+// The path tracer's own uniforms (the non-sampler `uniform` declarations of
+// shaders/pathtracer-fragment-shader.glsl) with their GLSL types; SnellyParams holds each under
+// the same name, with the host's conversions applied. Scene code is pasted into that shader, so
+// it may read them.
+struct RendererUniform {
+  const char* name;
+  const char* glsl_type;
+  size_t params_offset;
+};
+#define SNELLY_RU(NAME, TYPE) {#NAME, TYPE, offsetof(SnellyParams, NAME)}
+const RendererUniform kRendererUniforms[] = {
+    SNELLY_RU(resolution, "vec2"), SNELLY_RU(camPos, "vec3"), SNELLY_RU(camDir, "vec3"), SNELLY_RU(camX, "vec3"),
+    SNELLY_RU(camY, "vec3"), SNELLY_RU(camFovy, "float"), SNELLY_RU(camAspect, "float"),
+    SNELLY_RU(camAperture, "float"), SNELLY_RU(camFocalDistance, "float"), SNELLY_RU(filterRadius, "float"),
+    SNELLY_RU(radianceClamp, "float"), SNELLY_RU(skipProbability, "float"), SNELLY_RU(shadowStrength, "float"),
+    SNELLY_RU(maxStepsIsMiss, "bool"), SNELLY_RU(wavelengthSamples, "int"), SNELLY_RU(lengthScale, "float"),
+    SNELLY_RU(minLengthScale, "float"), SNELLY_RU(maxLengthScale, "float"), SNELLY_RU(haveEnvMap, "bool"),
+    SNELLY_RU(envMapVisible, "bool"), SNELLY_RU(envMapPhiRotation, "float"), SNELLY_RU(envMapThetaRotation, "float"),
+    SNELLY_RU(envMapTransitionAngle, "float"), SNELLY_RU(skyPower, "float"), SNELLY_RU(skyTintUp, "vec3"),
+    SNELLY_RU(skyTintDown, "vec3"), SNELLY_RU(sunPower, "float"), SNELLY_RU(sunAngularSize, "float"),
+    SNELLY_RU(sunLatitude, "float"), SNELLY_RU(sunLongitude, "float"), SNELLY_RU(sunColor, "vec3"),
+    SNELLY_RU(sunDir, "vec3"), SNELLY_RU(sunVisibleDirectly, "bool"), SNELLY_RU(sphereLightPosition, "vec3"),
+    SNELLY_RU(sphereLightRadius, "float"), SNELLY_RU(sphereLightPower, "float"), SNELLY_RU(sphereLightColor, "vec3"),
+    SNELLY_RU(metalRoughness, "float"), SNELLY_RU(metalSpecAlbedoRGB, "vec3"), SNELLY_RU(dieleRoughness, "float"),
+    SNELLY_RU(dieleAbsorptionRGB, "vec3"), SNELLY_RU(dieleSpecAlbedoRGB, "vec3"),
+    SNELLY_RU(surfaceDiffuseAlbedoRGB, "vec3"), SNELLY_RU(surfaceSpecAlbedoRGB, "vec3"),
+    SNELLY_RU(surfaceRoughness, "float"), SNELLY_RU(surfaceIor, "float"), SNELLY_RU(subsurface, "float"),
+    SNELLY_RU(subsurfaceAlbedoRGB, "vec3"), SNELLY_RU(subsurfaceMFP, "float"), SNELLY_RU(subsurfaceAnisotropy, "float"),
+    SNELLY_RU(subsurfaceDiffuseWeight, "float"), SNELLY_RU(maxSSSSteps, "int"), SNELLY_RU(atmosphereBoundsMin, "vec3"),
+    SNELLY_RU(atmosphereBoundsMax, "vec3"), SNELLY_RU(atmosphereExtinctionCoeffRGB, "vec3"),
+    SNELLY_RU(atmosphereScatteringCoeffRGB, "vec3"), SNELLY_RU(atmosphereMFP, "float"),
+    SNELLY_RU(atmosphereAnisotropy, "float"), SNELLY_RU(fogEnable, "bool"), SNELLY_RU(fogMaxOpticalDepth, "float"),
+    SNELLY_RU(fogMFP, "float"), SNELLY_RU(fogEmission, "vec3"), SNELLY_RU(fogTint, "vec3"),
+    SNELLY_RU(volumeEmission, "float"), SNELLY_RU(volumeEmissionColorRGB, "vec3")};
+#undef SNELLY_RU
 
 enum TokKind { T_WS, T_COMMENT, T_PP, T_IDENT, T_NUM, T_PUNCT };
 struct Tok {
@@ -470,6 +510,15 @@ bool glsl_transform(const std::string& src, const std::string& name, const std::
   std::map<std::string, long> int_defines;  // simple `#define NAME <int>` for array sizes
   std::string body;                          // struct body (after reference members)
   size_t offset = 0, max_align = 4;
+  // identifiers the source uses (macro bodies included) and the names it declares at global
+  // scope, to find the renderer uniforms it reads without declaring
+  std::set<std::string> referenced, declared;
+  for (const Tok& k : t) {
+    if (k.k == T_IDENT) referenced.insert(k.s);
+    if (k.k == T_PP)
+      for (const Tok& q : tokenize(k.s.substr(1)))
+        if (q.k == T_IDENT) referenced.insert(q.s);
+  }
 
   size_t i = 0;
   while (i < t.size()) {
@@ -479,6 +528,7 @@ bool glsl_transform(const std::string& src, const std::string& name, const std::
       std::istringstream ss(k.s.substr(1));
       std::string dir, nm, val;
       ss >> dir >> nm >> val;
+      if (dir == "define") declared.insert(nm.substr(0, nm.find('(')));
       if (dir == "define" && !val.empty()) {
         char* endp = nullptr;
         long v = std::strtol(val.c_str(), &endp, 0);
@@ -574,11 +624,41 @@ bool glsl_transform(const std::string& src, const std::string& name, const std::
       size_t q = first_paren;
       while (q > b && (t[q - 1].k == T_WS || t[q - 1].k == T_COMMENT)) --q;
       if (q > b && t[q - 1].k == T_IDENT && is_function) out->functions.push_back(t[q - 1].s);
+      if (q > b && t[q - 1].k == T_IDENT) declared.insert(t[q - 1].s);
+    } else {
+      // a global variable (`[const] T name ...`) or a struct type (`struct S ...`) declares a name
+      size_t q = f;
+      while (q < e && t[q].k == T_IDENT && (t[q].s == "const" || dropped_qualifiers().count(t[q].s)))
+        q = next_sig(t, q + 1);
+      const bool st = q < e && t[q].s == "struct";
+      size_t r = next_sig(t, q + 1);
+      if (st && r < e && t[r].k == T_IDENT) declared.insert(t[r].s);
+      else if (!st && r < e && t[r].k == T_IDENT) declared.insert(t[r].s);
     }
     if (is_prototype) { i = e; continue; }
     body += rewrite_tokens(t, b, e);
     if (is_function) body += copy_in_out_overload(t, b, first_paren);
     i = e;
+  }
+
+  // renderer uniforms the source reads but does not declare, after its own uniforms
+  for (auto& u : out->uniforms) declared.insert(u.name);
+  for (const RendererUniform& ru : kRendererUniforms) {
+    if (!referenced.count(ru.name) || declared.count(ru.name)) continue;
+    UTypeInfo ut;
+    uniform_type(ru.glsl_type, &ut);
+    GlslUniform u;
+    u.name = ru.name;
+    u.glsl_type = ru.glsl_type;
+    u.kind = ut.kind;
+    u.components = ut.components;
+    u.elem_size = ut.size;
+    offset = (offset + ut.align - 1) / ut.align * ut.align;
+    max_align = std::max(max_align, ut.align);
+    u.offset = offset;
+    offset += ut.size;
+    u.params_offset = (long)ru.params_offset;
+    out->uniforms.push_back(u);
   }
 
   size_t block_size = (offset + max_align - 1) / max_align * max_align;
@@ -590,7 +670,7 @@ bool glsl_transform(const std::string& src, const std::string& name, const std::
     uniform_type(u.glsl_type, &ut);
     os << "  " << ut.cxx << " " << u.name;
     if (u.array_len) os << "[" << u.array_len << "]";
-    os << ";  // offset " << u.offset << "\n";
+    os << ";  // offset " << u.offset << (u.params_offset >= 0 ? ", renderer uniform" : "") << "\n";
   }
   os << "};\n";
   if (out->uniforms.empty()) block_size = 4;
@@ -617,6 +697,14 @@ bool glsl_transform(const std::string& src, const std::string& name, const std::
   out->code = os.str();
   out->block_size = block_size;
   return true;
+}
+
+void fill_renderer_uniforms(const std::vector<GlslUniform>& uniforms, const void* params,
+                            std::vector<unsigned char>& block) {
+  for (const GlslUniform& u : uniforms)
+    if (u.params_offset >= 0 && u.offset + u.elem_size <= block.size() &&
+        (size_t)u.params_offset + u.elem_size <= sizeof(SnellyParams))
+      std::memcpy(block.data() + u.offset, (const char*)params + u.params_offset, u.elem_size);
 }
 
 }  // namespace snelly

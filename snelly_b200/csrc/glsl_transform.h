@@ -33,6 +33,10 @@ struct GlslUniform {
   int components = 1;    // scalars per element (float/int components; samplers: 0)
   size_t offset = 0;     // byte offset in the uniform block
   size_t elem_size = 0;  // bytes per element
+  // >= 0: one of the renderer's own uniforms that the scene reads without declaring it (scene
+  // code sits inside the reference's fragment shader and sees its uniforms); the value comes from
+  // this byte offset of the job's SnellyParams, which holds every such uniform under its name
+  long params_offset = -1;
 };
 
 struct GlslTransformResult {
@@ -44,12 +48,18 @@ struct GlslTransformResult {
 };
 
 // extra_members: C++ member declarations prepended to the struct body (used when a whole
-// fragment shader is wrapped: gl_FragCoord and the like).
+// fragment shader is wrapped: gl_FragCoord and the like). A renderer uniform (the path tracer's
+// own uniforms, js/renderer.js:520-584) that the source reads but does not declare is added to
+// the uniform block after the source's own uniforms, with its params_offset set.
 bool glsl_transform(const std::string& src, const std::string& name,
                     const std::string& extra_members, GlslTransformResult* out);
 
 // Replace float literals, `float`, parameter qualifiers etc. in a free-standing fragment of
 // GLSL code (no global-scope handling). Used for #define bodies and tests.
 std::string glsl_rewrite_fragment(const std::string& src);
+
+// Copy the values of a block's renderer uniforms (params_offset >= 0) from a SnellyParams.
+void fill_renderer_uniforms(const std::vector<GlslUniform>& uniforms, const void* params,
+                            std::vector<unsigned char>& block);
 
 }  // namespace snelly

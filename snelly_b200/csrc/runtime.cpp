@@ -917,6 +917,7 @@ static int start_job(Context& c, uint64_t scene_id, const snelly_render_desc* de
     j.pick_y = pick->y;
   }
   j.ublock = s.ublock;
+  fill_renderer_uniforms(s.src.xf.uniforms, &j.params, j.ublock);  // renderer uniforms the scene reads
   size_t npix = (size_t)desc->width * desc->height;
   int rc;
   auto bail = [&](int code) {
@@ -1052,6 +1053,7 @@ int snelly_update_job(snelly_ctx* ctx, uint64_t job_id, const snelly_render_desc
   }
   j.params = np;
   j.ublock = j.scene->ublock;
+  fill_renderer_uniforms(j.scene->src.xf.uniforms, &j.params, j.ublock);
   RT_TRY(cudaMemcpyAsync(j.gparams.ptr, &j.params, sizeof(SnellyParams), cudaMemcpyHostToDevice, c.stream));
   RT_TRY(cudaStreamSynchronize(c.stream));  // j.params may change again before the copy runs
   return SNELLY_OK;

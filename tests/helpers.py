@@ -46,7 +46,7 @@ def oracle_firsthit(host, mode, pixels, frames, rng0=None, threads=0):
         rng0 = lib.seed(host.seed, pixels)
     p, keep = oracle.host_params(host)
     sh = host.scene_shader()
-    ub = oracle.pack_uniforms(lib.cpp, sh.calls, sh.textures)
+    ub = oracle.pack_uniforms(lib.cpp, sh.calls, sh.textures, params=p)
     return lib.firsthit(mode, p, ub, host.width, host.height, pixels, frames, rng0, threads)
 
 
@@ -62,7 +62,7 @@ def oracle_render(host, pixels, frames, rng0=None, threads=0):
         rng0 = lib.seed(host.seed, pixels)
     p, keep = oracle.host_params(host)
     sh = host.scene_shader()
-    ub = oracle.pack_uniforms(lib.cpp, sh.calls, sh.textures)
+    ub = oracle.pack_uniforms(lib.cpp, sh.calls, sh.textures, params=p)
     return lib.render(p, ub, host.width, host.height, pixels, frames, rng0, threads)
 
 

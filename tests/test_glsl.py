@@ -157,14 +157,13 @@ def test_constructors_conversions_and_matrix_operators():
 def test_reference_example_scenes_translate_and_compile():
     """Every example scene of the reference whose shader() is one template literal translates and
     compiles (host build) against the compatibility header, with each ${...} substitution replaced
-    by 1. Known exceptions: meshes/PBR_setup reads the renderer's own minLengthScale uniform, which
-    scene code does not see here, and fractals/IFS/meshmenger calls functions it never defines
-    (sd, sdf) and reads undeclared names (size, rot)."""
+    by 1. The one known exception, fractals/IFS/meshmenger, calls functions it never defines (sd,
+    sdf) and reads undeclared names (size, rot)."""
     import glob
     import re
 
     from conftest import REFERENCE
-    known = {"meshes/PBR_setup.html", "fractals/IFS/meshmenger.html"}
+    known = {"fractals/IFS/meshmenger.html"}
     base = os.path.join(REFERENCE, "exampleScenes")
     tried, failed = 0, []
     for f in sorted(glob.glob(os.path.join(base, "**", "*.html"), recursive=True)):
@@ -209,3 +208,28 @@ def test_reference_example_scene_compiles_for_the_gpu(rel):
     glsl = re.sub(r"\$\{[^}]*\}", "1", text[i + 1:text.find("`", i + 1)])
     nbytes, _ = N.compile_check(glsl, HostSnelly(scenes.PlainSphere(32, 32)).scene_opts())
     assert nbytes > 0
+
+
+def test_scene_reads_renderer_uniforms():
+    """Scene code sits inside the reference's fragment shader, so it may read the path tracer's
+    own uniforms (minLengthScale, sunDir, ...) without declaring them. The translation adds each
+    one it reads to the scene's uniform block, after the scene's own uniforms and marked as a
+    renderer uniform, and the job's parameters fill it (snelly_render here; the oracle's uniform
+    packing likewise). A uniform the scene declares itself stays the scene's own."""
+    import oracle
+    from snelly_b200 import _native as N
+    cpp = N.glsl_to_cpp("""uniform float R; uniform float skyPower;
+float SDF_SURFACE(vec3 X) { return length(X) - R - minLengthScale + 0.0 * (sunDir.x + skyPower); }""")
+    layout, size = oracle.uniform_layout(cpp)
+    assert [(n, t, off) for n, t, off, _ in layout] == [("R", "gfloat", 0), ("skyPower", "gfloat", 4),
+                                                         ("minLengthScale", "gfloat", 8), ("sunDir", "vec3", 12)]
+    assert oracle.renderer_uniforms(cpp) == {"minLengthScale", "sunDir"}
+    p = N.SnellyParams()
+    p.minLengthScale = 0.125
+    p.sunDir[:] = [1.0, 2.0, 3.0]
+    p.skyPower = 9.0  # the scene's own skyPower uniform is set by its syncShader, not from here
+    ub = np.frombuffer(oracle.pack_uniforms(cpp, {"R": ("float", [1.5]), "skyPower": ("float", [0.5])}, params=p),
+                       np.float32)
+    assert ub.tolist() == [1.5, 0.5, 0.125, 1.0, 2.0, 3.0]
+    plain = N.glsl_to_cpp("float SDF_SURFACE(vec3 X) { return length(X) - 1.0; }")
+    assert "renderer uniform" not in plain
